@@ -188,12 +188,19 @@ void ref_Rlamch(const char *c, double *out) { st(out, Rlamch_dd(c)); }
 // (Lal::getMinEigen, sdpa_linear.cpp:27-122).
 void ref_lanczos_min_eig(long n, double *L, double *X, double *out) {
     int nn = (int)n;
-    DenseMatrix lMat(nn, nn, DenseMatrix::DENSE), xMat(nn, nn, DenseMatrix::DENSE), Q(nn, nn, DenseMatrix::DENSE);
+    // default-construct first: the sized constructors read members that
+    // only the default constructor initialises (sdpa_struct.cpp:623-642)
+    DenseMatrix lMat, xMat, Q;
+    lMat.initialize(nn, nn, DenseMatrix::DENSE);
+    xMat.initialize(nn, nn, DenseMatrix::DENSE);
+    Q.initialize(nn, nn, DenseMatrix::DENSE);
     for (long i = 0; i < n * n; ++i) {
         lMat.de_ele[i] = ld(L + 2 * i);
         xMat.de_ele[i] = ld(X + 2 * i);
     }
-    Vector o(nn), b(nn), r(nn), q(nn), qold(nn), w(nn), tmp(nn), d1(nn), d2(nn), wv(std::max(1, 3 * nn - 1));
+    Vector o, b, r, q, qold, w, tmp, d1, d2, wv;
+    for (Vector *v : {&o, &b, &r, &q, &qold, &w, &tmp, &d1, &d2}) v->initialize(nn);
+    wv.initialize(std::max(1, 3 * nn - 1));
     st(out, Lal::getMinEigen(lMat, xMat, Q, o, b, r, q, qold, w, tmp, d1, d2, wv));
 }
 
