@@ -1,0 +1,152 @@
+/*
+ * sddd.h - C ABI of the B200 double-double (dd) Newton hot path of SDPA-DD.
+ *
+ * One opaque context per host thread; all problem, iterate and Newton data
+ * stay resident on one GPU.  dd values cross the boundary as sddd_dd
+ * {hi, lo}, byte-compatible with QD's dd_real (double x[2]).  Block spaces
+ * (X, Z, Dx, ...) are the SDP blocks of the problem in order, each
+ * n_l x n_l column-major, concatenated.
+ *
+ * Every call returns an int status: SDDD_OK (0); > 0 only from the
+ * Cholesky entry points, the 1-based column where the matrix stopped being
+ * positive definite (LAPACK info, as the reference's Rpotrf returns);
+ * < 0 an error (sddd_last_error() gives the message).  Nothing calls exit().
+ *
+ * Reference interfaces replaced (file:line in nakatamaho/sdpa-dd 7.1.3):
+ *   reading / InputData   sdpa_io.cpp:428-786, sdpa_dataset.cpp:470-493
+ *   Solutions             sdpa_dataset.cpp:35-143
+ *   Newton                sdpa_newton.cpp:694-1384
+ *   StepLength etc.       sdpa_parts.cpp:244-954
+ *   pinpal / sdpa_dd      sdpa_main.cpp:43-672
+ *   MPLAPACK kernels      mplapack/mpblas_dd.h:38-56, mplapack_dd.h:38-92
+ */
+#ifndef SDDD_H
+#define SDDD_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    double hi, lo;
+} sddd_dd;
+
+typedef struct sddd_ctx sddd_ctx;
+
+#define SDDD_OK 0
+#define SDDD_ERR_ARG (-1)
+#define SDDD_ERR_CUDA (-2)
+#define SDDD_ERR_NOCONV (-3)
+#define SDDD_ERR_STATE (-4)
+#define SDDD_ERR_NOMEM (-5)
+#define SDDD_ERR_IO (-6)
+#define SDDD_ERR_UNSUPPORTED (-7)
+
+/* Parameter (sdpa_parts.h:85-104; defaults sdpa_parts.cpp:136-171). */
+typedef struct {
+    int maxIteration;
+    double epsilonStar, lambdaStar, omegaStar, lowerBound, upperBound, betaStar, betaBar, gammaStar, epsilonDash;
+} sddd_param;
+
+/* Outcome of a solve (the numbers IO::printLastInfo reports,
+ * sdpa_io.cpp:1015-1203, with REVERSE_PRIMAL_DUAL applied). */
+typedef struct {
+    int phase;            /* SolveInfo::phaseType after Phase::reverse */
+    int iterations;
+    int stop_reason;      /* 1 loop condition, 2 Cholesky(B) failed, 3 pdFEAS early stop, 4 cannot move */
+    sddd_dd mu, relative_gap, gap;
+    sddd_dd objValPrimal; /* printed "objValPrimal" = -b.y */
+    sddd_dd objValDual;   /* printed "objValDual" = -C.X */
+    sddd_dd pfeas_error, dfeas_error;
+    double main_loop_seconds, schur_seconds, cholesky_seconds;
+} sddd_result;
+
+const char *sddd_version(void);
+const char *sddd_last_error(const sddd_ctx *ctx);
+
+/* Context on CUDA device `device`. */
+int sddd_create(int device, sddd_ctx **out);
+int sddd_destroy(sddd_ctx *ctx);
+
+/* -- parameters (Parameter::setDefaultParameter / readFile) -- */
+int sddd_param_default(int type, sddd_param *out); /* 0 default, 1 fast, 2 stable */
+int sddd_param_read(const char *path, sddd_param *out);
+
+/* -- problem (IO::read + InputData::initialize_index + changeToDense +
+ *    Newton::computeFormula_SDP) -- */
+/* Read SDPA text: sparse (.dat-s) when `sparse` != 0, else dense (.dat). */
+int sddd_read_problem(sddd_ctx *ctx, const char *path, int sparse, double kappa);
+/* The same from memory: nnz entries (k, blk, i, j, val) in SDPA's
+ * conventions (k = 0 is F_0, 1-based block/row/column, upper triangle);
+ * block_struct as in the file (negative = LP).  Data is copied. */
+int sddd_upload_problem(sddd_ctx *ctx, int m, int nblock, const int *block_struct, const sddd_dd *b, long nnz, const int *k, const int *blk,
+                        const int *i, const int *j, const sddd_dd *val, double kappa);
+/* m, number of SDP blocks, nDim; sizes[] gets the SDP block sizes. */
+int sddd_dims(const sddd_ctx *ctx, int *m, int *nsdp, long *ndim, int *sizes, int cap);
+/* Length in dd of a block space. */
+long sddd_space_len(const sddd_ctx *ctx);
+/* Formula table useFormula[k * nsdp + l] (0 F1, 1 F2, 2 F3, -1 absent). */
+int sddd_formula(const sddd_ctx *ctx, int *out);
+
+/* -- iterate (Solutions) -- */
+int sddd_init_point(sddd_ctx *ctx, sddd_dd lambda);
+/* Set X, y, Z (host arrays) and recompute L_X^-1, L_Z^-1, Z^-1; returns 1
+ * when a Cholesky factorisation of X or Z fails. */
+int sddd_set_point(sddd_ctx *ctx, const sddd_dd *X, const sddd_dd *y, const sddd_dd *Z);
+int sddd_get_point(sddd_ctx *ctx, sddd_dd *X, sddd_dd *y, sddd_dd *Z);
+int sddd_compute_inverse(sddd_ctx *ctx);
+
+/* -- Newton pieces (Newton::Mehrotra split open) -- */
+/* compute_rMat + Make_gVec; dual_infeasible = phase is pFEAS or noINFO. */
+int sddd_newton_rhs(sddd_ctx *ctx, int corrector, sddd_dd beta_mu, int dual_infeasible);
+int sddd_schur_build(sddd_ctx *ctx);   /* Make_bMat */
+int sddd_schur_factor(sddd_ctx *ctx);  /* Cholesky of B; > 0 = failing column */
+int sddd_solve_dy(sddd_ctx *ctx);      /* Dy = B^-1 g */
+int sddd_make_dz_dx(sddd_ctx *ctx, int dual_infeasible);
+/* min eigenvalue of L D L^T for the step length: which = 0 (L_X^-1, Dx) or 1 (L_Z^-1, Dz). */
+int sddd_min_eig(sddd_ctx *ctx, int which, sddd_dd *out);
+int sddd_update(sddd_ctx *ctx, sddd_dd alpha_primal, sddd_dd alpha_dual);
+int sddd_residuals(sddd_ctx *ctx, sddd_dd *norm_primal, sddd_dd *norm_dual);
+/* Inner products: 0 C.X, 1 b.y, 2 X.Z, 3 C.Dx, 4 b.Dy, 5 X.Dz, 6 Dx.Z, 7 Dx.Dz */
+int sddd_inner(sddd_ctx *ctx, int which, sddd_dd *out);
+/* Device arrays to host: 0 X 1 Z 2 y 3 invCholX 4 invCholZ 5 invZ 6 B
+ * 7 g 8 Dx 9 Dy 10 Dz 11 dual residual 12 primal residual.  Returns the
+ * number of dd written (with out == NULL: the number it would write). */
+long sddd_get(sddd_ctx *ctx, int what, sddd_dd *out);
+int sddd_set(sddd_ctx *ctx, int what, const sddd_dd *in);
+
+/* -- the whole solve (pinpal) -- */
+/* display/result may be NULL.  The result file gets the reference's
+ * layout; `display` is the console stream. */
+int sddd_solve(sddd_ctx *ctx, const sddd_param *param, const char *result_path, int print, sddd_result *out);
+/* Step-wise driving of the same loop: start, then sddd_iterate until it
+ * returns non-zero (1 = converged / loop ended, 2, 3, 4 as stop_reason). */
+int sddd_solver_start(sddd_ctx *ctx, const sddd_param *param);
+int sddd_iterate(sddd_ctx *ctx);
+int sddd_solver_result(sddd_ctx *ctx, sddd_result *out);
+/* The reference's command line (sdpa_main.cpp:493-672). */
+int sddd_cli_main(int argc, char **argv);
+
+/* -- dd kernels on device memory (MPLAPACK-like; pointers are device
+ *    pointers to column-major sddd_dd) -- */
+int sddd_Rgemm(sddd_ctx *ctx, char transa, char transb, long m, long n, long k, sddd_dd *A, long lda, sddd_dd *B, long ldb, sddd_dd *C, long ldc);
+int sddd_Rpotrf(sddd_ctx *ctx, long n, sddd_dd *A, long lda); /* lower, returns info */
+int sddd_Rtrsv(sddd_ctx *ctx, char trans, long n, sddd_dd *L, long lda, sddd_dd *x);
+/* Elementwise dd operation on n device values: 0 a+b, 1 a+=b, 2/3 a-b,
+ * 4 a*b, 5 a*=b, 6 a/b, 7 sqrt(a), 8 a*b.hi, 9 a+b.hi, 10 a-b.hi,
+ * 11 a.hi-b, 12 a/b.hi, 13 a.hi/b, 14 -a, 15 |a|, 16 a^2, 17 a.hi+b.hi
+ * (QD 2.3.23 dd_inline.h shapes).  ctx may be NULL. */
+int sddd_dd_op(sddd_ctx *ctx, int op, long n, const sddd_dd *a, const sddd_dd *b, sddd_dd *out);
+
+/* -- host-side dd (no GPU needed) -- */
+/* The same operations on host arrays, as the host scalar control uses them. */
+int sddd_host_dd_op(int op, long n, const sddd_dd *a, const sddd_dd *b, sddd_dd *out);
+/* Decimal string -> dd as QD's dd_real::read (dd_real.cpp:1198). */
+int sddd_host_dd_read(const char *s, sddd_dd *out);
+/* QD's operator<< text with `precision` digits after the point. */
+int sddd_host_dd_to_string(sddd_dd a, int precision, char *buf, int buflen);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

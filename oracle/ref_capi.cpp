@@ -83,6 +83,7 @@ struct RefSolver {
     dd_real alphaPredP, alphaPredD, betaPred, betaCorr, minEigX, minEigZ;
     dd_real muAtStep, thetaPAtStep, thetaDAtStep;
     dd_real objPAtStep, objDAtStep;
+    int phaseAtStep = 0;
 };
 
 } // namespace
@@ -322,6 +323,7 @@ void ref_formula(void *h, int *out) {
 int ref_step(void *h) {
     RefSolver *s = (RefSolver *)h;
     if (!(s->phase.updateCheck(s->currentRes, s->solveInfo, s->param) && s->pIteration < s->param.maxIteration)) return 1;
+    s->phaseAtStep = (int)s->phase.value;
     s->reduction.MehrotraPredictor(s->phase);
     s->beta.MehrotraPredictor(s->phase, s->reduction, s->param);
     s->betaPred = s->beta.value;
@@ -477,6 +479,8 @@ int ref_scalar(void *h, int what, double *out) {
 
 // Phase (SolveInfo::phaseType as int) and iteration counter.
 int ref_phase(void *h) { return (int)((RefSolver *)h)->phase.value; }
+// Phase at the start of the last pass (before the step's updates).
+int ref_phase_at_step(void *h) { return ((RefSolver *)h)->phaseAtStep; }
 int ref_iteration(void *h) { return ((RefSolver *)h)->pIteration; }
 
 } // extern "C"

@@ -1,6 +1,193 @@
-"""sdpa-dd_b200: the SDPA-DD dd Newton hot path on NVIDIA B200 (sm_100a).
+"""sdpa-dd_b200: the SDPA-DD double-double Newton hot path on NVIDIA B200.
 
-The product is the C-ABI library `libsddd.so` (declared in include/sddd.h)
-and the `sdpa_dd_b200` command-line driver built from csrc/.  This Python
-package only locates and binds them (ctypes) and generates workloads.
+The product is the C-ABI library `lib/libsddd.so` (include/sddd.h) and the
+`bin/sdpa_dd_b200` command-line driver, built from csrc/ by build.py.  This
+module binds the library with ctypes for tests and benchmarks; it has no
+compute of its own and raises if the library is missing.
 """
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+import numpy as np
+
+PKG = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libsddd.so"
+BIN_PATH = PKG / "bin" / "sdpa_dd_b200"
+
+DD = np.dtype([("hi", "<f8"), ("lo", "<f8")])
+
+
+class SdddDD(ctypes.Structure):
+    _fields_ = [("hi", ctypes.c_double), ("lo", ctypes.c_double)]
+
+
+class SdddParam(ctypes.Structure):
+    _fields_ = [("maxIteration", ctypes.c_int)] + [
+        (n, ctypes.c_double)
+        for n in ("epsilonStar", "lambdaStar", "omegaStar", "lowerBound", "upperBound", "betaStar", "betaBar", "gammaStar", "epsilonDash")
+    ]
+
+
+class SdddResult(ctypes.Structure):
+    _fields_ = [("phase", ctypes.c_int), ("iterations", ctypes.c_int), ("stop_reason", ctypes.c_int),
+                ("mu", SdddDD), ("relative_gap", SdddDD), ("gap", SdddDD), ("objValPrimal", SdddDD), ("objValDual", SdddDD),
+                ("pfeas_error", SdddDD), ("dfeas_error", SdddDD),
+                ("main_loop_seconds", ctypes.c_double), ("schur_seconds", ctypes.c_double), ("cholesky_seconds", ctypes.c_double)]
+
+
+PHASES = ["noINFO", "pFEAS", "dFEAS", "pdFEAS", "pdINF", "pFEAS_dINF", "pINF_dFEAS", "pdOPT", "pUNBD", "dUNBD"]
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded libsddd.so (raises when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python sdpa-dd_b200/build.py`")
+    L = ctypes.CDLL(str(LIB_PATH))
+    vp, ci, cl, cd, cc = ctypes.c_void_p, ctypes.c_int, ctypes.c_long, ctypes.c_double, ctypes.c_char
+    sig = {
+        "sddd_version": (ctypes.c_char_p, []),
+        "sddd_last_error": (ctypes.c_char_p, [vp]),
+        "sddd_create": (ci, [ci, ctypes.POINTER(vp)]),
+        "sddd_destroy": (ci, [vp]),
+        "sddd_param_default": (ci, [ci, ctypes.POINTER(SdddParam)]),
+        "sddd_param_read": (ci, [ctypes.c_char_p, ctypes.POINTER(SdddParam)]),
+        "sddd_read_problem": (ci, [vp, ctypes.c_char_p, ci, cd]),
+        "sddd_upload_problem": (ci, [vp, ci, ci, vp, vp, cl, vp, vp, vp, vp, vp, cd]),
+        "sddd_dims": (ci, [vp, vp, vp, vp, vp, ci]),
+        "sddd_space_len": (cl, [vp]),
+        "sddd_formula": (ci, [vp, vp]),
+        "sddd_init_point": (ci, [vp, SdddDD]),
+        "sddd_set_point": (ci, [vp, vp, vp, vp]),
+        "sddd_get_point": (ci, [vp, vp, vp, vp]),
+        "sddd_compute_inverse": (ci, [vp]),
+        "sddd_newton_rhs": (ci, [vp, ci, SdddDD, ci]),
+        "sddd_schur_build": (ci, [vp]),
+        "sddd_schur_factor": (ci, [vp]),
+        "sddd_solve_dy": (ci, [vp]),
+        "sddd_make_dz_dx": (ci, [vp, ci]),
+        "sddd_min_eig": (ci, [vp, ci, ctypes.POINTER(SdddDD)]),
+        "sddd_update": (ci, [vp, SdddDD, SdddDD]),
+        "sddd_residuals": (ci, [vp, ctypes.POINTER(SdddDD), ctypes.POINTER(SdddDD)]),
+        "sddd_inner": (ci, [vp, ci, ctypes.POINTER(SdddDD)]),
+        "sddd_get": (cl, [vp, ci, vp]),
+        "sddd_set": (ci, [vp, ci, vp]),
+        "sddd_solve": (ci, [vp, ctypes.POINTER(SdddParam), ctypes.c_char_p, ci, ctypes.POINTER(SdddResult)]),
+        "sddd_solver_start": (ci, [vp, ctypes.POINTER(SdddParam)]),
+        "sddd_iterate": (ci, [vp]),
+        "sddd_solver_result": (ci, [vp, ctypes.POINTER(SdddResult)]),
+        "sddd_cli_main": (ci, [ci, vp]),
+        "sddd_Rgemm": (ci, [vp, cc, cc, cl, cl, cl, vp, cl, vp, cl, vp, cl]),
+        "sddd_Rpotrf": (ci, [vp, cl, vp, cl]),
+        "sddd_Rtrsv": (ci, [vp, cc, cl, vp, cl, vp]),
+        "sddd_dd_op": (ci, [vp, ci, cl, vp, vp, vp]),
+        "sddd_host_dd_op": (ci, [ci, cl, vp, vp, vp]),
+        "sddd_host_dd_read": (ci, [ctypes.c_char_p, vp]),
+        "sddd_host_dd_to_string": (ci, [SdddDD, ci, ctypes.c_char_p, ci]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class SdddError(RuntimeError):
+    pass
+
+
+class Context:
+    """One device context (sddd_create) with its resident problem."""
+
+    GET = {"X": 0, "Z": 1, "y": 2, "invCholX": 3, "invCholZ": 4, "invZ": 5, "B": 6, "g": 7, "Dx": 8, "Dy": 9, "Dz": 10,
+           "dualMat": 11, "primalVec": 12}
+
+    def __init__(self, device: int = 0):
+        self.L = lib()
+        h = ctypes.c_void_p()
+        rc = self.L.sddd_create(device, ctypes.byref(h))
+        if rc != 0:
+            raise SdddError(f"sddd_create failed ({rc}): {self.L.sddd_last_error(None).decode()}")
+        self.h = h
+
+    def _check(self, rc, what):
+        if rc < 0:
+            raise SdddError(f"{what} failed ({rc}): {self.L.sddd_last_error(self.h).decode()}")
+        return rc
+
+    def close(self):
+        if self.h:
+            self.L.sddd_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def read_problem(self, path, sparse=True, kappa=1.2):
+        self._check(self.L.sddd_read_problem(self.h, str(path).encode(), int(sparse), kappa), "read_problem")
+        m, ns, nd = ctypes.c_int(), ctypes.c_int(), ctypes.c_long()
+        sizes = np.zeros(4096, np.int32)
+        self._check(self.L.sddd_dims(self.h, ctypes.byref(m), ctypes.byref(ns), ctypes.byref(nd), _ptr(sizes), 4096), "dims")
+        self.m, self.nsdp, self.ndim = m.value, ns.value, nd.value
+        self.sizes = [int(x) for x in sizes[: self.nsdp]]
+
+    def get(self, what):
+        w = self.GET[what] if isinstance(what, str) else what
+        n = self._check(self.L.sddd_get(self.h, w, None), "get")
+        out = np.zeros(n, DD)
+        self._check(self.L.sddd_get(self.h, w, _ptr(out)), "get")
+        return out
+
+    def set(self, what, arr):
+        w = self.GET[what] if isinstance(what, str) else what
+        arr = np.ascontiguousarray(arr, dtype=DD)
+        self._check(self.L.sddd_set(self.h, w, _ptr(arr)), "set")
+
+    def set_point(self, X, y, Z):
+        X, y, Z = (np.ascontiguousarray(a, dtype=DD) for a in (X, y, Z))
+        return self._check(self.L.sddd_set_point(self.h, _ptr(X), _ptr(y), _ptr(Z)), "set_point")
+
+    def formula(self):
+        out = np.zeros(self.m * self.nsdp, np.int32)
+        self._check(self.L.sddd_formula(self.h, _ptr(out)), "formula")
+        return out.reshape(self.m, self.nsdp)
+
+    def call(self, name, *args):
+        return self._check(getattr(self.L, name)(self.h, *args), name)
+
+    def dd_scalar(self, name, *args):
+        v = SdddDD()
+        self._check(getattr(self.L, name)(self.h, *args, ctypes.byref(v)), name)
+        return v.hi, v.lo
+
+    def solve(self, param: SdddParam, result_path=None, print_=False):
+        r = SdddResult()
+        self._check(self.L.sddd_solve(self.h, ctypes.byref(param), None if result_path is None else str(result_path).encode(), int(print_),
+                                      ctypes.byref(r)), "solve")
+        return r
+
+
+def param(path=None, type_=0) -> SdddParam:
+    p = SdddParam()
+    L = lib()
+    if path is None:
+        rc = L.sddd_param_default(type_, ctypes.byref(p))
+    else:
+        rc = L.sddd_param_read(str(path).encode(), ctypes.byref(p))
+    if rc != 0:
+        raise SdddError(f"parameters: {rc}")
+    return p

@@ -1,0 +1,32 @@
+// Host entry points of the dd dense kernels (blas.cu).  All pointers are
+// device pointers; matrices are column-major dd with a leading dimension.
+#pragma once
+#include "common.cuh"
+
+namespace sddd {
+
+enum GemmMode { GEMM_STORE = 0, GEMM_SUB = 1, GEMM_ACC = 2 };
+constexpr int POTRF_NB = 64;
+
+// C = op(A) op(B) (STORE: sum from zero; SUB: C - p_0 - p_1 - ...;
+// ACC: C + p_0 + ...), batched with strides, optionally the lower triangle
+// only.  op: 'N' or 'T'.
+void gemm(cudaStream_t st, char ta, char tb, int mode, int M, int N, int K, const dd_t *A, long lda, long sA, const dd_t *B, long ldb, long sB,
+          dd_t *C, long ldc, long sC, int batch, bool lower);
+// In-place lower Cholesky; *info_dev = 0 or the failing 1-based column.
+// rdiag_dev holds POTRF_NB dd of scratch.
+void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag_dev);
+void zero_upper(cudaStream_t st, dd_t *A, long lda, int n);
+void trsv_lower(cudaStream_t st, char trans, const dd_t *L, long lda, int n, dd_t *x);
+void inv_lower(cudaStream_t st, const dd_t *L, long lda, int n, dd_t *X, long ldx);
+void trmm_lt(cudaStream_t st, const dd_t *M, long ldm, int n, dd_t *B, long ldb);
+void symmetrize(cudaStream_t st, dd_t *A, int n);
+void fill(cudaStream_t st, dd_t *x, long n, dd_t v);
+void scal(cudaStream_t st, dd_t *y, long n, dd_t a);
+void copy_scal(cudaStream_t st, const dd_t *x, dd_t *y, long n, dd_t a);
+void axpy(cudaStream_t st, const dd_t *x, const dd_t *y, dd_t *z, long n, dd_t a);
+// out = x.y (device scalar); scratch >= 256 dd
+void dot(cudaStream_t st, const dd_t *x, long incx, const dd_t *y, long incy, long n, dd_t *out, dd_t *scratch);
+void maxabs(cudaStream_t st, const dd_t *x, long n, dd_t *out, dd_t *scratch);
+
+} // namespace sddd

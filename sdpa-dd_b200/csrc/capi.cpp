@@ -1,0 +1,487 @@
+// extern "C" boundary (include/sddd.h) over the device solver.
+#include "../../include/sddd.h"
+
+#include <chrono>
+#include <cstring>
+#include <ctime>
+#include <memory>
+#include <string>
+
+#include "blas.h"
+#include "capi_internal.h"
+#include "context.h"
+#include "newton.h"
+#include "solver.h"
+
+struct sddd_ctx {
+    std::unique_ptr<sddd::Context> c;
+    std::unique_ptr<sddd::Solver> solver;
+    std::string err;
+    int stop_reason = 0;
+};
+
+namespace {
+thread_local std::string g_err;
+
+template <class F>
+int guarded(sddd_ctx *ctx, F &&f) {
+    try {
+        if (ctx && ctx->c) cudaSetDevice(ctx->c->device);
+        return f();
+    } catch (const sddd::Error &e) {
+        if (ctx) ctx->err = e.what();
+        g_err = e.what();
+        return e.code;
+    } catch (const std::exception &e) {
+        if (ctx) ctx->err = e.what();
+        g_err = e.what();
+        return SDDD_ERR_STATE;
+    }
+}
+
+sddd::Context &need_problem(sddd_ctx *ctx) {
+    if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
+    if (!ctx->c->have_problem) throw sddd::Error(SDDD_ERR_STATE, "no problem uploaded");
+    return *ctx->c;
+}
+
+sddd::Param to_param(const sddd_param *p) {
+    sddd::Param q;
+    q.maxIteration = p->maxIteration;
+    q.epsilonStar = p->epsilonStar;
+    q.lambdaStar = p->lambdaStar;
+    q.omegaStar = p->omegaStar;
+    q.lowerBound = p->lowerBound;
+    q.upperBound = p->upperBound;
+    q.betaStar = p->betaStar;
+    q.betaBar = p->betaBar;
+    q.gammaStar = p->gammaStar;
+    q.epsilonDash = p->epsilonDash;
+    return q;
+}
+void from_param(const sddd::Param &q, sddd_param *p) {
+    p->maxIteration = q.maxIteration;
+    p->epsilonStar = q.epsilonStar;
+    p->lambdaStar = q.lambdaStar;
+    p->omegaStar = q.omegaStar;
+    p->lowerBound = q.lowerBound;
+    p->upperBound = q.upperBound;
+    p->betaStar = q.betaStar;
+    p->betaBar = q.betaBar;
+    p->gammaStar = q.gammaStar;
+    p->epsilonDash = q.epsilonDash;
+}
+inline dd_t D(sddd_dd v) { return dd_make(v.hi, v.lo); }
+inline sddd_dd S(dd_t v) { return sddd_dd{v.hi, v.lo}; }
+
+void fill_result(sddd_ctx *ctx, sddd_result *out) {
+    sddd::Solver &s = *ctx->solver;
+    std::memset(out, 0, sizeof(*out));
+    out->phase = (int)s.phase;
+    out->iterations = s.pIteration;
+    out->stop_reason = ctx->stop_reason;
+    dd_t mean = dd_div_d(dd_add(dd_abs(s.objValPrimal), dd_abs(s.objValDual)), 2.0);
+    dd_t gap = dd_abs(dd_sub(s.objValPrimal, s.objValDual));
+    out->mu = S(s.mu_current);
+    out->relative_gap = S(dd_lt_d(mean, 1.0) ? gap : dd_div(gap, mean));
+    out->gap = S(dd_mul_d(s.mu_current, (double)s.c.nDim));
+    out->objValPrimal = S(dd_neg(s.objValDual));
+    out->objValDual = S(dd_neg(s.objValPrimal));
+    out->pfeas_error = S(s.normDualMat);
+    out->dfeas_error = S(s.normPrimalVec);
+    out->main_loop_seconds = s.tm.mainLoop;
+    out->schur_seconds = s.tm.makebMat;
+    out->cholesky_seconds = s.tm.choleskybMat;
+}
+} // namespace
+
+extern "C" {
+
+const char *sddd_version(void) { return "sdpa-dd_b200 0.1 (sm_100a, dd on the FP64 pipe)"; }
+const char *sddd_last_error(const sddd_ctx *ctx) { return ctx ? ctx->err.c_str() : g_err.c_str(); }
+
+int sddd_create(int device, sddd_ctx **out) {
+    if (!out) return SDDD_ERR_ARG;
+    *out = nullptr;
+    return guarded(nullptr, [&] {
+        auto *ctx = new sddd_ctx();
+        ctx->c.reset(sddd::create_context(device));
+        *out = ctx;
+        return SDDD_OK;
+    });
+}
+
+int sddd_destroy(sddd_ctx *ctx) {
+    if (!ctx) return SDDD_OK;
+    ctx->solver.reset();
+    if (ctx->c) cudaSetDevice(ctx->c->device);
+    ctx->c.reset();
+    delete ctx;
+    return SDDD_OK;
+}
+
+int sddd_param_default(int type, sddd_param *out) {
+    if (!out || type < 0 || type > 2) return SDDD_ERR_ARG;
+    from_param(sddd::default_param(type), out);
+    return SDDD_OK;
+}
+
+int sddd_param_read(const char *path, sddd_param *out) {
+    if (!path || !out) return SDDD_ERR_ARG;
+    return guarded(nullptr, [&] {
+        from_param(sddd::read_param(path), out);
+        return SDDD_OK;
+    });
+}
+
+int sddd_read_problem(sddd_ctx *ctx, const char *path, int sparse, double kappa) {
+    if (!ctx || !path) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Problem p = sddd::read_problem(path, sparse != 0);
+        sddd::finalize_problem(p, kappa);
+        ctx->solver.reset();
+        sddd::upload_problem(*ctx->c, std::move(p));
+        return SDDD_OK;
+    });
+}
+
+int sddd_upload_problem(sddd_ctx *ctx, int m, int nblock, const int *block_struct, const sddd_dd *b, long nnz, const int *k, const int *blk,
+                        const int *i, const int *j, const sddd_dd *val, double kappa) {
+    if (!ctx || !block_struct || !b || (nnz > 0 && (!k || !blk || !i || !j || !val))) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Problem p = sddd::make_problem(m, nblock, block_struct, reinterpret_cast<const dd_t *>(b), nnz, k, blk, i, j,
+                                             reinterpret_cast<const dd_t *>(val));
+        sddd::finalize_problem(p, kappa);
+        ctx->solver.reset();
+        sddd::upload_problem(*ctx->c, std::move(p));
+        return SDDD_OK;
+    });
+}
+
+int sddd_dims(const sddd_ctx *cctx, int *m, int *nsdp, long *ndim, int *sizes, int cap) {
+    sddd_ctx *ctx = const_cast<sddd_ctx *>(cctx);
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        if (m) *m = c.m;
+        if (nsdp) *nsdp = c.nSDP;
+        if (ndim) *ndim = c.nDim;
+        if (sizes)
+            for (int l = 0; l < c.nSDP && l < cap; ++l) sizes[l] = c.sizes[l];
+        return SDDD_OK;
+    });
+}
+
+long sddd_space_len(const sddd_ctx *ctx) { return (ctx && ctx->c && ctx->c->have_problem) ? ctx->c->space_len : -1; }
+
+int sddd_formula(const sddd_ctx *cctx, int *out) {
+    sddd_ctx *ctx = const_cast<sddd_ctx *>(cctx);
+    if (!out) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        for (long q = 0; q < (long)c.m * c.nSDP; ++q) out[q] = -1;
+        for (int l = 0; l < c.nSDP; ++l)
+            for (size_t t = 0; t < c.prob.cons[l].size(); ++t) out[(long)c.prob.cons[l][t] * c.nSDP + l] = c.prob.formula[l][t];
+        return SDDD_OK;
+    });
+}
+
+int sddd_init_point(sddd_ctx *ctx, sddd_dd lambda) {
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        sddd::init_point(c, D(lambda));
+        CK(cudaStreamSynchronize(c.stream));
+        return SDDD_OK;
+    });
+}
+
+int sddd_set_point(sddd_ctx *ctx, const sddd_dd *X, const sddd_dd *y, const sddd_dd *Z) {
+    if (!X || !y || !Z) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        sddd::space_from_host(c, c.X, reinterpret_cast<const dd_t *>(X));
+        sddd::space_from_host(c, c.Z, reinterpret_cast<const dd_t *>(Z));
+        CK(cudaMemcpyAsync(c.y.p, y, sizeof(dd_t) * c.m, cudaMemcpyHostToDevice, c.stream));
+        return sddd::compute_inverse(c) ? SDDD_OK : 1;
+    });
+}
+
+int sddd_get_point(sddd_ctx *ctx, sddd_dd *X, sddd_dd *y, sddd_dd *Z) {
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        if (X) sddd::space_to_host(c, c.X, reinterpret_cast<dd_t *>(X));
+        if (Z) sddd::space_to_host(c, c.Z, reinterpret_cast<dd_t *>(Z));
+        if (y) {
+            CK(cudaMemcpyAsync(y, c.y.p, sizeof(dd_t) * c.m, cudaMemcpyDeviceToHost, c.stream));
+            CK(cudaStreamSynchronize(c.stream));
+        }
+        return SDDD_OK;
+    });
+}
+
+int sddd_compute_inverse(sddd_ctx *ctx) {
+    return guarded(ctx, [&] { return sddd::compute_inverse(need_problem(ctx)) ? SDDD_OK : 1; });
+}
+
+int sddd_newton_rhs(sddd_ctx *ctx, int corrector, sddd_dd beta_mu, int dual_infeasible) {
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        sddd::make_rhs(c, corrector != 0, D(beta_mu), dual_infeasible != 0);
+        CK(cudaStreamSynchronize(c.stream));
+        return SDDD_OK;
+    });
+}
+
+int sddd_schur_build(sddd_ctx *ctx) {
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        sddd::schur_build(c);
+        CK(cudaStreamSynchronize(c.stream));
+        return SDDD_OK;
+    });
+}
+
+int sddd_schur_factor(sddd_ctx *ctx) {
+    return guarded(ctx, [&] { return sddd::schur_factor(need_problem(ctx)); });
+}
+
+int sddd_solve_dy(sddd_ctx *ctx) {
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        sddd::solve_dy(c);
+        CK(cudaStreamSynchronize(c.stream));
+        return SDDD_OK;
+    });
+}
+
+int sddd_make_dz_dx(sddd_ctx *ctx, int dual_infeasible) {
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        sddd::make_dz_dx(c, dual_infeasible != 0);
+        CK(cudaStreamSynchronize(c.stream));
+        return SDDD_OK;
+    });
+}
+
+int sddd_min_eig(sddd_ctx *ctx, int which, sddd_dd *out) {
+    if (!out || which < 0 || which > 1) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        *out = S(which == 0 ? sddd::min_eig(c, c.invCholX, c.Dx) : sddd::min_eig(c, c.invCholZ, c.Dz));
+        return SDDD_OK;
+    });
+}
+
+int sddd_update(sddd_ctx *ctx, sddd_dd ap, sddd_dd ad) {
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        sddd::update_point(c, D(ap), D(ad));
+        return sddd::compute_inverse(c) ? SDDD_OK : 1;
+    });
+}
+
+int sddd_residuals(sddd_ctx *ctx, sddd_dd *np, sddd_dd *nd) {
+    return guarded(ctx, [&] {
+        dd_t a, b;
+        sddd::residuals(need_problem(ctx), a, b);
+        if (np) *np = S(a);
+        if (nd) *nd = S(b);
+        return SDDD_OK;
+    });
+}
+
+int sddd_inner(sddd_ctx *ctx, int which, sddd_dd *out) {
+    if (!out) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        dd_t v;
+        switch (which) {
+        case 0: v = sddd::inner_C(c, c.X); break;
+        case 1: v = sddd::inner_b(c, c.y.p); break;
+        case 2: v = sddd::inner_space(c, c.X, c.Z); break;
+        case 3: v = sddd::inner_C(c, c.Dx); break;
+        case 4: v = sddd::inner_b(c, c.Dy.p); break;
+        case 5: v = sddd::inner_space(c, c.X, c.Dz); break;
+        case 6: v = sddd::inner_space(c, c.Dx, c.Z); break;
+        case 7: v = sddd::inner_space(c, c.Dx, c.Dz); break;
+        default: throw sddd::Error(SDDD_ERR_ARG, "unknown inner product");
+        }
+        *out = S(v);
+        return SDDD_OK;
+    });
+}
+
+static void *target_of(sddd::Context &c, int what, long &len) {
+    const long L = c.space_len;
+    switch (what) {
+    case 0: len = L; return c.X.buf.p;
+    case 1: len = L; return c.Z.buf.p;
+    case 2: len = c.m; return c.y.p;
+    case 3: len = L; return c.invCholX.buf.p;
+    case 4: len = L; return c.invCholZ.buf.p;
+    case 5: len = L; return c.invZ.buf.p;
+    case 6: len = (long)c.m * c.m; return c.B.p;
+    case 7: len = c.m; return c.g.p;
+    case 8: len = L; return c.Dx.buf.p;
+    case 9: len = c.m; return c.Dy.p;
+    case 10: len = L; return c.Dz.buf.p;
+    case 11: len = L; return c.dualMat.buf.p;
+    case 12: len = c.m; return c.primalVec.p;
+    default: throw sddd::Error(SDDD_ERR_ARG, "unknown array selector");
+    }
+}
+
+long sddd_get(sddd_ctx *ctx, int what, sddd_dd *out) {
+    long result = 0;
+    int rc = guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        long len = 0;
+        void *p = target_of(c, what, len);
+        if (out) {
+            CK(cudaMemcpyAsync(out, p, sizeof(dd_t) * len, cudaMemcpyDeviceToHost, c.stream));
+            CK(cudaStreamSynchronize(c.stream));
+        }
+        result = len;
+        return SDDD_OK;
+    });
+    return rc == SDDD_OK ? result : rc;
+}
+
+int sddd_set(sddd_ctx *ctx, int what, const sddd_dd *in) {
+    if (!in) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        long len = 0;
+        void *p = target_of(c, what, len);
+        CK(cudaMemcpyAsync(p, in, sizeof(dd_t) * len, cudaMemcpyHostToDevice, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+        return SDDD_OK;
+    });
+}
+
+int sddd_solver_start(sddd_ctx *ctx, const sddd_param *param) {
+    if (!param) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        ctx->solver.reset(new sddd::Solver(c, to_param(param)));
+        ctx->solver->start();
+        ctx->stop_reason = 0;
+        return SDDD_OK;
+    });
+}
+
+int sddd_iterate(sddd_ctx *ctx) {
+    return guarded(ctx, [&] {
+        if (!ctx->solver) throw sddd::Error(SDDD_ERR_STATE, "solver not started");
+        int rc = ctx->solver->step(nullptr, nullptr);
+        if (rc != 0) ctx->stop_reason = rc;
+        return rc;
+    });
+}
+
+int sddd_solver_result(sddd_ctx *ctx, sddd_result *out) {
+    if (!out) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (!ctx->solver) throw sddd::Error(SDDD_ERR_STATE, "solver not started");
+        fill_result(ctx, out);
+        return SDDD_OK;
+    });
+}
+
+int sddd_solve(sddd_ctx *ctx, const sddd_param *param, const char *result_path, int print, sddd_result *out) {
+    if (!param) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        FILE *fo = nullptr;
+        if (result_path) {
+            fo = std::fopen(result_path, "w");
+            if (!fo) throw sddd::Error(SDDD_ERR_IO, std::string("Cannot open out file ") + result_path);
+        }
+        FILE *disp = print ? stdout : nullptr;
+        const auto t0 = std::chrono::steady_clock::now();
+        ctx->solver.reset(new sddd::Solver(c, to_param(param)));
+        sddd::Solver &s = *ctx->solver;
+        s.start();
+        if (fo) std::fprintf(fo, "   mu      thetaP  thetaD  objP      objD      alphaP  alphaD  beta \n");
+        if (disp) std::fprintf(disp, "   mu      thetaP  thetaD  objP      objD      alphaP  alphaD  beta \n");
+        int rc = 0;
+        while ((rc = s.step(disp, fo)) == 0) {
+        }
+        ctx->stop_reason = rc;
+        s.finish();
+        const double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        s.tm.total = total;
+        s.print_last_info(disp, fo, total, "");
+        if (fo) std::fclose(fo);
+        if (out) fill_result(ctx, out);
+        return SDDD_OK;
+    });
+}
+
+int sddd_Rgemm(sddd_ctx *ctx, char ta, char tb, long m, long n, long k, sddd_dd *A, long lda, sddd_dd *B, long ldb, sddd_dd *C, long ldc) {
+    return guarded(ctx, [&] {
+        if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
+        sddd::gemm(ctx->c->stream, ta, tb, sddd::GEMM_STORE, (int)m, (int)n, (int)k, reinterpret_cast<dd_t *>(A), lda, 0, reinterpret_cast<dd_t *>(B), ldb, 0,
+                   reinterpret_cast<dd_t *>(C), ldc, 0, 1, false);
+        CK(cudaStreamSynchronize(ctx->c->stream));
+        return SDDD_OK;
+    });
+}
+
+int sddd_Rpotrf(sddd_ctx *ctx, long n, sddd_dd *A, long lda) {
+    return guarded(ctx, [&] {
+        if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
+        sddd::Context &c = *ctx->c;
+        if (!c.info.p) c.info.alloc(4);
+        if (!c.rdiag.p) c.rdiag.alloc(256);
+        CK(cudaMemsetAsync(c.info.p, 0, sizeof(int), c.stream));
+        sddd::potrf(c.stream, reinterpret_cast<dd_t *>(A), lda, (int)n, c.info.p, c.rdiag.p);
+        int info = 0;
+        CK(cudaMemcpyAsync(&info, c.info.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+        return info;
+    });
+}
+
+int sddd_Rtrsv(sddd_ctx *ctx, char trans, long n, sddd_dd *L, long lda, sddd_dd *x) {
+    return guarded(ctx, [&] {
+        if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
+        sddd::trsv_lower(ctx->c->stream, trans, reinterpret_cast<dd_t *>(L), lda, (int)n, reinterpret_cast<dd_t *>(x));
+        CK(cudaStreamSynchronize(ctx->c->stream));
+        return SDDD_OK;
+    });
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------- CLI glue
+// (C++ linkage: used by cli.cpp only)
+void sddd_attach_problem(sddd_ctx *ctx, sddd::Problem &&p) {
+    ctx->solver.reset();
+    sddd::upload_problem(*ctx->c, std::move(p));
+}
+
+int sddd_solve_stream(sddd_ctx *ctx, const sddd_param *param, FILE *disp, FILE *fo, double fileRead, double *mainLoop) {
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        const auto t0 = std::chrono::steady_clock::now();
+        ctx->solver.reset(new sddd::Solver(c, to_param(param)));
+        sddd::Solver &s = *ctx->solver;
+        s.start();
+        s.tm.fileRead = fileRead;
+        if (fo) std::fprintf(fo, "   mu      thetaP  thetaD  objP      objD      alphaP  alphaD  beta \n");
+        if (disp) std::fprintf(disp, "   mu      thetaP  thetaD  objP      objD      alphaP  alphaD  beta \n");
+        int rc = 0;
+        const auto tl = std::chrono::steady_clock::now();
+        while ((rc = s.step(disp, fo)) == 0) {
+        }
+        const double ml = std::chrono::duration<double>(std::chrono::steady_clock::now() - tl).count();
+        ctx->stop_reason = rc;
+        s.finish();
+        s.tm.mainLoop = ml;
+        const double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() + fileRead;
+        s.tm.total = total;
+        s.print_last_info(disp, fo, total, "");
+        if (mainLoop) *mainLoop = ml;
+        return SDDD_OK;
+    });
+}

@@ -1,0 +1,9 @@
+// C++-linkage helpers shared by the C ABI and the command-line driver.
+#pragma once
+#include <cstdio>
+
+#include "../../include/sddd.h"
+#include "problem.h"
+
+void sddd_attach_problem(sddd_ctx *ctx, sddd::Problem &&p);
+int sddd_solve_stream(sddd_ctx *ctx, const sddd_param *param, FILE *disp, FILE *fo, double fileRead, double *mainLoop);

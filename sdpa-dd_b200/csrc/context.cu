@@ -1,0 +1,308 @@
+// Upload of the problem into its device layout and allocation of the
+// solver state (see context.h).
+#include "context.h"
+
+#include <algorithm>
+#include <numeric>
+
+namespace sddd {
+
+BlockView BlockDev::view() const {
+    BlockView v;
+    v.n = n;
+    v.nc = nc;
+    v.nsparse = nsparse;
+    v.all_dense = all_dense ? 1 : 0;
+    v.con = con.p;
+    v.formula = formula.p;
+    v.perm = perm.p;
+    v.coo_off = coo_off.p;
+    v.nnz = nnz.p;
+    v.dense_off = dense_off.p;
+    v.row = row.p;
+    v.col = col.p;
+    v.val = val.p;
+    v.dense = dense.p;
+    v.el_ptr = el_ptr.p;
+    v.el_con = el_con.p;
+    v.el_val = el_val.p;
+    v.c_present = c_present ? 1 : 0;
+    v.c_dense = c_dense ? 1 : 0;
+    v.c_nnz = (int)c_row.n;
+    v.c_dense_val = c_dense_val.p;
+    v.c_row = c_row.p;
+    v.c_col = c_col.p;
+    v.c_val = c_val.p;
+    v.c_el_ptr = c_el_ptr.p;
+    v.c_el_val = c_el_val.p;
+    return v;
+}
+
+Context::~Context() {
+    if (stream) cudaStreamDestroy(stream);
+}
+
+Context *create_context(int device) {
+    int count = 0;
+    CK(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) throw Error(ERR_ARG, "no such CUDA device");
+    CK(cudaSetDevice(device));
+    auto *c = new Context();
+    c->device = device;
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    return c;
+}
+
+static void build_block(Context &c, const Problem &P, int l, BlockDev &bd) {
+    const int n = P.sdpSize[l];
+    const auto &cl = P.cons[l];
+    const int nc = (int)cl.size();
+    bd.n = n;
+    bd.nc = nc;
+    std::vector<int> con(cl.begin(), cl.end()), formula(P.formula[l]), effect(nc), coo_off(nc, -1), nnz(nc);
+    std::vector<long> dense_off(nc, -1);
+    std::vector<int> row, col;
+    std::vector<dd_t> val, dense;
+    int ndense = 0;
+    for (int t = 0; t < nc; ++t) {
+        const BlockMat &M = P.A[cl[t]].at(l);
+        effect[t] = M.effect;
+        if (M.dense) {
+            dense_off[t] = (long)ndense * n * n;
+            dense.insert(dense.end(), M.val.begin(), M.val.end());
+            ++ndense;
+            nnz[t] = n * n;
+        } else {
+            coo_off[t] = (int)row.size();
+            nnz[t] = (int)M.row.size();
+            row.insert(row.end(), M.row.begin(), M.row.end());
+            col.insert(col.end(), M.col.begin(), M.col.end());
+            val.insert(val.end(), M.val.begin(), M.val.end());
+        }
+    }
+    std::vector<int> perm(nc);
+    std::iota(perm.begin(), perm.end(), 0);
+    std::sort(perm.begin(), perm.end(), [&](int a, int b) { return effect[a] != effect[b] ? effect[a] < effect[b] : con[a] < con[b]; });
+    bd.nsparse = nc - ndense;
+    for (int s = 0; s < nc; ++s) {
+        bool sp = coo_off[perm[s]] >= 0;
+        if (sp != (s < bd.nsparse)) throw Error(ERR_STATE, "internal: sparse matrices do not sort before dense ones");
+    }
+    bd.all_dense = (bd.nsparse == 0);
+    cudaStream_t st = c.stream;
+    bd.h_perm = perm;
+    bd.h_dense_off = dense_off;
+    bd.con.upload(con, st);
+    bd.formula.upload(formula, st);
+    bd.effect.upload(effect, st);
+    bd.perm.upload(perm, st);
+    bd.coo_off.upload(coo_off, st);
+    bd.nnz.upload(nnz, st);
+    bd.dense_off.upload(dense_off, st);
+    bd.row.upload(row, st);
+    bd.col.upload(col, st);
+    bd.val.upload(val, st);
+    bd.dense.upload(dense, st);
+    // element lists for sum_k y_k A_k (InputData::multi_plusToA order:
+    // k ascending, entries of one matrix in input order)
+    if (!bd.all_dense) {
+        const long ne = (long)n * n;
+        std::vector<int> cnt(ne + 1, 0);
+        for (int t = 0; t < nc; ++t) {
+            const BlockMat &M = P.A[cl[t]].at(l);
+            if (M.dense) {
+                for (long e = 0; e < ne; ++e) cnt[e + 1]++;
+            } else {
+                for (size_t q = 0; q < M.row.size(); ++q) {
+                    int i = M.row[q], j = M.col[q];
+                    cnt[i + (long)n * j + 1]++;
+                    if (i != j) cnt[j + (long)n * i + 1]++;
+                }
+            }
+        }
+        for (long e = 0; e < ne; ++e) cnt[e + 1] += cnt[e];
+        std::vector<int> el_con(cnt[ne]);
+        std::vector<dd_t> el_val(cnt[ne]);
+        std::vector<int> fillp(cnt.begin(), cnt.end() - 1);
+        for (int t = 0; t < nc; ++t) {
+            const BlockMat &M = P.A[cl[t]].at(l);
+            if (M.dense) {
+                for (long e = 0; e < ne; ++e) {
+                    el_con[fillp[e]] = cl[t];
+                    el_val[fillp[e]++] = M.val[e];
+                }
+            } else {
+                for (size_t q = 0; q < M.row.size(); ++q) {
+                    int i = M.row[q], j = M.col[q];
+                    long e1 = i + (long)n * j, e2 = j + (long)n * i;
+                    el_con[fillp[e1]] = cl[t];
+                    el_val[fillp[e1]++] = M.val[q];
+                    if (i != j) {
+                        el_con[fillp[e2]] = cl[t];
+                        el_val[fillp[e2]++] = M.val[q];
+                    }
+                }
+            }
+        }
+        bd.el_ptr.upload(cnt, st);
+        bd.el_con.upload(el_con, st);
+        bd.el_val.upload(el_val, st);
+    }
+    // C of this block
+    auto it = P.C.find(l);
+    bd.c_present = it != P.C.end();
+    if (bd.c_present) {
+        const BlockMat &M = it->second;
+        bd.c_dense = M.dense;
+        if (M.dense) {
+            bd.c_dense_val.upload(M.val, st);
+        } else {
+            bd.c_row.upload(M.row, st);
+            bd.c_col.upload(M.col, st);
+            bd.c_val.upload(M.val, st);
+            const long ne = (long)n * n;
+            std::vector<int> cnt(ne + 1, 0);
+            for (size_t q = 0; q < M.row.size(); ++q) {
+                int i = M.row[q], j = M.col[q];
+                cnt[i + (long)n * j + 1]++;
+                if (i != j) cnt[j + (long)n * i + 1]++;
+            }
+            for (long e = 0; e < ne; ++e) cnt[e + 1] += cnt[e];
+            std::vector<dd_t> ev(cnt[ne]);
+            std::vector<int> fillp(cnt.begin(), cnt.end() - 1);
+            for (size_t q = 0; q < M.row.size(); ++q) {
+                int i = M.row[q], j = M.col[q];
+                ev[fillp[i + (long)n * j]++] = M.val[q];
+                if (i != j) ev[fillp[j + (long)n * i]++] = M.val[q];
+            }
+            bd.c_el_ptr.upload(cnt, st);
+            bd.c_el_val.upload(ev, st);
+        }
+    }
+    // Schur owners
+    bd.h_ownFG.clear();
+    bd.h_ownF3.clear();
+    std::vector<int> fg_index(nc, -1);
+    for (int s = 0; s < nc; ++s) {
+        int f = formula[perm[s]];
+        if (f == F3) {
+            bd.h_ownF3.push_back(s);
+        } else {
+            fg_index[s] = (int)bd.h_ownFG.size();
+            bd.h_ownFG.push_back(s);
+        }
+    }
+    // row lists of the sparse FG owners
+    {
+        std::vector<int> rl_off(bd.h_ownFG.size(), -1), rl_ptr, rl_src;
+        std::vector<dd_t> rl_val;
+        for (size_t r = 0; r < bd.h_ownFG.size(); ++r) {
+            int t = perm[bd.h_ownFG[r]];
+            const BlockMat &M = P.A[cl[t]].at(l);
+            if (M.dense) continue;
+            rl_off[r] = (int)rl_ptr.size();
+            std::vector<std::vector<std::pair<int, dd_t>>> rows(n);
+            for (size_t q = 0; q < M.row.size(); ++q) {
+                if (dd_is_zero(M.val[q])) continue; // Raxpy returns when da == 0
+                int i = M.row[q], j = M.col[q];
+                rows[i].push_back({j, M.val[q]});
+                if (i != j) rows[j].push_back({i, M.val[q]});
+            }
+            int base = (int)rl_src.size();
+            for (int i = 0; i < n; ++i) {
+                rl_ptr.push_back(base);
+                for (auto &pr : rows[i]) {
+                    rl_src.push_back(pr.first);
+                    rl_val.push_back(pr.second);
+                    ++base;
+                }
+            }
+            rl_ptr.push_back(base);
+        }
+        bd.h_rl_off = rl_off;
+        bd.rl_off.upload(rl_off, st);
+        bd.rl_ptr.upload(rl_ptr, st);
+        bd.rl_src.upload(rl_src, st);
+        bd.rl_val.upload(rl_val, st);
+    }
+    bd.ownFG.upload(bd.h_ownFG, st);
+    bd.ownF3.upload(bd.h_ownF3, st);
+    bd.fg_index.upload(fg_index, st);
+    bd.fg_dense_contig = !bd.h_ownFG.empty();
+    for (size_t r = 0; r < bd.h_ownFG.size(); ++r) {
+        int t = perm[bd.h_ownFG[r]];
+        if (dense_off[t] < 0 || dense_off[t] != dense_off[perm[bd.h_ownFG[0]]] + (long)r * n * n) bd.fg_dense_contig = false;
+    }
+}
+
+void upload_problem(Context &c, Problem &&p) {
+    if (p.nLP > 0) throw Error(ERR_UNSUPPORTED, "LP blocks are not supported by the device path yet");
+    if (p.nSDP == 0) throw Error(ERR_ARG, "no SDP block");
+    CK(cudaSetDevice(c.device));
+    c.prob = std::move(p);
+    const Problem &P = c.prob;
+    c.m = P.m;
+    c.nSDP = P.nSDP;
+    c.nDim = P.nDim();
+    c.sizes = P.sdpSize;
+    c.off.assign(c.nSDP + 1, 0);
+    for (int l = 0; l < c.nSDP; ++l) c.off[l + 1] = c.off[l] + (long)c.sizes[l] * c.sizes[l];
+    c.space_len = c.off[c.nSDP];
+    c.blocks.clear();
+    for (int l = 0; l < c.nSDP; ++l) {
+        c.blocks.emplace_back(new BlockDev());
+        build_block(c, P, l, *c.blocks.back());
+    }
+    std::vector<BlockView> views;
+    for (auto &bd : c.blocks) views.push_back(bd->view());
+    c.views.upload(views, c.stream);
+    c.d_off.upload(c.off, c.stream);
+    c.d_sizes.upload(c.sizes, c.stream);
+    std::vector<int> ptr(c.m + 1, 0), bl, tt;
+    for (int k = 0; k < c.m; ++k) {
+        for (auto &kv : P.A[k]) {
+            int l = kv.first;
+            const auto &cl = P.cons[l];
+            int t = (int)(std::lower_bound(cl.begin(), cl.end(), k) - cl.begin());
+            bl.push_back(l);
+            tt.push_back(t);
+        }
+        ptr[k + 1] = (int)bl.size();
+    }
+    c.cb_ptr.upload(ptr, c.stream);
+    c.cb_block.upload(bl, c.stream);
+    c.cb_t.upload(tt, c.stream);
+    c.b.upload(P.b, c.stream);
+    alloc_state(c);
+    CK(cudaStreamSynchronize(c.stream));
+    c.have_problem = true;
+}
+
+void alloc_state(Context &c) {
+    const size_t sl = (size_t)c.space_len;
+    for (Space *s : {&c.X, &c.Z, &c.invCholX, &c.invCholZ, &c.invZ, &c.Dx, &c.Dz, &c.rzinv, &c.xrdzinv, &c.dualMat, &c.W1, &c.W2}) s->buf.alloc(sl);
+    c.y.alloc(c.m);
+    c.Dy.alloc(c.m);
+    c.g.alloc(c.m);
+    c.primalVec.alloc(c.m);
+    c.B.alloc((size_t)c.m * c.m);
+    size_t fg = 0;
+    for (auto &bd : c.blocks) fg = std::max(fg, (size_t)bd->nFG() * bd->n * bd->n);
+    c.Fbuf.alloc(std::max<size_t>(fg, 1));
+    c.Gbuf.alloc(std::max<size_t>(fg, 1));
+    c.scal.alloc(64);
+    c.red.alloc(4096);
+    c.info.alloc(4);
+    c.rdiag.alloc(256);
+    c.h_scal.assign(64, dd_zero());
+}
+
+void space_to_host(Context &c, const Space &s, dd_t *out) {
+    CK(cudaMemcpyAsync(out, s.buf.p, sizeof(dd_t) * c.space_len, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+}
+void space_from_host(Context &c, Space &s, const dd_t *in) {
+    CK(cudaMemcpyAsync(s.buf.p, in, sizeof(dd_t) * c.space_len, cudaMemcpyHostToDevice, c.stream));
+}
+
+} // namespace sddd

@@ -1,0 +1,163 @@
+// Device-resident solver state: the problem in its per-block layout and the
+// iterate, direction and work spaces of the reference's Solutions /
+// Newton / Residuals / WorkVariables (sdpa_dataset.h, sdpa_newton.h), all
+// in HBM for the whole solve.
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "problem.h"
+
+namespace sddd {
+
+// Device buffer owning cudaMalloc'd memory.
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        if (count == n && p) return;
+        release();
+        if (count == 0) return;
+        CK(cudaMalloc(&p, sizeof(T) * count));
+        n = count;
+    }
+    void upload(const std::vector<T> &v, cudaStream_t st) {
+        alloc(v.size());
+        if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st));
+    }
+};
+
+// Kernel-side view of one block's problem data (pointers into BlockDev).
+struct BlockView {
+    int n, nc, nsparse, all_dense;
+    const int *con, *formula, *perm, *coo_off, *nnz;
+    const long *dense_off;
+    const int *row, *col;
+    const dd_t *val, *dense;
+    const int *el_ptr, *el_con;
+    const dd_t *el_val;
+    int c_present, c_dense, c_nnz;
+    const dd_t *c_dense_val;
+    const int *c_row, *c_col;
+    const dd_t *c_val;
+    const int *c_el_ptr;
+    const dd_t *c_el_val;
+};
+
+// Per-SDP-block problem data on the device.
+//  t  : position of a constraint in the block's constraint list (ascending k)
+//  s  : position in the order sorted by (NonZeroEffect, k); a pair (i, j) is
+//       evaluated by its owner i when s(j) <= s(i) (sdpa_newton.cpp:1024)
+struct BlockDev {
+    int n = 0, nc = 0;
+    int nsparse = 0; // sparse matrices occupy sorted positions [0, nsparse)
+    DBuf<int> con;       // [t] constraint index
+    DBuf<int> formula;   // [t]
+    DBuf<int> effect;    // [t]
+    DBuf<int> perm;      // [s] -> t
+    DBuf<int> coo_off;   // [t] offset into row/col/val (sparse), -1 dense
+    DBuf<int> nnz;       // [t]
+    DBuf<long> dense_off; // [t] offset (elements) into dense (dense), -1 sparse
+    DBuf<int> row, col;
+    DBuf<dd_t> val;
+    DBuf<dd_t> dense;    // dense matrices, t order, n*n each
+    bool all_dense = false;
+    // sum_k y_k A_k by element (when not all dense): CSR over the n*n entries
+    DBuf<int> el_ptr, el_con;
+    DBuf<dd_t> el_val;
+    // C of this block: dense or element lists
+    bool c_present = false, c_dense = false;
+    DBuf<dd_t> c_dense_val;       // n*n
+    DBuf<int> c_row, c_col;       // COO in input order (for the inner product)
+    DBuf<dd_t> c_val;
+    DBuf<int> c_el_ptr;           // CSR over entries for C accumulation
+    DBuf<dd_t> c_el_val;
+    // Schur owner lists (sorted positions, ascending)
+    std::vector<int> h_ownFG, h_ownF3;
+    DBuf<int> ownFG, ownF3;
+    DBuf<int> fg_index;  // [s] -> index in ownFG or -1
+    bool fg_dense_contig = false; // all FG owners dense and contiguous in t
+    // F = A_i Z^-1 for sparse FG owners as row lists: row i of F is the
+    // ordered sum of v * (row src of Z^-1) (Raxpy row updates,
+    // sdpa_linear.cpp:832-893); per owner r: rl_off[r] into rl_ptr (n+1)
+    std::vector<int> h_rl_off;
+    DBuf<int> rl_off, rl_ptr, rl_src;
+    DBuf<dd_t> rl_val;
+    std::vector<int> h_perm;
+    std::vector<long> h_dense_off;
+    BlockView view() const;
+    int nFG() const { return (int)h_ownFG.size(); }
+    int nF3() const { return (int)h_ownF3.size(); }
+};
+
+// A block space (DenseLinearSpace restricted to SDP blocks): one device
+// buffer, block l at offset off[l], n_l x n_l column-major.
+struct Space {
+    DBuf<dd_t> buf;
+    dd_t *blk(const std::vector<long> &off, int l) const { return buf.p + off[l]; }
+};
+
+struct Context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    bool have_problem = false;
+    Problem prob;
+    int m = 0, nSDP = 0;
+    long nDim = 0;
+    std::vector<int> sizes;
+    std::vector<long> off; // block offsets within a space
+    long space_len = 0;
+    std::vector<std::unique_ptr<BlockDev>> blocks;
+    DBuf<BlockView> views; // [l]
+    DBuf<long> d_off;      // [l] block offsets within a space
+    DBuf<int> d_sizes;     // [l] block sizes
+    // per constraint: (block, t) pairs ascending by block
+    DBuf<int> cb_ptr, cb_block, cb_t;
+    DBuf<dd_t> b;
+    // iterate and derived (Solutions)
+    Space X, Z, invCholX, invCholZ, invZ;
+    DBuf<dd_t> y;
+    // Newton
+    Space Dx, Dz, rzinv, xrdzinv;
+    DBuf<dd_t> Dy, g;
+    DBuf<dd_t> B;   // m x m Schur matrix, factored in place
+    // Residuals
+    Space dualMat;
+    DBuf<dd_t> primalVec;
+    // WorkVariables
+    Space W1, W2;
+    // Schur work: F_i and G_i of FG owners (largest block)
+    DBuf<dd_t> Fbuf, Gbuf;
+    // small scratch
+    DBuf<dd_t> scal;   // device scalars
+    DBuf<dd_t> red;    // reduction scratch
+    DBuf<int> info;
+    DBuf<dd_t> rdiag;
+    std::vector<dd_t> h_scal;
+    ~Context();
+};
+
+Context *create_context(int device);
+void upload_problem(Context &c, Problem &&p);
+void alloc_state(Context &c);
+
+// Host<->device for spaces laid out as the C-ABI defines: SDP blocks
+// concatenated, each n_l x n_l column-major.
+void space_to_host(Context &c, const Space &s, dd_t *out);
+void space_from_host(Context &c, Space &s, const dd_t *in);
+
+} // namespace sddd

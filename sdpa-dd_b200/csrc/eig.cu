@@ -1,0 +1,369 @@
+// Step-length eigenvalue lambda_min(L D L^T) per SDP block
+// (Jal::getMinEigen, sdpa_jordan.cpp:55-88):
+//   n > 20   Lanczos of Lal::getMinEigen (sdpa_linear.cpp:27-122) - same
+//            start vector, recurrences (Rtrmv/Rgemv/Rdot orders), checkpoint
+//            and stopping rules; the k x k tridiagonal eigenproblem at a
+//            checkpoint is solved for its smallest eigenpair by warp-parallel
+//            Sturm multisection plus inverse iteration (the reference uses
+//            implicit QR, Rsteqr; both give the eigenvalue and the last
+//            eigenvector component to dd rounding).
+//   n <= 20  M = L (D L^T) by two Rgemm, then the smallest eigenvalue of the
+//            lower triangle of M (the reference's Rsyev "N","L") by
+//            Householder tridiagonalisation and bisection.
+// The whole Lanczos loop runs in one CTA per block: no host round trip per
+// step.
+#include "newton.h"
+
+#include "blas.h"
+#include "devops.cuh"
+
+namespace sddd {
+
+constexpr int LZ_THREADS = 512;
+constexpr int LZ_KMAX = 128;
+
+// QD double-vs-dd comparisons (dd_inline.h operator< / operator>)
+__device__ __forceinline__ bool d_lt_dd(double a, dd_t b) { return a < b.hi || (a == b.hi && b.lo > 0.0); }
+__device__ __forceinline__ bool d_gt_dd(double a, dd_t b) { return a > b.hi || (a == b.hi && b.lo < 0.0); }
+
+// Number of eigenvalues of tridiagonal (d, e2 = e^2) below x.
+__device__ int sturm_count(int k, const dd_t *d, const dd_t *e2, dd_t x) {
+    int c = 0;
+    dd_t q = dd_sub(d[0], x);
+    if (q.hi < 0.0) c++;
+    for (int i = 1; i < k; ++i) {
+        if (dd_is_zero(q)) q = dd_make(1e-300, 0.0);
+        q = dd_sub(dd_sub(d[i], x), dd_div(e2[i - 1], q));
+        if (q.hi < 0.0) c++;
+    }
+    return c;
+}
+
+// Smallest eigenvalue of the k x k tridiagonal (d, e) by multisection over
+// the 32 lanes of one warp; every lane returns the same value.
+__device__ dd_t tri_min_eigenvalue(int k, const dd_t *d, const dd_t *e, dd_t *e2) {
+    const int lane = threadIdx.x & 31;
+    dd_t lo = d[0], hi = d[0];
+    for (int i = 0; i < k; ++i) {
+        dd_t r = dd_zero();
+        if (i > 0) r = dd_add(r, dd_abs(e[i - 1]));
+        if (i + 1 < k) r = dd_add(r, dd_abs(e[i]));
+        dd_t a = dd_sub(d[i], r), b = dd_add(d[i], r);
+        if (dd_lt(a, lo)) lo = a;
+        if (dd_gt(b, hi)) hi = b;
+    }
+    if (lane == 0)
+        for (int i = 0; i + 1 < k; ++i) e2[i] = dd_mul(e[i], e[i]);
+    __syncwarp();
+    dd_t w = dd_sub(hi, lo);
+    lo = dd_sub(lo, dd_mul_d(w, 1e-10));
+    hi = dd_add(hi, dd_mul_d(w, 1e-10));
+    for (int round = 0; round < 40; ++round) {
+        dd_t width = dd_sub(hi, lo);
+        // x_lane = lo + width * (lane+1)/33
+        dd_t x = dd_add(lo, dd_div_d(dd_mul_d(width, (double)(lane + 1)), 33.0));
+        bool below = (dd_lt(lo, x) && dd_lt(x, hi)) ? sturm_count(k, d, e2, x) >= 1 : (lane == 31);
+        unsigned ball = __ballot_sync(0xffffffffu, below);
+        int first = ball ? __ffs(ball) - 1 : 31;
+        dd_t nlo, nhi;
+        // lanes agree on x values: recompute the bracket from lane indices
+        nhi = dd_add(lo, dd_div_d(dd_mul_d(width, (double)(first + 1)), 33.0));
+        nlo = first == 0 ? lo : dd_add(lo, dd_div_d(dd_mul_d(width, (double)first), 33.0));
+        if (!(dd_lt(nlo, nhi)) || (dd_eq(nlo, lo) && dd_eq(nhi, hi))) break;
+        lo = nlo;
+        hi = nhi;
+    }
+    return dd_mul_d(dd_add(lo, hi), 0.5);
+}
+
+// Last component of the unit eigenvector of (d, e) for eigenvalue l:
+// three steps of inverse iteration with a partially pivoted tridiagonal
+// solve (single thread; k <= LZ_KMAX).
+__device__ dd_t tri_last_component(int k, const dd_t *d, const dd_t *e, dd_t l, dd_t tnorm, dd_t *v, dd_t *dd_, dd_t *du, dd_t *du2, dd_t *dl, int *piv) {
+    for (int i = 0; i < k; ++i) v[i] = dd_from(1.0);
+    for (int it = 0; it < 3; ++it) {
+        for (int i = 0; i < k; ++i) {
+            dd_[i] = dd_sub(d[i], l);
+            du[i] = (i + 1 < k) ? e[i] : dd_zero();
+            dl[i] = (i + 1 < k) ? e[i] : dd_zero();
+            du2[i] = dd_zero();
+        }
+        for (int i = 0; i + 1 < k; ++i) {
+            if (!dd_lt(dd_abs(dd_[i]), dd_abs(dl[i]))) {
+                piv[i] = 0;
+                if (dd_is_zero(dd_[i])) dd_[i] = dd_mul_d(tnorm, 1e-32);
+                dd_t f = dd_div(dl[i], dd_[i]);
+                dl[i] = f;
+                dd_[i + 1] = dd_sub(dd_[i + 1], dd_mul(f, du[i]));
+            } else {
+                piv[i] = 1;
+                dd_t f = dd_div(dd_[i], dl[i]);
+                dd_[i] = dl[i];
+                dl[i] = f;
+                dd_t t = du[i];
+                du[i] = dd_[i + 1];
+                dd_[i + 1] = dd_sub(t, dd_mul(f, dd_[i + 1]));
+                if (i + 2 < k) {
+                    du2[i] = du[i + 1];
+                    du[i + 1] = dd_neg(dd_mul(f, du[i + 1]));
+                }
+            }
+        }
+        if (dd_is_zero(dd_[k - 1])) dd_[k - 1] = dd_mul_d(tnorm, 1e-32);
+        for (int i = 0; i + 1 < k; ++i) {
+            if (piv[i]) {
+                dd_t t = v[i];
+                v[i] = v[i + 1];
+                v[i + 1] = dd_sub(t, dd_mul(dl[i], v[i + 1]));
+            } else {
+                v[i + 1] = dd_sub(v[i + 1], dd_mul(dl[i], v[i]));
+            }
+        }
+        for (int i = k - 1; i >= 0; --i) {
+            dd_t t = v[i];
+            if (i + 1 < k) t = dd_sub(t, dd_mul(du[i], v[i + 1]));
+            if (i + 2 < k) t = dd_sub(t, dd_mul(du2[i], v[i + 2]));
+            v[i] = dd_div(t, dd_[i]);
+        }
+        dd_t nrm = dd_zero();
+        for (int i = 0; i < k; ++i) nrm = dd_acc(nrm, dd_mul(v[i], v[i]));
+        nrm = dd_sqrt(nrm);
+        for (int i = 0; i < k; ++i) v[i] = dd_div(v[i], nrm);
+    }
+    return v[k - 1];
+}
+
+struct LanczosShared {
+    dd_t diag[LZ_KMAX], off[LZ_KMAX], e2[LZ_KMAX];
+    dd_t v[LZ_KMAX], t0[LZ_KMAX], t1[LZ_KMAX], t2[LZ_KMAX], t3[LZ_KMAX];
+    int piv[LZ_KMAX];
+    dd_t alpha, beta, value, mn, mn_old, err, rr;
+    int go, check;
+};
+
+// One CTA per block: work holds 5 n-vectors (q, qold, r, w, tmp).
+__global__ void __launch_bounds__(LZ_THREADS) lanczos_kernel(const int *blk_ids, const int *sizes, const long *off, const dd_t *Lsp, const dd_t *Dsp,
+                                                             dd_t *work, long work_stride, dd_t *out) {
+    __shared__ LanczosShared S;
+    const int b = blk_ids[blockIdx.x];
+    const int n = sizes[b];
+    const dd_t *L = Lsp + off[b], *X = Dsp + off[b];
+    dd_t *q = work + blockIdx.x * work_stride, *qold = q + n, *r = qold + n, *w = r + n, *tmp = w + n;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int i = tid; i < n; i += nt) {
+        st_dd(q + i, dd_zero());
+        st_dd(r + i, dd_from(1.0));
+    }
+    if (tid == 0) {
+        S.mn = dd_from(1.0e+51);
+        S.mn_old = dd_from(1.0e+52);
+        S.err = dd_from(1.0e+10);
+        S.beta = dd_sqrt(dd_from((double)n));
+    }
+    __syncthreads();
+    const dd_t sqn10 = dd_add_d(dd_sqrt(dd_from((double)n)), 10.0);
+    const dd_t sqn9 = dd_sqrt(dd_add_d(dd_from((double)n), 9.0));
+    int k = 0, kk = 0;
+    while (true) {
+        if (tid == 0) {
+            const dd_t mn = S.mn, mo = S.mn_old;
+            bool c1 = dd_gt(dd_abs(dd_sub(mn, mo)), dd_add_d(dd_mul_d(dd_abs(mn), 1.0e-5), 1.0e-8));
+            bool c2 = dd_gt(dd_abs(dd_mul(S.err, S.beta)), dd_add_d(dd_mul_d(dd_abs(mn), 1.0e-2), 1.0e-4));
+            S.go = (k < n && k < LZ_KMAX && d_lt_dd((double)k, sqn10) && dd_gt_d(S.beta, 1.0e-16) && (c1 || c2)) ? 1 : 0;
+            S.value = dd_div(dd_from(1.0), S.beta);
+        }
+        __syncthreads();
+        if (!S.go) break;
+        const dd_t value = S.value;
+        // qold = q; q = r * value (Rcopy + Rscal)
+        for (int i = tid; i < n; i += nt) {
+            st_dd(qold + i, ld_dd(q + i));
+            dd_t qi = dd_mul(value, ld_dd(r + i));
+            st_dd(q + i, qi);
+        }
+        __syncthreads();
+        // w = L^T q (Rtrmv "Lower","Transpose")
+        for (int j = tid; j < n; j += nt) {
+            dd_t t = dd_mul(ld_dd(q + j), ld_dd(L + j + (long)n * j));
+            for (int i = j + 1; i < n; ++i) t = dd_acc(t, dd_mul(ld_dd(L + i + (long)n * j), ld_dd(q + i)));
+            st_dd(w + j, t);
+        }
+        __syncthreads();
+        // tmp = X w (Rgemv "N", alpha 1, beta 0)
+        for (int i = tid; i < n; i += nt) {
+            dd_t t = dd_zero();
+            for (int j = 0; j < n; ++j) t = dd_acc(t, dd_mul(dd_mul(dd_from(1.0), ld_dd(w + j)), ld_dd(X + i + (long)n * j)));
+            st_dd(tmp + i, t);
+        }
+        __syncthreads();
+        // w = L tmp (Rtrmv "Lower","NoTranspose": row i, j descending)
+        for (int i = tid; i < n; i += nt) {
+            dd_t t = dd_mul(ld_dd(tmp + i), ld_dd(L + i + (long)n * i));
+            for (int j = i - 1; j >= 0; --j) {
+                dd_t xj = ld_dd(tmp + j);
+                if (!dd_is_zero(xj)) t = dd_acc(t, dd_mul(xj, ld_dd(L + i + (long)n * j)));
+            }
+            st_dd(w + i, t);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            S.alpha = seq_dot(n, q, w);
+            S.diag[k] = S.alpha;
+        }
+        __syncthreads();
+        const dd_t ma = dd_neg(S.alpha), mb = dd_neg(S.beta);
+        // r = w - alpha q - beta qold (Rcopy, Raxpy, Raxpy)
+        for (int i = tid; i < n; i += nt) {
+            dd_t ri = ld_dd(w + i);
+            if (!dd_is_zero(ma)) ri = dd_acc(ri, dd_mul(ma, ld_dd(q + i)));
+            if (!dd_is_zero(mb)) ri = dd_acc(ri, dd_mul(mb, ld_dd(qold + i)));
+            st_dd(r + i, ri);
+        }
+        __syncthreads();
+        // checkpoint: kk >= sqrt(k) || k == n-1 || k > sqrt(n+9)
+        const dd_t sk = dd_sqrt(dd_from((double)k));
+        const bool check = dd_le_d(sk, (double)kk) || k == n - 1 || d_gt_dd((double)k, sqn9);
+        if (check) {
+            kk = 0;
+            if (tid < 32) {
+                dd_t lam = tri_min_eigenvalue(k + 1, S.diag, S.off, S.e2);
+                if (tid == 0) {
+                    dd_t lo = S.diag[0], hi = S.diag[0];
+                    for (int i = 0; i <= k; ++i) {
+                        lo = dd_min(lo, S.diag[i]);
+                        hi = dd_max(hi, S.diag[i]);
+                    }
+                    dd_t tnorm = dd_add(dd_add(dd_abs(lo), dd_abs(hi)), dd_from(1e-300));
+                    dd_t last = tri_last_component(k + 1, S.diag, S.off, lam, tnorm, S.v, S.t0, S.t1, S.t2, S.t3, S.piv);
+                    S.mn_old = S.mn;
+                    S.mn = lam;
+                    S.err = last;
+                }
+            }
+        }
+        if (tid == 0) S.rr = seq_dot(n, r, r);
+        __syncthreads();
+        if (tid == 0) {
+            S.beta = dd_sqrt(S.rr);
+            S.off[k] = S.beta;
+        }
+        __syncthreads();
+        ++k;
+        ++kk;
+    }
+    if (tid == 0) out[blockIdx.x] = dd_sub(S.mn, dd_abs(dd_mul(S.err, S.beta)));
+}
+
+// Smallest eigenvalue of the lower triangle of an n x n symmetric M
+// (n <= 32): Householder tridiagonalisation then bisection.  One thread.
+__global__ void small_min_eig_kernel(const int *blk_ids, const int *sizes, const long *off, const dd_t *Msp, dd_t *out) {
+    if (threadIdx.x != 0) return;
+    const int b = blk_ids[blockIdx.x];
+    const int n = sizes[b];
+    const dd_t *M = Msp + off[b];
+    dd_t A[32][32], d[32], e[32], e2[32], v[32], p[32];
+    for (int j = 0; j < n; ++j)
+        for (int i = j; i < n; ++i) {
+            A[i][j] = ld_dd(M + i + (long)n * j);
+            A[j][i] = A[i][j];
+        }
+    for (int k = 0; k + 2 < n; ++k) {
+        dd_t s = dd_zero();
+        for (int i = k + 1; i < n; ++i) s = dd_acc(s, dd_mul(A[i][k], A[i][k]));
+        dd_t nrm = dd_sqrt(s);
+        if (dd_is_zero(nrm)) continue;
+        dd_t alpha = A[k + 1][k].hi < 0.0 ? nrm : dd_neg(nrm);
+        for (int i = 0; i < n; ++i) v[i] = dd_zero();
+        v[k + 1] = dd_sub(A[k + 1][k], alpha);
+        for (int i = k + 2; i < n; ++i) v[i] = A[i][k];
+        dd_t vv = dd_zero();
+        for (int i = k + 1; i < n; ++i) vv = dd_acc(vv, dd_mul(v[i], v[i]));
+        if (dd_is_zero(vv)) continue;
+        dd_t tau = dd_div(dd_from(2.0), vv);
+        // p = tau A v ; K = tau/2 v^T p ; w = p - K v ; A -= v w^T + w v^T
+        for (int i = 0; i < n; ++i) {
+            dd_t t = dd_zero();
+            for (int j = k + 1; j < n; ++j) t = dd_acc(t, dd_mul(A[i][j], v[j]));
+            p[i] = dd_mul(tau, t);
+        }
+        dd_t vp = dd_zero();
+        for (int i = k + 1; i < n; ++i) vp = dd_acc(vp, dd_mul(v[i], p[i]));
+        dd_t K = dd_mul(dd_mul_d(tau, 0.5), vp);
+        for (int i = 0; i < n; ++i) p[i] = dd_sub(p[i], dd_mul(K, v[i]));
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) A[i][j] = dd_sub(dd_sub(A[i][j], dd_mul(v[i], p[j])), dd_mul(p[i], v[j]));
+    }
+    for (int i = 0; i < n; ++i) d[i] = A[i][i];
+    for (int i = 0; i + 1 < n; ++i) {
+        e[i] = A[i + 1][i];
+        e2[i] = dd_mul(e[i], e[i]);
+    }
+    dd_t lo = d[0], hi = d[0];
+    for (int i = 0; i < n; ++i) {
+        dd_t r = dd_zero();
+        if (i > 0) r = dd_add(r, dd_abs(e[i - 1]));
+        if (i + 1 < n) r = dd_add(r, dd_abs(e[i]));
+        lo = dd_min(lo, dd_sub(d[i], r));
+        hi = dd_max(hi, dd_add(d[i], r));
+    }
+    dd_t w = dd_sub(hi, lo);
+    lo = dd_sub(lo, dd_mul_d(w, 1e-10));
+    hi = dd_add(hi, dd_mul_d(w, 1e-10));
+    for (int it = 0; it < 400; ++it) {
+        dd_t mid = dd_mul_d(dd_add(lo, hi), 0.5);
+        if (!(dd_lt(lo, mid) && dd_lt(mid, hi))) break;
+        if (sturm_count(n, d, e2, mid) >= 1)
+            hi = mid;
+        else
+            lo = mid;
+    }
+    out[blockIdx.x] = dd_mul_d(dd_add(lo, hi), 0.5);
+}
+
+dd_t min_eig(Context &c, const Space &L, const Space &D) {
+    cudaStream_t st = c.stream;
+    std::vector<int> big, small;
+    for (int l = 0; l < c.nSDP; ++l) (c.sizes[l] > 20 ? big : small).push_back(l);
+    static_assert(LZ_KMAX >= 64, "Lanczos step bound");
+    std::vector<dd_t> vals;
+    if (!big.empty()) {
+        DBuf<int> ids;
+        ids.upload(big, st);
+        long maxn = 0;
+        for (int l : big) maxn = std::max<long>(maxn, c.sizes[l]);
+        DBuf<dd_t> work;
+        work.alloc(5 * maxn * big.size());
+        lanczos_kernel<<<(unsigned)big.size(), LZ_THREADS, 0, st>>>(ids.p, c.d_sizes.p, c.d_off.p, L.buf.p, D.buf.p, work.p, 5 * maxn, c.scal.p);
+        CK_LAUNCH();
+        std::vector<dd_t> h(big.size());
+        CK(cudaMemcpyAsync(h.data(), c.scal.p, sizeof(dd_t) * big.size(), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        vals.insert(vals.end(), h.begin(), h.end());
+    }
+    if (!small.empty()) {
+        // DLS2 = D L^T (Rgemm "N","T"); DLS1 = L DLS2 (Rgemm "N","N")
+        for (int l : small) {
+            const int n = c.sizes[l];
+            gemm(st, 'N', 'T', GEMM_STORE, n, n, n, D.blk(c.off, l), n, 0, L.blk(c.off, l), n, 0, c.W2.blk(c.off, l), n, 0, 1, false);
+            gemm(st, 'N', 'N', GEMM_STORE, n, n, n, L.blk(c.off, l), n, 0, c.W2.blk(c.off, l), n, 0, c.W1.blk(c.off, l), n, 0, 1, false);
+        }
+        DBuf<int> ids;
+        ids.upload(small, st);
+        small_min_eig_kernel<<<(unsigned)small.size(), 32, 0, st>>>(ids.p, c.d_sizes.p, c.d_off.p, c.W1.buf.p, c.scal.p + 32);
+        CK_LAUNCH();
+        std::vector<dd_t> h(small.size());
+        CK(cudaMemcpyAsync(h.data(), c.scal.p + 32, sizeof(dd_t) * small.size(), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        vals.insert(vals.end(), h.begin(), h.end());
+    }
+    // blocks in order: re-sort the values by block index
+    std::vector<dd_t> byblock(c.nSDP);
+    size_t bi = 0, si = 0;
+    for (int l = 0; l < c.nSDP; ++l) byblock[l] = (c.sizes[l] > 20) ? vals[bi++] : vals[big.size() + si++];
+    dd_t mn = dd_from(1.0e50);
+    for (int l = 0; l < c.nSDP; ++l)
+        if (dd_lt(byblock[l], mn)) mn = byblock[l];
+    return mn;
+}
+
+} // namespace sddd

@@ -1,0 +1,273 @@
+// The device side of the reference's Newton step, update and residuals
+// (sdpa_newton.cpp, sdpa_dataset.cpp), on block spaces resident in HBM.
+#include "newton.h"
+
+#include <algorithm>
+
+#include "blas.h"
+#include "devops.cuh"
+
+namespace sddd {
+
+static const dd_t ONE = {1.0, 0.0};
+static const dd_t MONE = {-1.0, 0.0};
+
+// --------------------------------------------------- per-constraint A_k . M
+// InputData::multi_InnerProductToA (sdpa_dataset.cpp:477-485) followed by
+// "v = v * (-1); v = v + w" (the callers' Lal::let pair, Rscal then Raxpy).
+__global__ void constraint_inner_kernel(int m, const BlockView *views, const long *off, const int *cb_ptr, const int *cb_block, const int *cb_t,
+                                        const dd_t *M, const dd_t *addv, dd_t *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    dd_t ret = dd_zero();
+    for (int p = cb_ptr[i]; p < cb_ptr[i + 1]; ++p) {
+        const int l = cb_block[p], t = cb_t[p];
+        const BlockView &v = views[l];
+        const dd_t *Ml = M + off[l];
+        dd_t tmp;
+        const long doff = v.dense_off[t];
+        if (doff >= 0) {
+            tmp = seq_dot((long)v.n * v.n, v.dense + doff, Ml);
+        } else {
+            const int o = v.coo_off[t];
+            tmp = sparse_dot_dense(v.n, v.nnz[t], v.row + o, v.col + o, v.val + o, Ml);
+        }
+        ret = dd_acc(ret, tmp);
+    }
+    st_dd(out + i, dd_acc(dd_mul(MONE, ret), dd_mul(ONE, ld_dd(addv + i))));
+}
+
+static void constraint_inner(Context &c, const Space &M, const dd_t *addv, dd_t *out) {
+    constraint_inner_kernel<<<ceil_div(c.m, 64), 64, 0, c.stream>>>(c.m, c.views.p, c.d_off.p, c.cb_ptr.p, c.cb_block.p, c.cb_t.p, M.buf.p, addv, out);
+    CK_LAUNCH();
+}
+
+// ------------------------------------------------------- sum_k y_k A_k
+// InputData::multi_plusToA (sdpa_dataset.cpp:488-493), entry by entry, then
+// mode 0 (compute_DzMat, sdpa_newton.cpp:1318-1327): r = -r (+ D)
+// mode 1 (Residuals::compute, sdpa_dataset.cpp:632-636): r = -r + C - Z
+__global__ void sum_yA_kernel(BlockView v, const dd_t *y, dd_t *out, int mode, const dd_t *D, const dd_t *Z) {
+    const long ne = (long)v.n * v.n;
+    const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    dd_t acc = dd_zero();
+    if (v.all_dense) {
+        for (int t = 0; t < v.nc; ++t) acc = dd_acc(acc, dd_mul(ld_dd(v.dense + v.dense_off[t] + e), ld_dd(y + v.con[t])));
+    } else {
+        for (int q = v.el_ptr[e]; q < v.el_ptr[e + 1]; ++q) acc = dd_acc(acc, dd_mul(v.el_val[q], ld_dd(y + v.el_con[q])));
+    }
+    dd_t r = dd_mul(MONE, acc);
+    if (mode == 0) {
+        if (D) r = dd_acc(r, dd_mul(ONE, ld_dd(D + e)));
+    } else {
+        if (v.c_present) {
+            if (v.c_dense) {
+                r = dd_acc(r, dd_mul(ONE, ld_dd(v.c_dense_val + e)));
+            } else {
+                for (int q = v.c_el_ptr[e]; q < v.c_el_ptr[e + 1]; ++q) r = dd_acc(r, dd_mul(v.c_el_val[q], ONE));
+            }
+        }
+        r = dd_acc(r, dd_mul(MONE, ld_dd(Z + e)));
+    }
+    st_dd(out + e, r);
+}
+
+static void sum_yA(Context &c, const dd_t *y, Space &out, int mode, const Space *D, const Space *Z) {
+    for (int l = 0; l < c.nSDP; ++l) {
+        const BlockDev &bd = *c.blocks[l];
+        const long ne = (long)bd.n * bd.n;
+        sum_yA_kernel<<<ceil_div(ne, 128), 128, 0, c.stream>>>(bd.view(), y, out.blk(c.off, l), mode, D ? D->blk(c.off, l) : nullptr,
+                                                               Z ? Z->blk(c.off, l) : nullptr);
+        CK_LAUNCH();
+    }
+}
+
+// ------------------------------------------------------------ init point
+__global__ void set_identity_kernel(dd_t *A, int n, dd_t v) {
+    long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (e >= (long)n * n) return;
+    st_dd(A + e, (e % n == e / n) ? v : dd_zero());
+}
+static void set_identity(Context &c, Space &s, dd_t v) {
+    for (int l = 0; l < c.nSDP; ++l) {
+        int n = c.sizes[l];
+        set_identity_kernel<<<ceil_div((long)n * n, 256), 256, 0, c.stream>>>(s.blk(c.off, l), n, v);
+        CK_LAUNCH();
+    }
+}
+
+void init_point(Context &c, dd_t lambda) {
+    set_identity(c, c.X, lambda);
+    set_identity(c, c.Z, lambda);
+    fill(c.stream, c.y.p, c.m, dd_zero());
+    dd_t ris = dd_div(ONE, dd_sqrt(lambda));
+    set_identity(c, c.invCholX, ris);
+    set_identity(c, c.invCholZ, ris);
+    set_identity(c, c.invZ, dd_div(ONE, lambda));
+}
+
+// ------------------------------------------------------- inverses of X, Z
+// Jal::getInvChol / getInvCholAndInv (sdpa_jordan.cpp:123-170): copy,
+// Rpotrf, zero the upper triangle, Rtrsm on the identity; for Z also
+// Z^-1 = L_Z^-T L_Z^-1 by Rtrmm.
+bool compute_inverse(Context &c) {
+    cudaStream_t st = c.stream;
+    CK(cudaMemsetAsync(c.info.p, 0, sizeof(int) * 2, st));
+    for (int l = 0; l < c.nSDP; ++l) {
+        const int n = c.sizes[l];
+        dd_t *w1 = c.W1.blk(c.off, l), *w2 = c.W2.blk(c.off, l);
+        CK(cudaMemcpyAsync(w1, c.X.blk(c.off, l), sizeof(dd_t) * n * n, cudaMemcpyDeviceToDevice, st));
+        potrf(st, w1, n, n, c.info.p, c.rdiag.p);
+        zero_upper(st, w1, n, n);
+        inv_lower(st, w1, n, n, c.invCholX.blk(c.off, l), n);
+        CK(cudaMemcpyAsync(w2, c.Z.blk(c.off, l), sizeof(dd_t) * n * n, cudaMemcpyDeviceToDevice, st));
+        potrf(st, w2, n, n, c.info.p + 1, c.rdiag.p + 128);
+        zero_upper(st, w2, n, n);
+        inv_lower(st, w2, n, n, c.invCholZ.blk(c.off, l), n);
+        trmm_lt(st, c.invCholZ.blk(c.off, l), n, n, c.invZ.blk(c.off, l), n);
+    }
+    int info[2];
+    CK(cudaMemcpyAsync(info, c.info.p, sizeof(info), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return info[0] == 0 && info[1] == 0;
+}
+
+// ------------------------------------------------------------ Newton step
+static void triple(Context &c, const Space &A, const Space &B, const Space &C, Space &out) {
+    // Jal::ns_jordan_triple_product: work = A B; out = work C (two Rgemm)
+    for (int l = 0; l < c.nSDP; ++l) {
+        const int n = c.sizes[l];
+        gemm(c.stream, 'N', 'N', GEMM_STORE, n, n, n, A.blk(c.off, l), n, 0, B.blk(c.off, l), n, 0, c.W2.blk(c.off, l), n, 0, 1, false);
+        gemm(c.stream, 'N', 'N', GEMM_STORE, n, n, n, c.W2.blk(c.off, l), n, 0, C.blk(c.off, l), n, 0, out.blk(c.off, l), n, 0, 1, false);
+    }
+}
+
+void make_rhs(Context &c, bool corrector, dd_t beta_mu, bool dual_infeasible) {
+    cudaStream_t st = c.stream;
+    const long L = c.space_len;
+    // r_zinv = beta*mu * Z^-1 - X  (compute_rMat, sdpa_newton.cpp:821-837)
+    copy_scal(st, c.invZ.buf.p, c.rzinv.buf.p, L, beta_mu);
+    axpy(st, c.rzinv.buf.p, c.X.buf.p, c.rzinv.buf.p, L, MONE);
+    if (corrector) {
+        triple(c, c.Dx, c.Dz, c.invZ, c.W1);
+        axpy(st, c.rzinv.buf.p, c.W1.buf.p, c.rzinv.buf.p, L, MONE);
+    }
+    // Make_gVec (sdpa_newton.cpp:839-893)
+    if (dual_infeasible) {
+        if (!corrector) triple(c, c.X, c.dualMat, c.invZ, c.xrdzinv);
+        axpy(st, c.rzinv.buf.p, c.xrdzinv.buf.p, c.W1.buf.p, L, MONE);
+    } else {
+        CK(cudaMemcpyAsync(c.W1.buf.p, c.rzinv.buf.p, sizeof(dd_t) * L, cudaMemcpyDeviceToDevice, st));
+    }
+    constraint_inner(c, c.W1, c.primalVec.p, c.g.p);
+}
+
+int schur_factor(Context &c) {
+    CK(cudaMemsetAsync(c.info.p, 0, sizeof(int), c.stream));
+    potrf(c.stream, c.B.p, c.m, c.m, c.info.p, c.rdiag.p);
+    int info = 0;
+    CK(cudaMemcpyAsync(&info, c.info.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return info;
+}
+
+void solve_dy(Context &c) {
+    CK(cudaMemcpyAsync(c.Dy.p, c.g.p, sizeof(dd_t) * c.m, cudaMemcpyDeviceToDevice, c.stream));
+    trsv_lower(c.stream, 'N', c.B.p, c.m, c.m, c.Dy.p);
+    trsv_lower(c.stream, 'T', c.B.p, c.m, c.m, c.Dy.p);
+}
+
+void make_dz_dx(Context &c, bool dual_infeasible) {
+    sum_yA(c, c.Dy.p, c.Dz, 0, dual_infeasible ? &c.dualMat : nullptr, nullptr);
+    triple(c, c.X, c.Dz, c.invZ, c.W1);
+    axpy(c.stream, c.rzinv.buf.p, c.W1.buf.p, c.Dx.buf.p, c.space_len, MONE);
+    for (int l = 0; l < c.nSDP; ++l) symmetrize(c.stream, c.Dx.blk(c.off, l), c.sizes[l]);
+}
+
+// ------------------------------------------------------------ inner products
+static dd_t fetch_sum(Context &c, int nslots) {
+    std::vector<dd_t> h(nslots);
+    CK(cudaMemcpyAsync(h.data(), c.scal.p, sizeof(dd_t) * nslots, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    dd_t r = dd_zero();
+    for (int s = 0; s < nslots; ++s) r = dd_acc(r, h[s]);
+    return r;
+}
+
+// Lal::getInnerProduct(DenseLinearSpace, DenseLinearSpace)
+// (sdpa_linear.cpp:1571-1611): Rdot per block, summed with "+=".
+dd_t inner_space(Context &c, const Space &a, const Space &b) {
+    for (int l = 0; l < c.nSDP; ++l) {
+        const long nn = (long)c.sizes[l] * c.sizes[l];
+        dot(c.stream, a.blk(c.off, l), 1, b.blk(c.off, l), 1, nn, c.scal.p + l, c.red.p + 256 * (l % 8));
+    }
+    return fetch_sum(c, c.nSDP);
+}
+
+__global__ void sparse_inner_kernel(int n, int nnz, const int *row, const int *col, const dd_t *val, const dd_t *D, dd_t *out) {
+    if (threadIdx.x == 0) st_dd(out, sparse_dot_dense(n, nnz, row, col, val, D));
+}
+
+// Lal::getInnerProduct(SparseLinearSpace C, DenseLinearSpace X)
+// (sdpa_linear.cpp:1616-1650) over C's nonzero SDP blocks.
+dd_t inner_C(Context &c, const Space &x) {
+    int slots = 0;
+    for (int l = 0; l < c.nSDP; ++l) {
+        const BlockDev &bd = *c.blocks[l];
+        if (!bd.c_present) continue;
+        const long nn = (long)bd.n * bd.n;
+        if (bd.c_dense) {
+            dot(c.stream, bd.c_dense_val.p, 1, x.blk(c.off, l), 1, nn, c.scal.p + slots, c.red.p + 256 * (slots % 8));
+        } else {
+            sparse_inner_kernel<<<1, 32, 0, c.stream>>>(bd.n, (int)bd.c_row.n, bd.c_row.p, bd.c_col.p, bd.c_val.p, x.blk(c.off, l), c.scal.p + slots);
+            CK_LAUNCH();
+        }
+        ++slots;
+    }
+    if (slots == 0) return dd_zero();
+    return fetch_sum(c, slots);
+}
+
+// Lal::getInnerProduct(Vector, Vector): Rdot over m.
+dd_t inner_b(Context &c, const dd_t *v) {
+    dot(c.stream, c.b.p, 1, v, 1, c.m, c.scal.p, c.red.p);
+    return fetch_sum(c, 1);
+}
+
+// ----------------------------------------------------------------- update
+void update_point(Context &c, dd_t alphaP, dd_t alphaD) {
+    axpy(c.stream, c.X.buf.p, c.Dx.buf.p, c.X.buf.p, c.space_len, alphaP);
+    axpy(c.stream, c.y.p, c.Dy.p, c.y.p, c.m, alphaD);
+    axpy(c.stream, c.Z.buf.p, c.Dz.buf.p, c.Z.buf.p, c.space_len, alphaD);
+}
+
+// -------------------------------------------------------------- residuals
+void residuals(Context &c, dd_t &normPrimal, dd_t &normDual) {
+    constraint_inner(c, c.X, c.b.p, c.primalVec.p);
+    sum_yA(c, c.y.p, c.dualMat, 1, nullptr, &c.Z);
+    maxabs(c.stream, c.primalVec.p, c.m, c.scal.p, c.red.p);
+    maxabs(c.stream, c.dualMat.buf.p, c.space_len, c.scal.p + 1, c.red.p + 512);
+    dd_t h[2];
+    CK(cudaMemcpyAsync(h, c.scal.p, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    normPrimal = h[0];
+    normDual = h[1];
+}
+
+__global__ void lambda_trace_kernel(const dd_t *S, const long *off, const int *sizes, int nb, double lambda, dd_t *out) {
+    if (threadIdx.x != 0) return;
+    dd_t r = dd_zero();
+    for (int b = 0; b < nb; ++b) {
+        const int n = sizes[b];
+        for (int i = 0; i < n; ++i) r = dd_acc(r, dd_mul_d(ld_dd(S + off[b] + i + (long)n * i), lambda));
+    }
+    st_dd(out, r);
+}
+
+dd_t lambda_trace(Context &c, const Space &s, double lambda) {
+    lambda_trace_kernel<<<1, 32, 0, c.stream>>>(s.buf.p, c.d_off.p, c.d_sizes.p, c.nSDP, lambda, c.scal.p);
+    CK_LAUNCH();
+    return fetch_sum(c, 1);
+}
+
+} // namespace sddd

@@ -1,0 +1,38 @@
+// Device pieces of one interior-point iteration, each matching one routine
+// of the reference (see newton.cu for the file:line of each).
+#pragma once
+#include "context.h"
+
+namespace sddd {
+
+// Solutions::initialize (sdpa_dataset.cpp:35-60): X = Z = lambda I, y = 0,
+// L_X^-1 = L_Z^-1 = I / sqrt(lambda), Z^-1 = I / lambda.
+void init_point(Context &c, dd_t lambda);
+// Solutions::computeInverse (sdpa_dataset.cpp:96-118); false when a
+// Cholesky factorisation of X or Z fails.
+bool compute_inverse(Context &c);
+// Newton::compute_rMat + Newton::Make_gVec (sdpa_newton.cpp:821-893).
+// dual_infeasible: phase is pFEAS or noINFO.
+void make_rhs(Context &c, bool corrector, dd_t beta_mu, bool dual_infeasible);
+// Newton::Make_bMat (schur.cu).
+void schur_build(Context &c);
+// Lal::choleskyFactorWithAdjust on B; returns LAPACK's info.
+int schur_factor(Context &c);
+// Dy = B^-1 g from the factor (Lal::solveSystems, sdpa_linear.cpp:639-651).
+void solve_dy(Context &c);
+// Newton::compute_DzMat + compute_DxMat (sdpa_newton.cpp:1318-1343).
+void make_dz_dx(Context &c, bool dual_infeasible);
+// Inner products of the reference's Lal::let(ret, '=', a, '.', b).
+dd_t inner_space(Context &c, const Space &a, const Space &b);
+dd_t inner_C(Context &c, const Space &x);
+dd_t inner_b(Context &c, const dd_t *v);
+// Solutions::update's three axpys (sdpa_dataset.cpp:120-131).
+void update_point(Context &c, dd_t alphaP, dd_t alphaD);
+// Residuals::compute (sdpa_dataset.cpp:625-645); returns the two max norms.
+void residuals(Context &c, dd_t &normPrimal, dd_t &normDual);
+// sum_l sum_i lambda * M_l(i,i) (SolveInfo::update, sdpa_parts.cpp:684-690)
+dd_t lambda_trace(Context &c, const Space &s, double lambda);
+// Jal::getMinEigen(L, D) over the SDP blocks (sdpa_jordan.cpp:55-88).
+dd_t min_eig(Context &c, const Space &L, const Space &D);
+
+} // namespace sddd

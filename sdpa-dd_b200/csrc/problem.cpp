@@ -1,0 +1,387 @@
+// SDPA input reading and problem set-up on the host (see problem.h).
+#include "problem.h"
+
+#include <algorithm>
+#include <cctype>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+#include "common.cuh"
+
+namespace sddd {
+
+long Problem::nDim() const {
+    long s = 0;
+    for (int n : sdpSize) s += n;
+    return s + nLP;
+}
+
+// ------------------------------------------------------------ decimal reader
+// QD's dd_real::read: digits accumulate as r = r*10 + d (operator*=(double),
+// operator+=(double)), then one multiplication by 10^e where the power is
+// QD's npwr (binary powering with operator*= and sqr, reciprocal for e < 0).
+static dd_t npwr(dd_t a, int n) {
+    if (n == 0) return dd_from(1.0);
+    dd_t r = a, s = dd_from(1.0);
+    int N = std::abs(n);
+    if (N > 1) {
+        while (N > 0) {
+            if (N % 2 == 1) s = dd_muleq(s, r);
+            N /= 2;
+            if (N > 0) r = dd_sqr(r);
+        }
+    } else {
+        s = r;
+    }
+    if (n < 0) return dd_div(dd_from(1.0), s);
+    return s;
+}
+
+int dd_read(const char *s, dd_t *out) {
+    const char *p = s;
+    int sign = 0, point = -1, nd = 0, e = 0;
+    bool done = false;
+    dd_t r = dd_zero();
+    while (*p == ' ') p++;
+    while (!done && *p != '\0') {
+        char ch = *p;
+        if (ch >= '0' && ch <= '9') {
+            r = dd_mul_d(r, 10.0);
+            r = dd_add_d(r, (double)(ch - '0'));
+            nd++;
+        } else {
+            switch (ch) {
+            case '.':
+                if (point >= 0) return -1;
+                point = nd;
+                break;
+            case '-':
+            case '+':
+                if (sign != 0 || nd > 0) return -1;
+                sign = (ch == '-') ? -1 : 1;
+                break;
+            case 'E':
+            case 'e':
+                if (std::sscanf(p + 1, "%d", &e) != 1) return -1;
+                done = true;
+                break;
+            default:
+                return -1;
+            }
+        }
+        p++;
+    }
+    if (point >= 0) e -= (nd - point);
+    if (e != 0) r = dd_muleq(r, npwr(dd_from(10.0), e));
+    *out = (sign == -1) ? dd_neg(r) : r;
+    return 0;
+}
+
+// QD's operator=(const char*) turns an unreadable string into NaN.
+static dd_t dd_parse(const std::string &tok) {
+    dd_t v;
+    if (dd_read(tok.c_str(), &v) != 0) {
+        double nan = std::nan("");
+        return dd_make(nan, nan);
+    }
+    return v;
+}
+
+// --------------------------------------------------------------- tokenizer
+// The fscanf patterns of sdpa_io.cpp over an in-memory copy of the file.
+namespace {
+struct Scanner {
+    const std::string &t;
+    size_t p = 0;
+    explicit Scanner(const std::string &s) : t(s) {}
+    static bool signdigit(char c) { return (c >= '0' && c <= '9') || c == '+' || c == '-'; }
+    static bool tokdelim(char c) { return c == ',' || c == '}' || c == ' ' || c == '\t' || c == '\n'; }
+    // "%*[^0-9+-]": a non-empty run of other characters (else no match)
+    bool skip_nonnum() {
+        size_t q = p;
+        while (q < t.size() && !signdigit(t[q])) ++q;
+        if (q == p || q >= t.size()) {
+            p = q;
+            return false;
+        }
+        p = q;
+        return true;
+    }
+    // "%d" after the skip
+    bool int_(int &v) {
+        while (p < t.size() && std::isspace((unsigned char)t[p])) ++p;
+        size_t q = p;
+        if (q < t.size() && (t[q] == '+' || t[q] == '-')) ++q;
+        size_t d = q;
+        while (q < t.size() && std::isdigit((unsigned char)t[q])) ++q;
+        if (q == d) return false;
+        v = std::atoi(t.substr(p, q - p).c_str());
+        p = q;
+        return true;
+    }
+    bool skip_int(int &v) { return skip_nonnum() && int_(v); }
+    // "%*[^0-9+-]%[^,} \t\n]"
+    bool skip_token(std::string &tok) {
+        if (!skip_nonnum()) return false;
+        size_t q = p;
+        while (q < t.size() && !tokdelim(t[q])) ++q;
+        if (q == p) return false;
+        tok = t.substr(p, q - p);
+        p = q;
+        return true;
+    }
+};
+} // namespace
+
+static void set_blocks(Problem &P, const std::vector<int> &bs) {
+    // pinpal, sdpa_main.cpp:114-131
+    P.nBlock = (int)bs.size();
+    P.blockStruct.resize(P.nBlock);
+    P.blockType.resize(P.nBlock);
+    P.blockNumber.resize(P.nBlock);
+    for (int i = 0; i < P.nBlock; ++i) {
+        int s = bs[i];
+        if (s >= 2) {
+            P.blockType[i] = 1;
+            P.blockNumber[i] = P.nSDP++;
+            P.blockStruct[i] = s;
+            P.sdpSize.push_back(s);
+        } else if (s < 0 || s == 1) {
+            P.blockType[i] = 3;
+            P.blockStruct[i] = s < 0 ? -s : s;
+            P.blockNumber[i] = P.nLP;
+            P.nLP += P.blockStruct[i];
+        } else {
+            throw Error(ERR_IO, "block struct");
+        }
+    }
+}
+
+// SparseLinearSpace::setElement_SDP (sdpa_struct.cpp:1217-1249)
+static void add_entry(Problem &P, int k, int l2, int i, int j, dd_t v) {
+    if (l2 < 0 || l2 >= P.nBlock) throw Error(ERR_IO, "block index out of range in input data");
+    if (P.blockType[l2] == 1) {
+        int l = P.blockNumber[l2];
+        int n = P.blockStruct[l2];
+        if (i < 0 || j < 0 || i >= n || j >= n) throw Error(ERR_IO, "out of range in input data");
+        BlockMat &M = (k == 0) ? P.C[l] : P.A[k - 1][l];
+        M.n = n;
+        M.row.push_back(i);
+        M.col.push_back(j);
+        M.val.push_back(k == 0 ? dd_neg(v) : v);
+        M.effect += (i == j) ? 1 : 2;
+    } else {
+        if (i != j) throw Error(ERR_IO, "LP part 3rd element != 4th element");
+        int idx = P.blockNumber[l2] + i;
+        if (k == 0)
+            P.lpC[idx] = dd_neg(v);
+        else
+            P.lpA[k - 1].push_back({idx, v});
+    }
+}
+
+Problem read_problem_text(const std::string &text, bool sparse) {
+    Problem P;
+    // IO::read(fpData, fpout, m, str), sdpa_io.cpp:428-438: comment lines
+    // start with '*' or '"'; the first other line holds m.
+    size_t pos = 0;
+    bool have_m = false;
+    while (pos < text.size()) {
+        size_t eol = text.find('\n', pos);
+        if (eol == std::string::npos) eol = text.size();
+        std::string line = text.substr(pos, eol - pos);
+        pos = std::min(eol + 1, text.size());
+        if (!line.empty() && (line[0] == '*' || line[0] == '"')) {
+            P.comments.push_back(line);
+            continue;
+        }
+        if (std::sscanf(line.c_str(), "%d", &P.m) != 1) throw Error(ERR_IO, "cannot read mDIM");
+        have_m = true;
+        break;
+    }
+    if (!have_m || P.m <= 0) throw Error(ERR_IO, "cannot read mDIM");
+    std::string rest = text.substr(pos);
+    Scanner sc(rest);
+    int nb = 0;
+    if (!sc.int_(nb) || nb <= 0) throw Error(ERR_IO, "cannot read nBLOCK");
+    std::vector<int> bs(nb);
+    for (int l = 0; l < nb; ++l)
+        if (!sc.skip_int(bs[l])) throw Error(ERR_IO, "cannot read bLOCKsTRUCT");
+    set_blocks(P, bs);
+    P.A.resize(P.m);
+    P.lpA.resize(P.m);
+    P.lpC.assign(P.nLP, dd_zero());
+    P.b.resize(P.m);
+    for (int k = 0; k < P.m; ++k) {
+        std::string tok;
+        if (!sc.skip_token(tok)) throw Error(ERR_IO, "cannot read the objective vector");
+        P.b[k] = dd_parse(tok);
+    }
+    if (sparse) {
+        // IO::setElement, sdpa_io.cpp:653-700
+        while (true) {
+            int k, l, i, j;
+            std::string tok;
+            if (!sc.skip_int(k)) break;
+            if (!sc.skip_int(l)) break;
+            if (!sc.skip_int(i)) break;
+            if (!sc.skip_int(j)) break;
+            if (!sc.skip_token(tok)) break;
+            double probe;
+            if (std::sscanf(tok.c_str(), "%lf", &probe) <= 0) break;
+            if (k < 0 || k > P.m) throw Error(ERR_IO, "constraint index out of range in input data");
+            add_entry(P, k, l - 1, i - 1, j - 1, dd_parse(tok));
+        }
+    } else {
+        // dense: every entry of every block, k = 0..m (sdpa_io.cpp:701-786)
+        for (int k = 0; k <= P.m; ++k)
+            for (int l2 = 0; l2 < P.nBlock; ++l2) {
+                int n = P.blockStruct[l2];
+                if (P.blockType[l2] == 1) {
+                    for (int i = 0; i < n; ++i)
+                        for (int j = 0; j < n; ++j) {
+                            std::string tok;
+                            if (!sc.skip_token(tok)) throw Error(ERR_IO, "dense data ended early");
+                            dd_t v = dd_parse(tok);
+                            if (i <= j && !dd_is_zero(v)) add_entry(P, k, l2, i, j, v);
+                        }
+                } else {
+                    for (int j = 0; j < n; ++j) {
+                        std::string tok;
+                        if (!sc.skip_token(tok)) throw Error(ERR_IO, "dense data ended early");
+                        dd_t v = dd_parse(tok);
+                        if (!dd_is_zero(v)) add_entry(P, k, l2, j, j, v);
+                    }
+                }
+            }
+    }
+    return P;
+}
+
+Problem read_problem(const std::string &path, bool sparse) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) throw Error(ERR_IO, "Cannot open data file " + path);
+    std::stringstream ss;
+    ss << f.rdbuf();
+    return read_problem_text(ss.str(), sparse);
+}
+
+Problem make_problem(int m, int nblock, const int *blockStruct, const dd_t *b, long nnz, const int *k, const int *blk, const int *i, const int *j,
+                     const dd_t *val) {
+    if (m <= 0 || nblock <= 0) throw Error(ERR_ARG, "m and nblock must be positive");
+    Problem P;
+    P.m = m;
+    set_blocks(P, std::vector<int>(blockStruct, blockStruct + nblock));
+    P.A.resize(m);
+    P.lpA.resize(m);
+    P.lpC.assign(P.nLP, dd_zero());
+    P.b.assign(b, b + m);
+    for (long e = 0; e < nnz; ++e) {
+        if (k[e] < 0 || k[e] > m) throw Error(ERR_ARG, "constraint index out of range");
+        add_entry(P, k[e], blk[e] - 1, i[e] - 1, j[e] - 1, val[e]);
+    }
+    return P;
+}
+
+// SparseMatrix::changeToDense (sdpa_struct.cpp:458-498): at least 20% of the
+// n*n entries stored -> dense, later entries overwrite earlier ones.
+static void change_to_dense(BlockMat &M) {
+    if (M.dense) return;
+    const int n = M.n;
+    if ((double)M.row.size() < (double)(n * n) * 0.20) return;
+    std::vector<dd_t> D((size_t)n * n, dd_zero());
+    for (size_t e = 0; e < M.row.size(); ++e) {
+        int i = M.row[e], j = M.col[e];
+        D[i + (size_t)n * j] = M.val[e];
+        D[j + (size_t)n * i] = M.val[e];
+    }
+    M.dense = true;
+    M.val.swap(D);
+    M.row.clear();
+    M.col.clear();
+    M.effect = n * n;
+}
+
+void finalize_problem(Problem &P, double kappa) {
+    for (auto &kv : P.C) change_to_dense(kv.second);
+    for (auto &Ak : P.A)
+        for (auto &kv : Ak) change_to_dense(kv.second);
+    P.cons.assign(P.nSDP, {});
+    for (int k = 0; k < P.m; ++k)
+        for (auto &kv : P.A[k]) P.cons[kv.first].push_back(k);
+    // formula choice with the reference's dd cost model
+    P.formula.assign(P.nSDP, {});
+    const dd_t K = dd_from(kappa);
+    for (int l = 0; l < P.nSDP; ++l) {
+        const auto &cl = P.cons[l];
+        const int nc = (int)cl.size();
+        std::vector<int> eff(nc);
+        for (int t = 0; t < nc; ++t) eff[t] = P.A[cl[t]].at(l).effect;
+        // "up": sum of the effects that sort below this one
+        std::vector<int> order(nc);
+        for (int t = 0; t < nc; ++t) order[t] = t;
+        std::sort(order.begin(), order.end(), [&](int a, int b) { return eff[a] != eff[b] ? eff[a] < eff[b] : cl[a] < cl[b]; });
+        std::vector<long> up(nc);
+        long run = 0;
+        for (int s = 0; s < nc; ++s) {
+            int t = order[s];
+            up[t] = eff[t] + run; // itself plus every (jnz < inz) or (jnz == inz and j < i)
+            run += eff[t];
+        }
+        P.formula[l].resize(nc);
+        const dd_t nn = dd_from((double)P.sdpSize[l]);
+        for (int t = 0; t < nc; ++t) {
+            const BlockMat &M = P.A[cl[t]].at(l);
+            dd_t inz = dd_from((double)eff[t]), u = dd_from((double)up[t]);
+            dd_t f1 = dd_add(dd_add(dd_mul(dd_mul(K, nn), inz), dd_mul(dd_mul(nn, nn), nn)), dd_mul(K, u));
+            dd_t f2 = dd_add(dd_mul(dd_mul(K, nn), inz), dd_mul(dd_mul(K, dd_add_d(nn, 1.0)), u));
+            dd_t f3 = dd_div(dd_mul(dd_mul(K, dd_add_d(dd_mul(dd_mul_d(K, 2.0), inz), 1.0)), u), K);
+            int f;
+            if (M.dense)
+                f = dd_lt(f1, f2) ? F1 : F2;
+            else if (dd_lt(f1, f2) && dd_lt(f1, f3))
+                f = F1;
+            else if (dd_lt(f2, f3))
+                f = F2;
+            else
+                f = F3;
+            P.formula[l][t] = f;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- params
+Param default_param(int type) {
+    Param p;
+    if (type == 2) { // PARAMETER_STABLE_BUT_SLOW
+        p.maxIteration = 1000;
+        p.lambdaStar = 1.0e+2;
+        p.betaStar = 0.2;
+        p.betaBar = 0.4;
+        p.gammaStar = 0.5;
+    } else if (type == 1) { // PARAMETER_UNSTABLE_BUT_FAST
+        p.maxIteration = 100;
+        p.lambdaStar = 1.0e+2;
+        p.betaStar = 0.01;
+        p.betaBar = 0.02;
+        p.gammaStar = 0.98;
+    }
+    return p;
+}
+
+Param read_param(const std::string &path) {
+    FILE *f = std::fopen(path.c_str(), "r");
+    if (!f) throw Error(ERR_IO, "Cannot open parameter file " + path);
+    Param p;
+    // fscanf("%d%*[^\n]") / fscanf("%lf%*[^\n]") per line
+    int rc = std::fscanf(f, "%d%*[^\n]", &p.maxIteration);
+    double *dst[] = {&p.epsilonStar, &p.lambdaStar, &p.omegaStar, &p.lowerBound, &p.upperBound, &p.betaStar, &p.betaBar, &p.gammaStar, &p.epsilonDash};
+    for (double *d : dst) rc = std::fscanf(f, "%lf%*[^\n]", d);
+    (void)rc;
+    std::fclose(f);
+    return p;
+}
+
+} // namespace sddd

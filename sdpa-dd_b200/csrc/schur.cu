@@ -1,0 +1,291 @@
+// Schur complement B_ij = (X A_i Z^-1) . A_j on the device
+// (Newton::Make_bMat / compute_bMat_dense_SDP, sdpa_newton.cpp:979-1068,
+// 1223-1244).
+//
+// Per SDP block the reference visits every pair (i, j) of constraints once,
+// from the owner i with (NonZeroEffect_i, i) >= (NonZeroEffect_j, j), using
+// the owner's formula:
+//   F1  G = X (A_i Z^-1) once per owner, value = A_j . G (calF1, :895)
+//   F2  F = A_i Z^-1, value from rows of X and columns of F per nonzero of
+//       A_j (calF2, :897-935); for dense A_j it switches to G = X F
+//   F3  double loop over the nonzeros of A_i and A_j (calF3, :937-977)
+// and adds value to B(i,j) and B(j,i) ("+=", blocks in order).
+//
+// On the B200 the pairs are regrouped by kind - never reordering the work on
+// one entry:
+//   - dense partners of F1/F2 owners: one TN GEMM  W^T V  over
+//     W = [vec G_owner] and V = [vec A_dense] (k = n^2, each entry a
+//     sequential dot), lower-triangle tiles only, scattered into B;
+//   - sparse partners of F1/F2 owners and all F3 pairs: one thread (F1, F3)
+//     or one warp (F2) per pair.
+#include "context.h"
+#include "blas.h"
+#include "newton.h"
+#include "devops.cuh"
+
+namespace sddd {
+
+static BlockView view(const BlockDev &b) { return b.view(); }
+
+// B(i,j) += v; B(j,i) += v for i != j (the reference's "+=").
+__device__ __forceinline__ void b_add(dd_t *B, int m, int i, int j, dd_t v) {
+    dd_t *p = B + i + (long)m * j;
+    st_dd(p, dd_acc(ld_dd(p), v));
+    if (i != j) {
+        dd_t *q = B + j + (long)m * i;
+        st_dd(q, dd_acc(ld_dd(q), v));
+    }
+}
+
+// ------------------------------------------------- F = A Z^-1, sparse A
+// Row i of F is the ordered sum over the row list of v * (row src of Z^-1).
+__global__ void f_sparse_kernel(int n, const int *ownFG, const int *rl_off, const int *rl_ptr, const int *rl_src, const dd_t *rl_val, const dd_t *invZ,
+                                dd_t *F, int nfg) {
+    const int r = blockIdx.y;
+    const int off = rl_off[r];
+    if (off < 0) return;
+    long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (e >= (long)n * n) return;
+    const int i = e % n, c = e / n;
+    const int *ptr = rl_ptr + off;
+    dd_t acc = dd_zero();
+    for (int q = ptr[i]; q < ptr[i + 1]; ++q) acc = dd_acc(acc, dd_mul(rl_val[q], ld_dd(invZ + rl_src[q] + (long)n * c)));
+    st_dd(F + (long)r * n * n + e, acc);
+}
+
+// --------------------------------------------- dense partners: W^T V GEMM
+// C(r, d) = sum_k G_r[k] A_d[k] (Rdot over n^2 entries, calF1 / calF2 dense
+// branch), for dense partner d with sorted position nsparse + d <= s(owner r).
+template <int BM, int BN, int BK, int TM, int TN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+    schur_dense_pairs_kernel(BlockView bv, const int *ownFG, int nfg, int ndense, const dd_t *__restrict__ W, const dd_t *__restrict__ V, dd_t *B, int m) {
+    constexpr int TX = BN / TN, TY = BM / TM, NT = TX * TY;
+    __shared__ double2 As[BK][BM + 1];
+    __shared__ double2 Bs[BK][BN + 1];
+    __shared__ int s_row[BM];
+    const long K = (long)bv.n * bv.n;
+    const int r0 = blockIdx.y * BM, d0 = blockIdx.x * BN;
+    const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+    for (int e = tid; e < BM; e += NT) s_row[e] = (r0 + e < nfg) ? ownFG[r0 + e] : -1;
+    __syncthreads();
+    const int rlast = min(r0 + BM, nfg) - 1;
+    if (bv.nsparse + d0 > s_row[rlast - r0]) return; // no valid pair in the tile
+    dd_t acc[TM][TN];
+#pragma unroll
+    for (int r = 0; r < TM; ++r)
+#pragma unroll
+        for (int c = 0; c < TN; ++c) acc[r][c] = dd_zero();
+    for (long k0 = 0; k0 < K; k0 += BK) {
+        for (int e = tid; e < BM * BK; e += NT) {
+            int kk = e % BK, ii = e / BK;
+            long gk = k0 + kk;
+            int gi = r0 + ii;
+            double2 v = make_double2(0.0, 0.0);
+            if (gi < nfg && gk < K) v = *reinterpret_cast<const double2 *>(W + gk + K * gi);
+            As[kk][ii] = v;
+        }
+        for (int e = tid; e < BN * BK; e += NT) {
+            int kk = e % BK, jj = e / BK;
+            long gk = k0 + kk;
+            int gj = d0 + jj;
+            double2 v = make_double2(0.0, 0.0);
+            if (gj < ndense && gk < K) v = *reinterpret_cast<const double2 *>(V + gk + K * gj);
+            Bs[kk][jj] = v;
+        }
+        __syncthreads();
+        const int kmax = (int)min((long)BK, K - k0);
+        for (int kk = 0; kk < kmax; ++kk) {
+            dd_t a[TM], b[TN];
+#pragma unroll
+            for (int r = 0; r < TM; ++r) {
+                double2 v = As[kk][ty + TY * r];
+                a[r] = dd_make(v.x, v.y);
+            }
+#pragma unroll
+            for (int c = 0; c < TN; ++c) {
+                double2 v = Bs[kk][tx + TX * c];
+                b[c] = dd_make(v.x, v.y);
+            }
+#pragma unroll
+            for (int r = 0; r < TM; ++r)
+#pragma unroll
+                for (int c = 0; c < TN; ++c) acc[r][c] = dd_acc(acc[r][c], dd_mul(b[c], a[r]));
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int r = 0; r < TM; ++r)
+#pragma unroll
+        for (int c = 0; c < TN; ++c) {
+            int gi = r0 + ty + TY * r, gd = d0 + tx + TX * c;
+            if (gi >= nfg || gd >= ndense) continue;
+            int s_own = s_row[ty + TY * r];
+            int s_par = bv.nsparse + gd;
+            if (s_par > s_own) continue;
+            int i = bv.con[bv.perm[s_own]], j = bv.con[bv.perm[s_par]];
+            // acc holds the Rdot partial (templ); Rdot returns 0 + templ
+            b_add(B, m, i, j, dd_acc(dd_zero(), acc[r][c]));
+        }
+}
+
+// ------------------------------------------ sparse partners of F1 owners
+// value = A_j . G (calF1 with a sparse A_j)
+__global__ void schur_f1_sparse_kernel(BlockView bv, const int *ownFG, int nfg, const dd_t *G, dd_t *B, int m) {
+    const int r = blockIdx.y;
+    const int s_own = ownFG[r];
+    const int t_own = bv.perm[s_own];
+    if (bv.formula[t_own] != F1) return;
+    const int sp = blockIdx.x * blockDim.x + threadIdx.x; // sparse partner position
+    if (sp >= bv.nsparse || sp > s_own) return;
+    const int tj = bv.perm[sp];
+    const int off = bv.coo_off[tj];
+    dd_t v = sparse_dot_dense(bv.n, bv.nnz[tj], bv.row + off, bv.col + off, bv.val + off, G + (long)r * bv.n * bv.n);
+    b_add(B, m, bv.con[t_own], bv.con[tj], v);
+}
+
+// ------------------------------------------ sparse partners of F2 owners
+// calF2 SPARSE (sdpa_newton.cpp:903-922): value = sum over nonzeros of A_j
+// of v * Rdot(n, X(alpha, :), F(:, beta)) (+ the swapped term).  One warp per
+// pair: lanes compute the dots, lane 0 accumulates in order.
+constexpr int F2_WARPS = 4;
+__global__ void schur_f2_sparse_kernel(BlockView bv, const int *ownFG, int nfg, const dd_t *X, const dd_t *F, dd_t *B, int m) {
+    __shared__ double2 dots[F2_WARPS][64];
+    const int r = blockIdx.y;
+    const int s_own = ownFG[r];
+    const int t_own = bv.perm[s_own];
+    if (bv.formula[t_own] != F2) return;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int sp = blockIdx.x * F2_WARPS + warp;
+    const bool active = sp < bv.nsparse && sp <= s_own;
+    const int n = bv.n;
+    const dd_t *Fr = F + (long)r * n * n;
+    dd_t ret = dd_zero();
+    int tj = 0;
+    if (active) {
+        tj = bv.perm[sp];
+        const int off = bv.coo_off[tj], nnz = bv.nnz[tj];
+        const int *row = bv.row + off, *col = bv.col + off;
+        const dd_t *val = bv.val + off;
+        for (int q0 = 0; q0 < nnz; q0 += 32) {
+            const int q = q0 + lane;
+            dd_t d1 = dd_zero(), d2 = dd_zero();
+            if (q < nnz) {
+                const int al = row[q], be = col[q];
+                for (int k = 0; k < n; ++k) d1 = dd_acc(d1, dd_mul(ld_dd(X + al + (long)n * k), ld_dd(Fr + k + (long)n * be)));
+                if (al != be)
+                    for (int k = 0; k < n; ++k) d2 = dd_acc(d2, dd_mul(ld_dd(X + be + (long)n * k), ld_dd(Fr + k + (long)n * al)));
+            }
+            dots[warp][2 * lane] = make_double2(d1.hi, d1.lo);
+            dots[warp][2 * lane + 1] = make_double2(d2.hi, d2.lo);
+            __syncwarp();
+            if (lane == 0) {
+                const int cnt = min(32, nnz - q0);
+                for (int u = 0; u < cnt; ++u) {
+                    dd_t v1 = val[q0 + u];
+                    ret = dd_acc(ret, dd_mul(v1, dd_make(dots[warp][2 * u].x, dots[warp][2 * u].y)));
+                    if (row[q0 + u] != col[q0 + u]) ret = dd_acc(ret, dd_mul(v1, dd_make(dots[warp][2 * u + 1].x, dots[warp][2 * u + 1].y)));
+                }
+            }
+            __syncwarp();
+        }
+        if (lane == 0) b_add(B, m, bv.con[t_own], bv.con[tj], ret);
+    }
+}
+
+// ----------------------------------------------------------- F3 owners
+// calF3 (sdpa_newton.cpp:937-977), one thread per pair.
+__global__ void schur_f3_kernel(BlockView bv, const int *ownF3, int nf3, const dd_t *X, const dd_t *invZ, dd_t *B, int m) {
+    const int r = blockIdx.y;
+    const int s_own = ownF3[r];
+    const int sp = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sp > s_own) return;
+    const int n = bv.n;
+    const int ti = bv.perm[s_own], tj = bv.perm[sp];
+    const int oi = bv.coo_off[ti], ni = bv.nnz[ti], oj = bv.coo_off[tj], nj = bv.nnz[tj];
+    const int *ri = bv.row + oi, *ci = bv.col + oi, *rj = bv.row + oj, *cj = bv.col + oj;
+    const dd_t *vi = bv.val + oi, *vj = bv.val + oj;
+    dd_t ret = dd_zero();
+    for (int q1 = 0; q1 < nj; ++q1) {
+        const int al = rj[q1], be = cj[q1];
+        const dd_t v1 = vj[q1];
+        dd_t sum = dd_zero();
+        for (int q2 = 0; q2 < ni; ++q2) {
+            const int ga = ri[q2], de = ci[q2];
+            const dd_t v2 = vi[q2];
+            sum = dd_acc(sum, dd_mul(dd_mul(v2, ld_dd(invZ + de + (long)n * be)), ld_dd(X + al + (long)n * ga)));
+            if (ga != de) sum = dd_acc(sum, dd_mul(dd_mul(v2, ld_dd(invZ + ga + (long)n * be)), ld_dd(X + al + (long)n * de)));
+        }
+        ret = dd_acc(ret, dd_mul(v1, sum));
+        if (al == be) continue;
+        sum = dd_zero();
+        for (int q2 = 0; q2 < ni; ++q2) {
+            const int ga = ri[q2], de = ci[q2];
+            const dd_t v2 = vi[q2];
+            sum = dd_acc(sum, dd_mul(dd_mul(v2, ld_dd(invZ + de + (long)n * al)), ld_dd(X + be + (long)n * ga)));
+            if (ga != de) sum = dd_acc(sum, dd_mul(dd_mul(v2, ld_dd(invZ + ga + (long)n * al)), ld_dd(X + be + (long)n * de)));
+        }
+        ret = dd_acc(ret, dd_mul(v1, sum));
+    }
+    b_add(B, m, bv.con[ti], bv.con[tj], ret);
+}
+
+void schur_build(Context &c) {
+    cudaStream_t st = c.stream;
+    const int m = c.m;
+    CK(cudaMemsetAsync(c.B.p, 0, sizeof(dd_t) * (size_t)m * m, st)); // bMat.setZero()
+    for (int l = 0; l < c.nSDP; ++l) {
+        BlockDev &bd = *c.blocks[l];
+        const BlockView bv = view(bd);
+        const int n = bd.n;
+        const long nn = (long)n * n;
+        const dd_t *X = c.X.blk(c.off, l), *Zi = c.invZ.blk(c.off, l);
+        const int nfg = bd.nFG();
+        if (nfg > 0) {
+            // F_r = A_r Z^-1
+            bool any_sparse = false;
+            for (int v : bd.h_rl_off) any_sparse |= v >= 0;
+            if (any_sparse) {
+                dim3 grid(ceil_div(nn, 128), nfg);
+                f_sparse_kernel<<<grid, 128, 0, st>>>(n, bd.ownFG.p, bd.rl_off.p, bd.rl_ptr.p, bd.rl_src.p, bd.rl_val.p, Zi, c.Fbuf.p, nfg);
+                CK_LAUNCH();
+            }
+            if (bd.fg_dense_contig) {
+                // the FG owners' dense matrices are consecutive in bd.dense
+                const long o0 = bd.h_dense_off[bd.h_perm[bd.h_ownFG[0]]];
+                gemm(st, 'N', 'N', GEMM_STORE, n, n, n, bd.dense.p + o0, n, nn, Zi, n, 0, c.Fbuf.p, n, nn, nfg, false);
+            } else {
+                for (int r = 0; r < nfg; ++r) {
+                    long o = bd.h_dense_off[bd.h_perm[bd.h_ownFG[r]]];
+                    if (o >= 0) gemm(st, 'N', 'N', GEMM_STORE, n, n, n, bd.dense.p + o, n, 0, Zi, n, 0, c.Fbuf.p + r * nn, n, 0, 1, false);
+                }
+            }
+            // G_r = X F_r
+            gemm(st, 'N', 'N', GEMM_STORE, n, n, n, X, n, 0, c.Fbuf.p, n, nn, c.Gbuf.p, n, nn, nfg, false);
+            // dense partners
+            const int ndense = bd.nc - bd.nsparse;
+            if (ndense > 0) {
+                constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4;
+                dim3 grid(ceil_div(ndense, BN), ceil_div(nfg, BM));
+                schur_dense_pairs_kernel<BM, BN, BK, TM, TN><<<grid, (BM / TM) * (BN / TN), 0, st>>>(bv, bd.ownFG.p, nfg, ndense, c.Gbuf.p, bd.dense.p, c.B.p, m);
+                CK_LAUNCH();
+            }
+            // sparse partners
+            if (bd.nsparse > 0) {
+                dim3 g1(ceil_div(bd.nsparse, 128), nfg);
+                schur_f1_sparse_kernel<<<g1, 128, 0, st>>>(bv, bd.ownFG.p, nfg, c.Gbuf.p, c.B.p, m);
+                CK_LAUNCH();
+                dim3 g2(ceil_div(bd.nsparse, F2_WARPS), nfg);
+                schur_f2_sparse_kernel<<<g2, 32 * F2_WARPS, 0, st>>>(bv, bd.ownFG.p, nfg, X, c.Fbuf.p, c.B.p, m);
+                CK_LAUNCH();
+            }
+        }
+        const int nf3 = bd.nF3();
+        if (nf3 > 0) {
+            dim3 grid(ceil_div(bd.nsparse, 128), nf3);
+            schur_f3_kernel<<<grid, 128, 0, st>>>(bv, bd.ownF3.p, nf3, X, Zi, c.B.p, m);
+            CK_LAUNCH();
+        }
+    }
+}
+
+} // namespace sddd

@@ -1,0 +1,225 @@
+"""GPU parity of the hot-path pieces, through the C ABI (libsddd.so).
+
+Every piece is given the same inputs as the reference and must return the
+reference's dd results bit for bit (+0 and -0 compared equal):
+  - the 18 dd operation shapes against QD;
+  - dd GEMM / Cholesky / triangular solves against the oracle;
+  - at real iterates of small seeded problems (dense F1, max-cut F3,
+    theta F2+F3, two-block F1): L_X^-1, L_Z^-1, Z^-1, the residuals, the
+    Schur matrix B, the predictor and corrector right-hand sides and the
+    directions Dx, Dy, Dz of the reference's own pinpal state.
+The step-length eigenvalue (Lanczos / small-block path) must agree within
+1e-26 relative: its tridiagonal eigensolver differs from the reference's QR
+by design.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import DD, RefSolver, as_dd, load_pkg, ptr
+from test_oracle import adversarial, rand_dd, same, spd
+
+pytestmark = pytest.mark.gpu
+
+SMALL = {
+    "dense": lambda P: P.dense_random(n=12, m=20, seed=10),
+    "maxcut": lambda P: P.maxcut(n=30, p=0.2, seed=11),
+    "theta": lambda P: P.theta(nv=24, p=0.5, seed=12),
+    "control": lambda P: P.control_like(sizes=(9, 6), m=25, seed=13),
+    "dense_big": lambda P: P.dense_random(n=50, m=40, seed=14),
+}
+
+
+@pytest.fixture(scope="module")
+def sddd():
+    return load_pkg()
+
+
+@pytest.fixture(scope="module")
+def problems(workdir):
+    P = load_pkg()
+    import importlib
+    prob = importlib.import_module("sdpa_dd_b200.problems")
+    out = {}
+    for name, make in SMALL.items():
+        path = workdir / f"gpu_{name}.dat-s"
+        path.write_text(make(prob))
+        out[name] = path
+    return out
+
+
+def to_dev(a):
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a).view(np.float64).copy()).cuda()
+    return t
+
+
+def from_dev(t, n):
+    out = t.cpu().numpy().view(DD)
+    return out[:n].copy()
+
+
+@pytest.mark.parametrize("op", list(range(18)))
+def test_device_dd_ops_match_qd(sddd, ref_lib, op):
+    import torch
+    L = sddd.lib()
+    rng = np.random.default_rng(300 + op)
+    n = 20000
+    a, b = adversarial(rng, n), adversarial(rng, n)
+    if op == 7:
+        a["hi"], a["lo"] = np.abs(a["hi"]), np.where(a["hi"] < 0, -a["lo"], a["lo"])
+    b["hi"][:500] = -a["hi"][:500]
+    da, db = to_dev(a), to_dev(b)
+    dout = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
+    assert L.sddd_dd_op(None, op, n, ctypes.c_void_p(da.data_ptr()), ctypes.c_void_p(db.data_ptr()), ctypes.c_void_p(dout.data_ptr())) == 0
+    got = from_dev(dout, n)
+    want = np.zeros(n, DD)
+    ref_lib.ref_dd_op(op, ctypes.c_long(n), ptr(a), ptr(b), ptr(want))
+    assert same(got, want)
+
+
+@pytest.fixture(scope="module")
+def ctx(sddd):
+    c = sddd.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (7, 5, 3), (65, 33, 17), (130, 70, 129)])
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T")])
+def test_device_gemm_matches_rgemm(ctx, oracle_lib, m, n, k, ta, tb):
+    import torch
+    rng = np.random.default_rng(m + 7 * n + 13 * k)
+    ra, ca = (m, k) if ta == "N" else (k, m)
+    rb, cb = (k, n) if tb == "N" else (n, k)
+    A, B = rand_dd(rng, ra * ca), rand_dd(rng, rb * cb)
+    dA, dB = to_dev(A), to_dev(B)
+    dC = torch.zeros(2 * m * n, dtype=torch.float64, device="cuda")
+    ctx.L.sddd_Rgemm(ctx.h, ta.encode(), tb.encode(), m, n, k, ctypes.c_void_p(dA.data_ptr()), ra, ctypes.c_void_p(dB.data_ptr()), rb,
+                     ctypes.c_void_p(dC.data_ptr()), m)
+    want = np.zeros(m * n, DD)
+    oracle_lib.o_gemm(ctypes.c_char(ta.encode()), ctypes.c_char(tb.encode()), ctypes.c_long(m), ctypes.c_long(n), ctypes.c_long(k), ptr(A),
+                      ctypes.c_long(ra), ptr(B), ctypes.c_long(rb), ptr(want), ctypes.c_long(m))
+    assert same(from_dev(dC, m * n), want)
+
+
+@pytest.mark.parametrize("n", [1, 5, 63, 64, 65, 130, 257])
+def test_device_potrf_trsv_match(ctx, oracle_lib, n):
+    rng = np.random.default_rng(500 + n)
+    A = spd(rng, n)
+    A["lo"] = rng.standard_normal(n * n) * 1e-18
+    want = A.copy()
+    info = oracle_lib.o_potrf(ctypes.c_long(n), ptr(want), ctypes.c_long(n))
+    assert info == 0
+    dA = to_dev(A)
+    got_info = ctx.L.sddd_Rpotrf(ctx.h, n, ctypes.c_void_p(dA.data_ptr()), n)
+    assert got_info == 0
+    got = from_dev(dA, n * n).reshape(n, n)
+    w = want.reshape(n, n)
+    for j in range(n):  # lower triangle of column j = row j of the (col-major) view
+        assert same(got[j, j:], w[j, j:]), j
+    # solves with the factor
+    b = rand_dd(rng, n)
+    for tr in ("N", "T"):
+        x = b.copy()
+        oracle_lib.o_trsv(ctypes.c_char(tr.encode()), ctypes.c_long(n), ptr(want), ctypes.c_long(n), ptr(x))
+        dx = to_dev(b)
+        ctx.L.sddd_Rtrsv(ctx.h, tr.encode(), n, ctypes.c_void_p(dA.data_ptr()), n, ctypes.c_void_p(dx.data_ptr()))
+        assert same(from_dev(dx, n), x), tr
+
+
+def test_device_potrf_reports_failing_column(ctx, oracle_lib):
+    rng = np.random.default_rng(9)
+    n = 150
+    A = spd(rng, n)
+    A["hi"][97 * n + 97] = -3.0
+    want = A.copy()
+    i1 = oracle_lib.o_potrf(ctypes.c_long(n), ptr(want), ctypes.c_long(n))
+    dA = to_dev(A)
+    i2 = ctx.L.sddd_Rpotrf(ctx.h, n, ctypes.c_void_p(dA.data_ptr()), n)
+    assert i1 == i2 == 98
+
+
+def _dd_scalar_eq(a, b):
+    return (a[0] == b["hi"] or (a[0] == 0 and b["hi"] == 0)) and (a[1] == b["lo"] or (a[1] == 0 and b["lo"] == 0))
+
+
+@pytest.mark.parametrize("name", list(SMALL))
+@pytest.mark.parametrize("k", [0, 2, 6])
+def test_newton_pieces_match_reference(sddd, ctx, ref_lib, problems, name, k):
+    """Set the GPU to the reference's point before its pass k+1 and replay
+    that pass piece by piece."""
+    path = problems[name]
+    ref = RefSolver(ref_lib, path)
+    try:
+        ctx.read_problem(path, sparse=True, kappa=1.2)
+        assert ctx.m == ref.m and ctx.sizes == ref.blocks
+        f_ref = ref.formula()
+        assert np.array_equal(ctx.formula(), f_ref)
+        for _ in range(k):
+            assert ref.step() == 0
+        X, y, Z = ref.get(0), ref.get(2), ref.get(1)
+        assert ctx.set_point(X, y, Z) == 0
+        for w_ref, w_gpu in ((3, "invCholX"), (4, "invCholZ"), (5, "invZ")):
+            assert same(ctx.get(w_gpu), ref.get(w_ref)), w_gpu
+        ctx.dd_scalar("sddd_residuals", ctypes.byref(sddd.SdddDD()))  # residuals of the point
+        assert same(ctx.get("dualMat"), ref.get(15))
+        assert same(ctx.get("primalVec"), ref.get(16))
+        # one reference pass
+        rc = ref.step()
+        assert rc == 0
+        phase = ref_lib.ref_phase_at_step(ref.h)
+        dinf = int(phase in (0, 1))  # noINFO or pFEAS
+        beta_p, mu = ref.scalar(16), ref.scalar(19)
+        # predictor: RHS, Schur, Cholesky, Dy, Dz, Dx
+        import importlib
+        bm = _ddmul(ref_lib, beta_p, mu)
+        ctx.call("sddd_newton_rhs", 0, sddd.SdddDD(*bm), dinf)
+        assert same(ctx.get("g"), ref.get(8)), "g (predictor)"
+        ctx.call("sddd_schur_build")
+        B = ctx.get("B")
+        assert same(B, _ref_B_at(ref_lib, path, X, y, Z, k)), "Schur matrix"
+        assert ctx.call("sddd_schur_factor") == 0
+        ctx.call("sddd_solve_dy")
+        assert same(ctx.get("Dy"), ref.get(13)), "Dy (predictor)"
+        ctx.call("sddd_make_dz_dx", dinf)
+        assert same(ctx.get("Dz"), ref.get(14)), "Dz (predictor)"
+        assert same(ctx.get("Dx"), ref.get(12)), "Dx (predictor)"
+        # corrector
+        beta_c = ref.scalar(6)
+        bm = _ddmul(ref_lib, beta_c, mu)
+        ctx.call("sddd_newton_rhs", 1, sddd.SdddDD(*bm), dinf)
+        ctx.call("sddd_solve_dy")
+        assert same(ctx.get("Dy"), ref.get(10)), "Dy (corrector)"
+        ctx.call("sddd_make_dz_dx", dinf)
+        assert same(ctx.get("Dz"), ref.get(11)), "Dz (corrector)"
+        assert same(ctx.get("Dx"), ref.get(9)), "Dx (corrector)"
+        # step-length eigenvalues
+        for which, sel in ((0, 17), (1, 18)):
+            got = ctx.dd_scalar("sddd_min_eig", which)
+            want = ref.scalar(sel)
+            diff = (got[0] - want["hi"]) + (got[1] - want["lo"])
+            assert abs(diff) <= 1e-26 * abs(want["hi"]), (which, got, want)
+    finally:
+        ref.close()
+
+
+def _ddmul(ref_lib, a, b):
+    aa = np.array([a], DD)
+    bb = np.array([b], DD)
+    out = np.zeros(1, DD)
+    ref_lib.ref_dd_op(4, ctypes.c_long(1), ptr(aa), ptr(bb), ptr(out))
+    return float(out["hi"][0]), float(out["lo"][0])
+
+
+def _ref_B_at(ref_lib, path, X, y, Z, k):
+    """The reference's B at point (X, y, Z): a second reference solver set to
+    that point (Make_bMat reads X and Z^-1 only)."""
+    r = RefSolver(ref_lib, path)
+    try:
+        if k > 0:
+            assert ref_lib.ref_set_point(r.h, ptr(X), ptr(y), ptr(Z)) == 0
+        return r.schur()
+    finally:
+        r.close()
