@@ -1,0 +1,352 @@
+#!/usr/bin/env python
+"""Newton-iteration throughput of the dd interior-point method on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the Lovasz-theta-shaped SDP with 200 vertices and edge probability
+0.5 (seed 2: 9979 edges, m = 9980 constraints, one 200 x 200 block), the
+configuration the headline target is quoted on.  A step is one full pass of
+the reference's main loop (sdpa_main.cpp:294-376): predictor and corrector
+Newton directions (Schur build, dd Cholesky of the 9980 x 9980 Schur matrix,
+solves), step lengths, update and residuals.  The metric is dd-GFLOP/s of
+the Schur build plus the Cholesky of B (the algorithmic counts of
+sddd_work: m^3/3 for the Cholesky), over the whole step time.
+
+One JSON line on rank 0.  Multi-GPU runs are replicas (the single solve
+does not shard): every rank solves its own copy, value sums the ranks' work
+over the slowest rank's time.  --impl reference times the reference build
+(oracle/_ref) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import datetime
+import importlib.util
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+WORKLOAD = dict(name="theta", nv=200, p=0.5, seed=2)
+CPU_SAMPLE = dict(name="theta", nv=120, p=0.5, seed=2)  # m = 3571
+EPS = 1e-25
+
+
+def load_pkg():
+    if "sdpa_dd_b200" in sys.modules:
+        return sys.modules["sdpa_dd_b200"]
+    pkg = ROOT / "sdpa-dd_b200"
+    spec = importlib.util.spec_from_file_location("sdpa_dd_b200", pkg / "__init__.py", submodule_search_locations=[str(pkg)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["sdpa_dd_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def problems():
+    load_pkg()
+    import importlib
+    return importlib.import_module("sdpa_dd_b200.problems")
+
+
+def write_workload(w, directory):
+    P = problems()
+    path = pathlib.Path(directory) / f"{w['name']}_nv{w['nv']}_s{w['seed']}.dat-s"
+    if not path.exists():
+        tmp = str(path) + f".tmp{os.getpid()}"
+        with open(tmp, "w") as f:
+            f.write(P.theta(nv=w["nv"], p=w["p"], seed=w["seed"]))
+        os.replace(tmp, path)
+    param = P.write_param(str(pathlib.Path(directory) / "bench.param"), eps=EPS)
+    return path, param
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def trailing_flops(m, nb=64):
+    """dd-flops of the Cholesky trailing updates (lower triangle incl. the
+    diagonal, nb multiply-subtracts = 2 nb dd-flops per entry) and their
+    launch count."""
+    fl, launches = 0.0, 0
+    for c0 in range(0, m, nb):
+        M = m - c0 - min(nb, m - c0)
+        if M > 0:
+            fl += float(nb) * M * (M + 1)
+            launches += 1
+    return fl, launches
+
+
+def cpu_reference(sample, warmup, steps, threads):
+    """Time the reference build (oracle/_ref/sdpa_ref_iter) on the host."""
+    P = problems()
+    exe = ROOT / "oracle" / "_ref" / "sdpa_ref_iter"
+    if not exe.exists():
+        return None, "oracle/_ref/sdpa_ref_iter is not built"
+    with tempfile.TemporaryDirectory() as td:
+        data, param = write_workload(sample, td)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        r = subprocess.run([str(exe), str(data), param, str(warmup), str(steps)], capture_output=True, text=True, env=env)
+        if r.returncode != 0:
+            return None, f"reference run failed: {r.stderr.strip()[-200:]}"
+        out = json.loads(r.stdout.strip().splitlines()[-1])
+    e = P.theta_edges(sample["nv"], sample["p"], sample["seed"])
+    schur, chol = P.theta_work(sample["nv"], e)
+    secs = out["pass_s"]
+    return {"value": (schur + chol) * len(secs) / sum(secs) / 1e9, "m": out["m"], "threads": out["threads"], "pass_s": secs}, None
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(world, v):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    res, why = cpu_reference(CPU_SAMPLE, args.warmup, args.steps, threads)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return 0
+    sample = f"theta-shaped SDP nv={CPU_SAMPLE['nv']} p={CPU_SAMPLE['p']} (m={res['m']}), {args.steps} main-loop passes after {args.warmup}"
+    line = {
+        "impl": "reference",
+        "metric": "Schur+Chol dd-GFLOP/s per Newton iteration",
+        "value": res["value"], "unit": "dd-GFLOP/s", "higher_is_better": True,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(res["pass_s"]) / len(res["pass_s"]),
+        "scaling": "weak", "vs_baseline": None, "dtype": "dd (f64 pairs)", "data": "synthetic",
+        "config": {"workload": sample, "reference": "oracle/_ref (SDPA-DD 7.1.3 built from its sources, OpenMP)"},
+        "cpu_baseline": {"value": res["value"], "unit": "dd-GFLOP/s", "cores": res["threads"], "kind": "reference", "sample": sample},
+        "e2e": {"value": res["value"], "unit": "dd-GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args, world, rank, local):
+    sddd = load_pkg()
+    L = sddd.lib()
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    workdir = pathlib.Path(tempfile.gettempdir()) / f"sddd_bench_{os.getuid()}_{local}"
+    workdir.mkdir(exist_ok=True)
+    data, param_path = write_workload(WORKLOAD, workdir)
+    ctx = sddd.Context(local)
+    t0 = time.perf_counter()
+    ctx.read_problem(data, sparse=True, kappa=1.2)
+    setup_s = time.perf_counter() - t0
+    schur = ctypes.c_double()
+    chol = ctypes.c_double()
+    L.sddd_work(ctx.h, ctypes.byref(schur), ctypes.byref(chol))
+    step_flops = schur.value + chol.value
+    par = sddd.param(param_path)
+    stream = torch.cuda.ExternalStream(L.sddd_stream(ctx.h))
+
+    def restart():
+        ctx.call("sddd_solver_start", ctypes.byref(par))
+
+    def iterate():
+        rc = L.sddd_iterate(ctx.h)
+        if rc < 0:
+            raise RuntimeError(L.sddd_last_error(ctx.h).decode())
+        if rc != 0:  # converged or stopped: continue from a fresh start
+            restart()
+            rc = L.sddd_iterate(ctx.h)
+            if rc != 0:
+                raise RuntimeError(f"solver stopped at its first iteration (rc={rc})")
+
+    restart()
+    for _ in range(args.warmup):
+        iterate()
+    # ---- device-resident timed region
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = Clocks(local) if rank == 0 else None
+    L.sddd_profile(ctx.h, 1)
+    L.sddd_profile_reset(ctx.h)
+    launches0 = L.sddd_launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        iterate()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = L.sddd_launch_count() - launches0
+    barrier(world)
+    clk = clocks.stop() if clocks else None
+    ms = ev0.elapsed_time(ev1)
+    kern = {}
+    for name in ("potrf_trailing_update", "potrf_panel", "potrf_diag", "trsv", "schur_build", "min_eig"):
+        t = ctypes.c_double()
+        n = ctypes.c_long()
+        L.sddd_profile_read(ctx.h, name.encode(), ctypes.byref(t), ctypes.byref(n))
+        kern[name] = (t.value, n.value)
+    L.sddd_profile(ctx.h, 0)
+    ms_max = allmax(world, ms)
+    value = world * args.steps * step_flops / (ms_max * 1e-3) / 1e9
+    # ---- end to end through the C ABI with host buffers
+    n_space = L.sddd_space_len(ctx.h)
+    m = ctx.m
+    X = torch.empty(2 * n_space, dtype=torch.float64).pin_memory()
+    Z = torch.empty(2 * n_space, dtype=torch.float64).pin_memory()
+    y = torch.empty(2 * m, dtype=torch.float64).pin_memory()
+    px, pz, py = (ctypes.c_void_p(t.data_ptr()) for t in (X, Z, y))
+    L.sddd_get_point(ctx.h, px, py, pz)
+    h2d = d2h = 16 * (2 * n_space + m)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        if L.sddd_set_point(ctx.h, px, py, pz) != 0:
+            raise RuntimeError("set_point failed")
+        iterate()
+        L.sddd_get_point(ctx.h, px, py, pz)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = allmax(world, e0.elapsed_time(e1))
+    e2e_value = world * args.steps * step_flops / (e2e_ms * 1e-3) / 1e9
+    # ---- roofline of the dominant kernel (Cholesky trailing update)
+    tr_fl, tr_launch = trailing_flops(m)
+    t_ms, t_n = kern["potrf_trailing_update"]
+    fp64 = ctypes.c_double()
+    L.sddd_fp64_peak(ctx.h, ctypes.byref(fp64))
+    # one dd multiply-subtract = 2 dd-flops = 20 FP64 instructions
+    peak_dd = fp64.value / 20.0
+    achieved = (tr_fl * args.steps) / (t_ms * 1e-3) / 1e9 if t_ms > 0 else None
+    traffic = None
+    tfile = ROOT / "profiles" / "potrf_trailing_update_traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get("bytes_per_launch")
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        res, why = cpu_reference(CPU_SAMPLE, 0, 1, threads)
+        if res is not None:
+            cpu = {"value": res["value"], "unit": "dd-GFLOP/s", "cores": res["threads"], "kind": "reference",
+                   "sample": f"oracle/_ref on a theta-shaped SDP nv={CPU_SAMPLE['nv']} (m={res['m']}), one main-loop pass, {res['threads']} OpenMP threads"}
+        else:
+            cpu = {"value": None, "unit": "dd-GFLOP/s", "cores": 0, "kind": "reference", "sample": why}
+    if rank == 0:
+        line = {
+            "metric": "Schur+Chol dd-GFLOP/s per Newton iteration",
+            "value": value, "unit": "dd-GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "dd (f64 pairs)", "data": "synthetic",
+            "config": {"workload": f"theta-shaped SDP nv={WORKLOAD['nv']} p={WORKLOAD['p']} seed={WORKLOAD['seed']}", "m": m,
+                       "block": ctx.sizes, "step": "one main-loop pass (predictor+corrector Newton, step length, update)",
+                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (Schur matrix %.2f GB)" % (16.0 * m * m / 1e9),
+                       "eps": EPS, "setup_s": setup_s},
+            "step_ddflops": {"schur": schur.value, "cholesky": chol.value},
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()},
+            "roofline": {"kernel": "potrf_trailing_update", "bound": "fp64", "achieved": achieved, "peak": peak_dd, "unit": "dd-GFLOP/s",
+                         "frac": (achieved / peak_dd) if achieved and peak_dd else None, "traffic": traffic,
+                         "peak_source": f"measured FP64 FMA rate {fp64.value:.0f} GFLOP/s / 20 FP64 instructions per dd multiply-add pair (2 dd-flops)",
+                         "launches_per_step": t_n / args.steps, "ddflops_per_launch": tr_fl / tr_launch},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "dd-GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = dist_init(args)
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank)
+        return run_ours(args, world, rank, local)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

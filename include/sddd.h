@@ -127,6 +127,23 @@ int sddd_solver_result(sddd_ctx *ctx, sddd_result *out);
 /* The reference's command line (sdpa_main.cpp:493-672). */
 int sddd_cli_main(int argc, char **argv);
 
+/* -- measurement -- */
+/* Kernels this library has launched in this process so far. */
+unsigned long long sddd_launch_count(void);
+/* The context's CUDA stream (cudaStream_t) for event timing by callers. */
+void *sddd_stream(sddd_ctx *ctx);
+/* Per-kernel CUDA-event timing inside the library, for the calling thread:
+ * enable/disable, read (collects: synchronises the stream) and reset.
+ * Names: potrf_trailing_update, potrf_diag, potrf_panel, trsv,
+ * schur_build, min_eig. */
+int sddd_profile(sddd_ctx *ctx, int enable);
+int sddd_profile_read(sddd_ctx *ctx, const char *name, double *ms, long *launches);
+int sddd_profile_reset(sddd_ctx *ctx);
+/* Algorithmic dd-flops of one Schur build and of one Cholesky of B. */
+int sddd_work(const sddd_ctx *ctx, double *schur_ddflops, double *chol_ddflops);
+/* Measured FP64 fused multiply-add throughput of the current device (GFLOP/s). */
+int sddd_fp64_peak(sddd_ctx *ctx, double *gflops);
+
 /* -- dd kernels on device memory (MPLAPACK-like; pointers are device
  *    pointers to column-major sddd_dd) -- */
 int sddd_Rgemm(sddd_ctx *ctx, char transa, char transb, long m, long n, long k, sddd_dd *A, long lda, sddd_dd *B, long ldb, sddd_dd *C, long ldc);

@@ -90,6 +90,13 @@ def lib() -> ctypes.CDLL:
         "sddd_host_dd_op": (ci, [ci, cl, vp, vp, vp]),
         "sddd_host_dd_read": (ci, [ctypes.c_char_p, vp]),
         "sddd_host_dd_to_string": (ci, [SdddDD, ci, ctypes.c_char_p, ci]),
+        "sddd_stream": (vp, [vp]),
+        "sddd_launch_count": (ctypes.c_ulonglong, []),
+        "sddd_profile": (ci, [vp, ci]),
+        "sddd_profile_read": (ci, [vp, ctypes.c_char_p, ctypes.POINTER(cd), ctypes.POINTER(cl)]),
+        "sddd_profile_reset": (ci, [vp]),
+        "sddd_work": (ci, [vp, ctypes.POINTER(cd), ctypes.POINTER(cd)]),
+        "sddd_fp64_peak": (ci, [vp, ctypes.POINTER(cd)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -18,6 +18,7 @@
 // The blocking below (tiles, panels) is the B200 schedule; it never
 // reorders the operations that land on one entry.
 #include "blas.h"
+#include "prof.h"
 
 #include <algorithm>
 
@@ -269,15 +270,22 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
     }
     for (int c0 = 0; c0 < n; c0 += nbmax) {
         const int nb = std::min(nbmax, n - c0);
-        potrf_diag_kernel<<<1, 256, sizeof(double2) * nb * nb, st>>>(A, lda, nb, c0, info_dev, rdiag_dev);
-        CK_LAUNCH();
+        {
+            PROF_SCOPE("potrf_diag", st);
+            potrf_diag_kernel<<<1, 256, sizeof(double2) * nb * nb, st>>>(A, lda, nb, c0, info_dev, rdiag_dev);
+            CK_LAUNCH();
+        }
         const int below = n - c0 - nb;
         if (below <= 0) break;
-        potrf_panel_kernel<<<ceil_div(below, PANEL_ROWS), 256, sizeof(double2) * (nb * nb + PANEL_ROWS * nb + nb), st>>>(A, lda, n, nb, c0, info_dev,
-                                                                                                                      rdiag_dev);
-        CK_LAUNCH();
+        {
+            PROF_SCOPE("potrf_panel", st);
+            potrf_panel_kernel<<<ceil_div(below, PANEL_ROWS), 256, sizeof(double2) * (nb * nb + PANEL_ROWS * nb + nb), st>>>(A, lda, n, nb, c0, info_dev,
+                                                                                                                          rdiag_dev);
+            CK_LAUNCH();
+        }
         dd_t *panel = A + (c0 + nb) + lda * (long)c0;
         dd_t *trail = A + (c0 + nb) + lda * (long)(c0 + nb);
+        PROF_SCOPE("potrf_trailing_update", st);
         gemm(st, 'N', 'T', GEMM_SUB, below, below, nb, panel, lda, 0, panel, lda, 0, trail, lda, 0, 1, true);
     }
 }
@@ -385,6 +393,7 @@ __global__ void trsv_bwd_kernel(const dd_t *L, long lda, int n, dd_t *x, int p, 
 
 void trsv_lower(cudaStream_t st, char trans, const dd_t *L, long lda, int n, dd_t *x) {
     if (n <= 0) return;
+    PROF_SCOPE("trsv", st);
     const int nblk = ceil_div(n, TRSV_B);
     if (trans == 'N') {
         for (int p = 0; p < nblk; ++p) {

@@ -11,11 +11,13 @@
 #include "capi_internal.h"
 #include "context.h"
 #include "newton.h"
+#include "prof.h"
 #include "solver.h"
 
 struct sddd_ctx {
     std::unique_ptr<sddd::Context> c;
     std::unique_ptr<sddd::Solver> solver;
+    std::unique_ptr<sddd::Profiler> prof;
     std::string err;
     int stop_reason = 0;
 };
@@ -113,6 +115,8 @@ int sddd_create(int device, sddd_ctx **out) {
 
 int sddd_destroy(sddd_ctx *ctx) {
     if (!ctx) return SDDD_OK;
+    if (ctx->prof && sddd::g_prof == ctx->prof.get()) sddd::g_prof = nullptr;
+    ctx->prof.reset();
     ctx->solver.reset();
     if (ctx->c) cudaSetDevice(ctx->c->device);
     ctx->c.reset();
@@ -413,6 +417,56 @@ int sddd_solve(sddd_ctx *ctx, const sddd_param *param, const char *result_path, 
         s.print_last_info(disp, fo, total, "");
         if (fo) std::fclose(fo);
         if (out) fill_result(ctx, out);
+        return SDDD_OK;
+    });
+}
+
+unsigned long long sddd_launch_count(void) { return sddd::g_launches; }
+
+void *sddd_stream(sddd_ctx *ctx) { return (ctx && ctx->c) ? (void *)ctx->c->stream : nullptr; }
+
+int sddd_profile(sddd_ctx *ctx, int enable) {
+    if (!ctx || !ctx->c) return SDDD_ERR_ARG;
+    if (enable) {
+        if (!ctx->prof) ctx->prof.reset(new sddd::Profiler());
+        sddd::g_prof = ctx->prof.get();
+    } else if (sddd::g_prof == ctx->prof.get()) {
+        sddd::g_prof = nullptr;
+    }
+    return SDDD_OK;
+}
+
+int sddd_profile_read(sddd_ctx *ctx, const char *name, double *ms, long *launches) {
+    if (!ctx || !ctx->c || !name) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (!ctx->prof) {
+            if (ms) *ms = 0;
+            if (launches) *launches = 0;
+            return SDDD_OK;
+        }
+        ctx->prof->collect(ctx->c->stream);
+        auto it = ctx->prof->totals.find(name);
+        if (ms) *ms = it == ctx->prof->totals.end() ? 0.0 : it->second.first;
+        if (launches) *launches = it == ctx->prof->totals.end() ? 0 : it->second.second;
+        return SDDD_OK;
+    });
+}
+
+int sddd_profile_reset(sddd_ctx *ctx) {
+    if (!ctx || !ctx->c) return SDDD_ERR_ARG;
+    if (ctx->prof) {
+        ctx->prof->collect(ctx->c->stream);
+        ctx->prof->totals.clear();
+    }
+    return SDDD_OK;
+}
+
+int sddd_work(const sddd_ctx *cctx, double *schur_ddflops, double *chol_ddflops) {
+    sddd_ctx *ctx = const_cast<sddd_ctx *>(cctx);
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        if (schur_ddflops) *schur_ddflops = c.schur_flops;
+        if (chol_ddflops) *chol_ddflops = c.chol_flops;
         return SDDD_OK;
     });
 }

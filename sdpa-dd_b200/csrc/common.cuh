@@ -37,8 +37,15 @@ inline void cuda_check(cudaError_t e, const char *what, const char *file, int li
         throw Error(e == cudaErrorMemoryAllocation ? ERR_NOMEM : ERR_CUDA, buf);
     }
 }
+// Kernels launched by this library in this process (every launch site
+// goes through CK_LAUNCH).
+extern unsigned long long g_launches;
 #define CK(call) ::sddd::cuda_check((call), #call, __FILE__, __LINE__)
-#define CK_LAUNCH() ::sddd::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+#define CK_LAUNCH()                                                                                                                                  \
+    do {                                                                                                                                             \
+        ++::sddd::g_launches;                                                                                                                        \
+        ::sddd::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__);                                                                 \
+    } while (0)
 
 inline unsigned ceil_div(long a, long b) { return (unsigned)((a + b - 1) / b); }
 

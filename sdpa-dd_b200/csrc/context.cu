@@ -225,6 +225,33 @@ static void build_block(Context &c, const Problem &P, int l, BlockDev &bd) {
         bd.rl_src.upload(rl_src, st);
         bd.rl_val.upload(rl_val, st);
     }
+    // algorithmic dd-flops of this block's part of Make_bMat: per owner the
+    // two n^3 products (F and G), 2 per term of the pair inner products,
+    // and for calF3 3 per product term (two multiplies, one add) plus the
+    // outer accumulation
+    {
+        double fl = 0;
+        const double n3 = 2.0 * n * (double)n * n;
+        std::vector<double> eff_s(nc);
+        for (int q = 0; q < nc; ++q) eff_s[q] = effect[perm[q]];
+        for (int q = 0; q < nc; ++q) {
+            const int f = formula[perm[q]];
+            const double ei = eff_s[q];
+            if (f == F3) {
+                double se = 0;
+                for (int r = 0; r <= q; ++r) se += eff_s[r];
+                fl += 3.0 * ei * se + 2.0 * se;
+            } else {
+                fl += (coo_off[perm[q]] >= 0 ? 2.0 * n * ei : n3) + n3;
+                for (int r = 0; r <= q; ++r) {
+                    const bool dense_partner = coo_off[perm[r]] < 0;
+                    if (dense_partner) fl += 2.0 * n * n;
+                    else fl += (f == F1 ? 2.0 * eff_s[r] : 2.0 * n * eff_s[r] + 2.0 * eff_s[r]);
+                }
+            }
+        }
+        c.schur_flops += fl;
+    }
     bd.ownFG.upload(bd.h_ownFG, st);
     bd.ownF3.upload(bd.h_ownF3, st);
     bd.fg_index.upload(fg_index, st);
@@ -249,6 +276,8 @@ void upload_problem(Context &c, Problem &&p) {
     for (int l = 0; l < c.nSDP; ++l) c.off[l + 1] = c.off[l] + (long)c.sizes[l] * c.sizes[l];
     c.space_len = c.off[c.nSDP];
     c.blocks.clear();
+    c.schur_flops = 0;
+    c.chol_flops = (double)c.m * c.m * c.m / 3.0;
     for (int l = 0; l < c.nSDP; ++l) {
         c.blocks.emplace_back(new BlockDev());
         build_block(c, P, l, *c.blocks.back());

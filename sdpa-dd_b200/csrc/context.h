@@ -148,6 +148,8 @@ struct Context {
     DBuf<int> info;
     DBuf<dd_t> rdiag;
     std::vector<dd_t> h_scal;
+    // algorithmic dd-flop counts of one Make_bMat and one Cholesky of B
+    double schur_flops = 0, chol_flops = 0;
     ~Context();
 };
 

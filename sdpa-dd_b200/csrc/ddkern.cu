@@ -34,7 +34,48 @@ __global__ void dd_op_kernel(int op, long n, const dd_t *a, const dd_t *b, dd_t 
     out[i] = r;
 }
 
+// FP64 issue-rate probe: 8 independent FMA chains per thread, full
+// occupancy; the FP64-pipe ceiling the dd kernels are measured against.
+__global__ void fp64_probe_kernel(double *out, int iters, double a, double b) {
+    double x[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = threadIdx.x * 1e-3 + j;
+    for (int it = 0; it < iters; ++it)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x[j] = __fma_rn(x[j], a, b);
+    double s = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s += x[j];
+    if (s == 1.2345) out[0] = s; // keeps the chains live
+}
+
 } // namespace sddd
+
+extern "C" int sddd_fp64_peak(sddd_ctx *, double *gflops) {
+    if (!gflops) return SDDD_ERR_ARG;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    double *d = nullptr;
+    if (cudaMalloc(&d, sizeof(double)) != cudaSuccess) return SDDD_ERR_CUDA;
+    const int iters = 4096, threads = 256, blocks = sms * 8;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    sddd::fp64_probe_kernel<<<blocks, threads>>>(d, iters, 0.999999, 1e-9);
+    cudaEventRecord(a);
+    sddd::fp64_probe_kernel<<<blocks, threads>>>(d, iters, 0.999999, 1e-9);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    if (cudaGetLastError() != cudaSuccess || ms <= 0) return SDDD_ERR_CUDA;
+    *gflops = 2.0 * 8.0 * iters * (double)threads * blocks / (ms * 1e-3) / 1e9;
+    return SDDD_OK;
+}
 
 extern "C" int sddd_dd_op(sddd_ctx *, int op, long n, const sddd_dd *a, const sddd_dd *b, sddd_dd *out) {
     if (n <= 0) return SDDD_OK;

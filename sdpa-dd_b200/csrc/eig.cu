@@ -16,6 +16,7 @@
 
 #include "blas.h"
 #include "devops.cuh"
+#include "prof.h"
 
 namespace sddd {
 
@@ -59,17 +60,29 @@ __device__ dd_t tri_min_eigenvalue(int k, const dd_t *d, const dd_t *e, dd_t *e2
     lo = dd_sub(lo, dd_mul_d(w, 1e-10));
     hi = dd_add(hi, dd_mul_d(w, 1e-10));
     for (int round = 0; round < 40; ++round) {
-        dd_t width = dd_sub(hi, lo);
-        // x_lane = lo + width * (lane+1)/33
-        dd_t x = dd_add(lo, dd_div_d(dd_mul_d(width, (double)(lane + 1)), 33.0));
-        bool below = (dd_lt(lo, x) && dd_lt(x, hi)) ? sturm_count(k, d, e2, x) >= 1 : (lane == 31);
-        unsigned ball = __ballot_sync(0xffffffffu, below);
-        int first = ball ? __ffs(ball) - 1 : 31;
+        const dd_t width = dd_sub(hi, lo);
+        // 32 interior points x_lane = lo + width (lane+1)/33; the smallest
+        // eigenvalue lies below the first x with a non-zero Sturm count,
+        // or above x_31 when there is none.
+        const dd_t x = dd_add(lo, dd_div_d(dd_mul_d(width, (double)(lane + 1)), 33.0));
+        bool below;
+        if (!dd_gt(x, lo))
+            below = false;
+        else if (!dd_lt(x, hi))
+            below = true;
+        else
+            below = sturm_count(k, d, e2, x) >= 1;
+        const unsigned ball = __ballot_sync(0xffffffffu, below);
         dd_t nlo, nhi;
-        // lanes agree on x values: recompute the bracket from lane indices
-        nhi = dd_add(lo, dd_div_d(dd_mul_d(width, (double)(first + 1)), 33.0));
-        nlo = first == 0 ? lo : dd_add(lo, dd_div_d(dd_mul_d(width, (double)first), 33.0));
-        if (!(dd_lt(nlo, nhi)) || (dd_eq(nlo, lo) && dd_eq(nhi, hi))) break;
+        if (ball == 0) {
+            nlo = dd_add(lo, dd_div_d(dd_mul_d(width, 32.0), 33.0));
+            nhi = hi;
+        } else {
+            const int first = __ffs(ball) - 1;
+            nhi = dd_add(lo, dd_div_d(dd_mul_d(width, (double)(first + 1)), 33.0));
+            nlo = first == 0 ? lo : dd_add(lo, dd_div_d(dd_mul_d(width, (double)first), 33.0));
+        }
+        if (!dd_lt(nlo, nhi) || (dd_eq(nlo, lo) && dd_eq(nhi, hi))) break;
         lo = nlo;
         hi = nhi;
     }
@@ -322,6 +335,7 @@ __global__ void small_min_eig_kernel(const int *blk_ids, const int *sizes, const
 
 dd_t min_eig(Context &c, const Space &L, const Space &D) {
     cudaStream_t st = c.stream;
+    PROF_SCOPE("min_eig", st);
     std::vector<int> big, small;
     for (int l = 0; l < c.nSDP; ++l) (c.sizes[l] > 20 ? big : small).push_back(l);
     static_assert(LZ_KMAX >= 64, "Lanczos step bound");

@@ -22,6 +22,7 @@
 #include "blas.h"
 #include "newton.h"
 #include "devops.cuh"
+#include "prof.h"
 
 namespace sddd {
 
@@ -231,6 +232,7 @@ __global__ void schur_f3_kernel(BlockView bv, const int *ownF3, int nf3, const d
 
 void schur_build(Context &c) {
     cudaStream_t st = c.stream;
+    PROF_SCOPE("schur_build", st);
     const int m = c.m;
     CK(cudaMemsetAsync(c.B.p, 0, sizeof(dd_t) * (size_t)m * m, st)); // bMat.setZero()
     for (int l = 0; l < c.nSDP; ++l) {

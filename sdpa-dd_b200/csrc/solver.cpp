@@ -29,27 +29,15 @@ struct EvSpan {
 struct EvClock {
     cudaStream_t st;
     std::vector<EvSpan> pending;
-    std::vector<cudaEvent_t> pool;
+    std::vector<cudaEvent_t> owned;
     explicit EvClock(cudaStream_t s) : st(s) {}
     ~EvClock() {
-        for (auto &p : pending) {
-            cudaEventDestroy(p.a);
-            cudaEventDestroy(p.b);
-        }
-        for (auto e : pool) cudaEventDestroy(e);
-    }
-    cudaEvent_t get() {
-        cudaEvent_t e;
-        if (!pool.empty()) {
-            e = pool.back();
-            pool.pop_back();
-        } else {
-            CK(cudaEventCreate(&e));
-        }
-        return e;
+        for (auto e : owned) cudaEventDestroy(e);
     }
     cudaEvent_t mark() {
-        cudaEvent_t e = get();
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        owned.push_back(e);
         CK(cudaEventRecord(e, st));
         return e;
     }
@@ -60,10 +48,6 @@ struct EvClock {
             float ms = 0;
             CK(cudaEventElapsedTime(&ms, p.a, p.b));
             *p.acc += ms * 1e-3;
-        }
-        for (auto &p : pending) {
-            pool.push_back(p.a);
-            pool.push_back(p.b);
         }
         pending.clear();
     }

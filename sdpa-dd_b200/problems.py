@@ -191,3 +191,26 @@ def write_param(path: str, eps: float = 1e-25, max_iter: int = 200, gamma: float
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
     return path
+
+
+def theta_edges(nv: int = 200, p: float = 0.5, seed: int = 2) -> int:
+    """Number of edges of the theta workload (same draw as theta())."""
+    rng = np.random.default_rng(seed)
+    iu, _ = np.triu_indices(nv, 1)
+    return int((rng.random(iu.shape[0]) < p).sum())
+
+
+def theta_work(nv: int, n_edges: int) -> tuple[float, float]:
+    """Algorithmic dd-flops of one Schur build and one Cholesky of B for the
+    theta workload, counted as the library counts them (sddd_work): the F2
+    owner F_1 = I needs F = A Z^-1 (2 n per nonzero) and G = X F (2 n^3),
+    then per partner 2 n + 2 per nonzero term; every edge owner (F3, two
+    off-diagonal terms) costs 3 eff_i eff_j + 2 eff_j per partner."""
+    n = float(nv)
+    m = 1 + n_edges
+    # sorted order: the E edges (effect 2) first, then F_1 (effect nv)
+    schur = 8.0 * n_edges * (n_edges + 1)          # sum_q (3*2 + 2) * 2 (q + 1)
+    schur += 2.0 * n * nv + 2.0 * n ** 3            # F and G of F_1
+    schur += n_edges * (2.0 * n * 2 + 2.0 * 2)      # F_1 with each edge
+    schur += 2.0 * n * nv + 2.0 * nv                # F_1 with itself
+    return schur, float(m) ** 3 / 3.0

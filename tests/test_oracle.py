@@ -36,13 +36,36 @@ def bits(a):
     return a.view(np.uint64)
 
 
+class Same:
+    """Truthy when two dd arrays are bitwise equal (+0 == -0); otherwise
+    falsy and its repr names the first differing entry."""
+
+    def __init__(self, a, b):
+        a = np.asarray(a).view(np.float64).copy()
+        b = np.asarray(b).view(np.float64).copy()
+        a[a == 0] = 0.0
+        b[b == 0] = 0.0
+        self.ok = a.shape == b.shape and np.array_equal(a.view(np.uint64), b.view(np.uint64))
+        self.msg = "equal"
+        if not self.ok:
+            if a.shape != b.shape:
+                self.msg = f"shapes {a.shape} vs {b.shape}"
+            else:
+                bad = np.nonzero(a.view(np.uint64) != b.view(np.uint64))[0]
+                i = int(bad[0]) // 2
+                self.msg = (f"{len(bad)} doubles differ; first dd #{i}: got ({a[2*i]!r}, {a[2*i+1]!r}) want ({b[2*i]!r}, {b[2*i+1]!r})"
+                            f"; max |diff| {np.max(np.abs(a - b)):.3e}")
+
+    def __bool__(self):
+        return self.ok
+
+    def __repr__(self):
+        return self.msg
+
+
 def same(a, b):
     """bitwise equal, treating +0 and -0 as equal"""
-    a = np.asarray(a).view(np.float64).copy()
-    b = np.asarray(b).view(np.float64).copy()
-    a[a == 0] = 0.0
-    b[b == 0] = 0.0
-    return np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    return Same(a, b)
 
 
 @pytest.mark.parametrize("op", list(range(18)))
