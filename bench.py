@@ -327,6 +327,29 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+def profile_case(args):
+    """One dd Cholesky of an m x m SPD matrix through sddd_Rpotrf (the
+    kernels of the bench's dominant phase, at a size an ncu capture can
+    replay); prints its time."""
+    sddd = load_pkg()
+    L = sddd.lib()
+    import torch
+    m = args.m
+    g = torch.Generator(device="cuda").manual_seed(7)
+    G = torch.randn(m, m, dtype=torch.float64, device="cuda", generator=g)
+    A = G @ G.T / m + torch.eye(m, dtype=torch.float64, device="cuda")
+    dd = torch.zeros(m * m, 2, dtype=torch.float64, device="cuda")
+    dd[:, 0] = A.T.reshape(-1)  # column-major
+    del G, A
+    with sddd.Context(0) as ctx:
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        info = L.sddd_Rpotrf(ctx.h, m, ctypes.c_void_p(dd.data_ptr()), m)
+        torch.cuda.synchronize()
+        print(json.dumps({"case": "potrf", "m": m, "info": info, "s": time.perf_counter() - t}))
+    return 0 if info == 0 else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -334,7 +357,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", choices=["potrf"], help="run one kernel-level case for an ncu capture and exit")
+    ap.add_argument("--m", type=int, default=4096)
     args = ap.parse_args()
+    if args.profile_case:
+        return profile_case(args)
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local = dist_init(args)
