@@ -1,12 +1,23 @@
 """Regenerate the end-to-end golden fixtures from the reference build.
 
-    OMP_NUM_THREADS=1 python tests/golden/make_golden.py
+    python tests/golden/make_golden.py
 
 Writes solves.json: for each seeded workload below, the reference's
 (oracle/_ref/sdpa_dd, one OpenMP thread) phase, iteration count and the two
 objective values as printed on stdout (32 digits, QD's dd output) and in
-the result file (16 digits).  Needs oracle/_ref built from the reference
-sources (make -C oracle ref); the GPU tests only read the JSON.
+the result file (16 digits), and its mu after every pass of the main loop
+(oracle/_ref/libsdpadd_ref.so stepped through ref_step).
+
+The reference's dd reductions (Rdot, Rgemv, the inner products) combine
+OpenMP partial sums in arrival order, so with more than one thread its
+trajectory, final phase and iteration count vary from run to run once mu
+nears the dd noise floor.  The same workloads are therefore also run with
+VARIANT_THREADS threads, each VARIANT_REPEATS times: the fixture keeps each
+run's phase, iteration count and objectives, and per pass the largest
+relative distance of a run's mu from the one-thread mu ("mu_spread").
+
+Needs oracle/_ref built from the reference sources (make -C oracle ref);
+the GPU tests only read the JSON.
 """
 import importlib.util
 import json
@@ -35,6 +46,10 @@ CASES = {
 }
 
 
+VARIANT_THREADS = (2, 3, 4, 8)
+VARIANT_REPEATS = 2
+
+
 def parse(stdout: str, result: str) -> dict:
     d = {}
     d["phase"] = re.search(r"phase.value = (\w+)", result).group(1)
@@ -48,9 +63,49 @@ def parse(stdout: str, result: str) -> dict:
     return d
 
 
-def main():
+def trajectory(name: str) -> list:
+    """mu (hi, lo) after every pass of the reference's main loop, stepped in
+    this process through oracle/_ref/libsdpadd_ref.so (ref_step returns 0
+    while the loop goes on)."""
+    import ctypes
+
+    import numpy as np
+    lib = ctypes.CDLL(str(ROOT / "oracle" / "_ref" / "libsdpadd_ref.so"))
+    lib.ref_open.restype = ctypes.c_void_p
+    make, eps = CASES[name]
+    mus = []
+    with tempfile.TemporaryDirectory() as td:
+        data = pathlib.Path(td) / f"{name}.dat-s"
+        data.write_text(make())
+        param = P.write_param(str(pathlib.Path(td) / f"{name}.param"), eps=eps)
+        h = ctypes.c_void_p(lib.ref_open(str(data).encode(), param.encode(), ctypes.c_double(1.2)))
+        out = np.zeros(2, np.float64)
+        try:
+            while lib.ref_step(h) == 0:
+                lib.ref_scalar(h, 0, out.ctypes.data_as(ctypes.c_void_p))
+                mus.append([float(out[0]), float(out[1])])
+        finally:
+            lib.ref_close(h)
+    return mus
+
+
+def _run(name, data, param, res, threads):
     ref = ROOT / "oracle" / "_ref" / "sdpa_dd"
-    env = dict(os.environ, OMP_NUM_THREADS="1")
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    r = subprocess.run([str(ref), "-ds", str(data), "-o", str(res), "-p", param], capture_output=True, text=True, env=env, check=True)
+    d = parse(r.stdout, res.read_text())
+    t = subprocess.run([sys.executable, __file__, "--trajectory", name], capture_output=True, text=True, env=env, check=True)
+    d["mu_trajectory"] = json.loads(t.stdout.strip().splitlines()[-1])  # the library prints a banner first
+    return d
+
+
+def _rel(a, b):
+    from decimal import Decimal
+    a, b = Decimal(a[0]) + Decimal(a[1]), Decimal(b[0]) + Decimal(b[1])
+    return float(abs(a - b) / max(abs(b), Decimal("1e-300")))
+
+
+def main():
     out = {}
     with tempfile.TemporaryDirectory() as td:
         td = pathlib.Path(td)
@@ -59,11 +114,21 @@ def main():
             data.write_text(make())
             param = P.write_param(str(td / f"{name}.param"), eps=eps)
             res = td / f"{name}.result"
-            r = subprocess.run([str(ref), "-ds", str(data), "-o", str(res), "-p", param], capture_output=True, text=True, env=env, check=True)
-            out[name] = dict(parse(r.stdout, res.read_text()), eps=eps)
-            print(name, out[name]["phase"], out[name]["iterations"], out[name]["objValPrimal32"], file=sys.stderr)
+            one = _run(name, data, param, res, 1)
+            variants = [dict(_run(name, data, param, res, t), threads=t) for t in VARIANT_THREADS for _ in range(VARIANT_REPEATS)]
+            mu1 = one["mu_trajectory"]
+            spread = []
+            for k in range(min(len(mu1), *(len(v["mu_trajectory"]) for v in variants))):
+                spread.append(max(_rel(v["mu_trajectory"][k], mu1[k]) for v in variants))
+            keep = ("threads", "phase", "iterations", "objValPrimal32", "objValDual32")
+            out[name] = dict(one, eps=eps, mu_spread=spread, variants=[{k: v[k] for k in keep} for v in variants])
+            print(name, out[name]["phase"], out[name]["iterations"], sorted({(v["phase"], v["iterations"]) for v in variants}),
+                  file=sys.stderr)
     (HERE / "solves.json").write_text(json.dumps(out, indent=1, sort_keys=True) + "\n")
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) == 3 and sys.argv[1] == "--trajectory":
+        print(json.dumps(trajectory(sys.argv[2])))
+    else:
+        main()
