@@ -105,6 +105,22 @@ int sddd_solve_dy(sddd_ctx *ctx);      /* Dy = B^-1 g */
 int sddd_make_dz_dx(sddd_ctx *ctx, int dual_infeasible);
 /* min eigenvalue of L D L^T for the step length: which = 0 (L_X^-1, Dx) or 1 (L_Z^-1, Dz). */
 int sddd_min_eig(sddd_ctx *ctx, int which, sddd_dd *out);
+/* The same eigenvalue for ONE block of order n, with no device allocation.
+ * It has no counterpart in the reference.  It is for callers that cannot
+ * let a library allocate: a process whose memory pool already holds the
+ * GPU (cudaMalloc would fail) or whose other streams must not stall
+ * (cudaFree synchronises the device).  L (lower triangle read), D
+ * (symmetric) and out (one dd) are device pointers, n x n column-major;
+ * the work goes on `stream` (a cudaStream_t, NULL = legacy default) of the
+ * current device and *out is written asynchronously on it.
+ * Scratch is a static device array that every GPU loading the library holds
+ * until exit: about 320 KiB, enough for n <= SDDD_MIN_EIG_NOALLOC_MAX_N;
+ * a larger n returns SDDD_ERR_ARG with a message in sddd_last_error(NULL).
+ * The first call on each device looks up the array's address (make it
+ * before any stream capture).  All calls share the array: calls that
+ * overlap on the GPU race. */
+#define SDDD_MIN_EIG_NOALLOC_MAX_N 4096
+int sddd_min_eig_noalloc(void *stream, long n, const sddd_dd *L, const sddd_dd *D, sddd_dd *out);
 int sddd_update(sddd_ctx *ctx, sddd_dd alpha_primal, sddd_dd alpha_dual);
 int sddd_residuals(sddd_ctx *ctx, sddd_dd *norm_primal, sddd_dd *norm_dual);
 /* Inner products: 0 C.X, 1 b.y, 2 X.Z, 3 C.Dx, 4 b.Dy, 5 X.Dz, 6 Dx.Z, 7 Dx.Dz */

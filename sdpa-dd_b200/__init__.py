@@ -73,6 +73,7 @@ def lib() -> ctypes.CDLL:
         "sddd_solve_dy": (ci, [vp]),
         "sddd_make_dz_dx": (ci, [vp, ci]),
         "sddd_min_eig": (ci, [vp, ci, ctypes.POINTER(SdddDD)]),
+        "sddd_min_eig_noalloc": (ci, [vp, cl, vp, vp, vp]),
         "sddd_update": (ci, [vp, SdddDD, SdddDD]),
         "sddd_residuals": (ci, [vp, ctypes.POINTER(SdddDD), ctypes.POINTER(SdddDD)]),
         "sddd_inner": (ci, [vp, ci, ctypes.POINTER(SdddDD)]),

@@ -41,6 +41,12 @@ int guarded(sddd_ctx *ctx, F &&f) {
     }
 }
 
+} // namespace
+
+void sddd_set_thread_error(const char *msg) { g_err = msg ? msg : ""; }
+
+namespace {
+
 sddd::Context &need_problem(sddd_ctx *ctx) {
     if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
     if (!ctx->c->have_problem) throw sddd::Error(SDDD_ERR_STATE, "no problem uploaded");

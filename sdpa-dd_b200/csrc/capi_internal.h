@@ -7,3 +7,6 @@
 
 void sddd_attach_problem(sddd_ctx *ctx, sddd::Problem &&p);
 int sddd_solve_stream(sddd_ctx *ctx, const sddd_param *param, FILE *disp, FILE *fo, double fileRead, double *mainLoop);
+// Records the message that sddd_last_error(NULL) returns on this thread
+// (for entry points that take no context).
+void sddd_set_thread_error(const char *msg);

@@ -16,12 +16,10 @@
 
 #include "blas.h"
 #include "devops.cuh"
+#include "eig_kernels.cuh"
 #include "prof.h"
 
 namespace sddd {
-
-constexpr int LZ_THREADS = 512;
-constexpr int LZ_KMAX = 128;
 
 // QD double-vs-dd comparisons (dd_inline.h operator< / operator>)
 __device__ __forceinline__ bool d_lt_dd(double a, dd_t b) { return a < b.hi || (a == b.hi && b.lo > 0.0); }
