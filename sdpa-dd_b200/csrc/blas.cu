@@ -303,109 +303,264 @@ void zero_upper(cudaStream_t st, dd_t *A, long lda, int n) {
 }
 
 // ===================================================================== TRSV
+// One cooperative launch per solve.  The matrix is cut into 64 x 64 tiles;
+// CTA b owns the 64-entry blocks c = b, b + G, ... of x (forward) or the
+// mirror order from the last block down (backward) and publishes each
+// finished block through a per-block flag that holds the solve's epoch.
+// Each entry keeps the reference's own chain (mplapack/Rtrsv.cpp, the
+// reference BLAS loop order):
+//   "N": x(i) -= x(j) L(i,j) for j ascending (skipped when x(j) == 0),
+//        then x(i) /= L(i,i) when x(i) != 0;
+//   "T": t = x(j); t -= L(i,j) x(i) for i descending; x(j) = t / L(j,j).
+// Warp 0 holds the 64 entries of the current block, two per lane, and runs
+// the chains; the other warps stage the next tile of L in shared memory
+// (padded leading dimension 65: conflict-free for rows and columns).
+// A CTA waits for a block with an acquire load bounded by a 2 s budget;
+// on expiry it records the block in the error word and returns.
 constexpr int TRSV_B = 64;
+constexpr int TRSV_LD = 65;
+constexpr int TRSV_THREADS = 256;
+constexpr size_t TRSV_SMEM = 2 * sizeof(double2) * TRSV_B * TRSV_LD + sizeof(double2) * TRSV_B;
 
-// Forward solve, launch p: rows of blocks c >= p first take block p-1's
-// solution (x(i) -= x(j) L(i,j), j ascending); then CTA p solves its own
-// diagonal block (x(j) /= L(j,j) when x(j) != 0, then x(i) -= x(j) L(i,j)).
-__global__ void trsv_fwd_kernel(const dd_t *L, long lda, int n, dd_t *x, int p) {
-    __shared__ double2 xs[TRSV_B];
-    const int c = p + blockIdx.x;
-    const int r0 = c * TRSV_B, tid = threadIdx.x;
-    const int i = r0 + tid;
-    dd_t xi = dd_zero();
-    if (i < n) xi = ld_dd(x + i);
-    if (p > 0) {
-        const int j0 = (p - 1) * TRSV_B;
-        for (int t = tid; t < TRSV_B; t += blockDim.x) xs[t] = *reinterpret_cast<const double2 *>(x + j0 + t);
-        __syncthreads();
-        if (i < n)
-            for (int t = 0; t < TRSV_B; ++t) {
-                dd_t xj = dd_make(xs[t].x, xs[t].y);
-                if (!dd_is_zero(xj)) xi = dd_sub(xi, dd_mul(xj, ld_dd(L + i + lda * (long)(j0 + t))));
-            }
-        __syncthreads();
-    }
-    if (c == p) {
-        const int nb = min(TRSV_B, n - r0);
-        xs[tid] = make_double2(xi.hi, xi.lo);
-        __syncthreads();
-        for (int t = 0; t < nb; ++t) {
-            if (tid == t) {
-                dd_t v = dd_make(xs[t].x, xs[t].y);
-                if (!dd_is_zero(v)) v = dd_div(v, ld_dd(L + (r0 + t) + lda * (long)(r0 + t)));
-                xs[t] = make_double2(v.hi, v.lo);
-            }
-            __syncthreads();
-            dd_t xt = dd_make(xs[t].x, xs[t].y);
-            if (tid > t && tid < nb && !dd_is_zero(xt)) {
-                dd_t v = dd_make(xs[tid].x, xs[tid].y);
-                v = dd_sub(v, dd_mul(xt, ld_dd(L + (r0 + tid) + lda * (long)(r0 + t))));
-                xs[tid] = make_double2(v.hi, v.lo);
-            }
-            __syncthreads();
-        }
-        xi = dd_make(xs[tid].x, xs[tid].y);
-    }
-    if (i < n) st_dd(x + i, xi);
+struct TrsvArgs {
+    const dd_t *L;
+    long lda;
+    int n, nblk, epoch;
+    dd_t *x;
+    int *flags, *err;
+};
+
+__device__ __forceinline__ int ld_acquire_gpu(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(int *p, int v) { asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory"); }
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
 
-// Backward solve with L^T, launch p (from the last block down): entries of
-// blocks c <= p take block p+1's solution (t -= L(i,j) x(i), i descending);
-// then CTA p finishes its block (j descending: x(j) = t(j) / L(j,j)).
-__global__ void trsv_bwd_kernel(const dd_t *L, long lda, int n, dd_t *x, int p, int nblk) {
-    __shared__ double2 xs[TRSV_B];
-    const int c = blockIdx.x; // blocks 0..p
-    const int r0 = c * TRSV_B, tid = threadIdx.x;
-    const int j = r0 + tid;
-    dd_t xj = dd_zero();
-    if (j < n) xj = ld_dd(x + j);
-    if (p + 1 < nblk) {
-        const int i0 = (p + 1) * TRSV_B;
-        const int ib = min(TRSV_B, n - i0);
-        for (int t = tid; t < ib; t += blockDim.x) xs[t] = *reinterpret_cast<const double2 *>(x + i0 + t);
-        __syncthreads();
-        if (j < n)
-            for (int t = ib - 1; t >= 0; --t) xj = dd_sub(xj, dd_mul(ld_dd(L + (i0 + t) + lda * (long)j), dd_make(xs[t].x, xs[t].y)));
-        __syncthreads();
-    }
-    if (c == p) {
-        const int nb = min(TRSV_B, n - r0);
-        xs[tid] = make_double2(xj.hi, xj.lo);
-        __syncthreads();
-        for (int t = nb - 1; t >= 0; --t) {
-            if (tid == t) {
-                dd_t v = dd_div(dd_make(xs[t].x, xs[t].y), ld_dd(L + (r0 + t) + lda * (long)(r0 + t)));
-                xs[t] = make_double2(v.hi, v.lo);
+// Lane 0 of the calling warp waits until flags[blk] == epoch; every lane
+// returns the outcome.
+__device__ bool trsv_wait(const TrsvArgs &a, int blk) {
+    int ok = 1;
+    if ((threadIdx.x & 31) == 0) {
+        const unsigned long long t0 = global_ns();
+        unsigned iter = 0;
+        while (ld_acquire_gpu(a.flags + blk) != a.epoch) {
+            if (ld_acquire_gpu(a.err) != 0 || ++iter > (1u << 26) || global_ns() - t0 > 2000000000ull) {
+                atomicCAS(a.err, 0, blk + 1);
+                ok = 0;
+                break;
             }
-            __syncthreads();
-            if (tid < t) {
-                dd_t v = dd_make(xs[tid].x, xs[tid].y);
-                v = dd_sub(v, dd_mul(ld_dd(L + (r0 + t) + lda * (long)(r0 + tid)), dd_make(xs[t].x, xs[t].y)));
-                xs[tid] = make_double2(v.hi, v.lo);
-            }
-            __syncthreads();
+            __nanosleep(64);
         }
-        xj = dd_make(xs[tid].x, xs[tid].y);
     }
-    if (j < n) st_dd(x + j, xj);
+    return __shfl_sync(0xffffffffu, ok, 0) != 0;
 }
 
-void trsv_lower(cudaStream_t st, char trans, const dd_t *L, long lda, int n, dd_t *x) {
+// T(i, j) = L(r0 + i, c0 + j) for i, j < 64 (zero outside the matrix).
+__device__ __forceinline__ void trsv_load_tile(double2 *T, const TrsvArgs &a, int r0, int c0, int t0, int nt) {
+    for (int e = t0; e < TRSV_B * TRSV_B; e += nt) {
+        const int i = e % TRSV_B, j = e / TRSV_B;
+        const int gi = r0 + i, gj = c0 + j;
+        double2 v = make_double2(0.0, 0.0);
+        if (gi < a.n && gj < a.n) v = __ldg(reinterpret_cast<const double2 *>(a.L + gi + a.lda * (long)gj));
+        T[i + TRSV_LD * j] = v;
+    }
+}
+
+__device__ __forceinline__ dd_t tile_dd(const double2 *T, int i, int j) {
+    const double2 v = T[i + TRSV_LD * j];
+    return dd_make(v.x, v.y);
+}
+__device__ __forceinline__ dd_t ldcg_dd(const dd_t *p) {
+    const double2 v = __ldcg(reinterpret_cast<const double2 *>(p));
+    return dd_make(v.x, v.y);
+}
+__device__ __forceinline__ dd_t shfl_dd(dd_t v, int src) {
+    return dd_make(__shfl_sync(0xffffffffu, v.hi, src), __shfl_sync(0xffffffffu, v.lo, src));
+}
+
+__global__ void __launch_bounds__(TRSV_THREADS) trsv_fwd_wave_kernel(TrsvArgs a) {
+    extern __shared__ double2 trsv_sm[];
+    double2 *xs = trsv_sm + 2 * TRSV_B * TRSV_LD;
+    __shared__ int fail;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) fail = 0;
+    for (int c = blockIdx.x; c < a.nblk; c += gridDim.x) {
+        const int r0 = c * TRSV_B;
+        const int i0 = r0 + lane, i1 = r0 + 32 + lane;
+        dd_t v0 = dd_zero(), v1 = dd_zero();
+        if (warp == 0) {
+            if (i0 < a.n) v0 = ld_dd(a.x + i0);
+            if (i1 < a.n) v1 = ld_dd(a.x + i1);
+        }
+        trsv_load_tile(trsv_sm, a, r0, 0, tid, blockDim.x);
+        __syncthreads();
+        for (int p = 0; p < c; ++p) {
+            const double2 *T = trsv_sm + (p & 1) * TRSV_B * TRSV_LD;
+            if (warp != 0) {
+                trsv_load_tile(trsv_sm + ((p + 1) & 1) * TRSV_B * TRSV_LD, a, r0, (p + 1) * TRSV_B, tid - 32, blockDim.x - 32);
+            } else if (!trsv_wait(a, p)) {
+                if (lane == 0) fail = 1;
+            } else {
+                // block p is complete (p < c): 64 entries
+                const dd_t xa = ldcg_dd(a.x + p * TRSV_B + lane), xb = ldcg_dd(a.x + p * TRSV_B + 32 + lane);
+                xs[lane] = make_double2(xa.hi, xa.lo);
+                xs[32 + lane] = make_double2(xb.hi, xb.lo);
+                __syncwarp();
+                for (int t = 0; t < TRSV_B; ++t) {
+                    const dd_t xt = dd_make(xs[t].x, xs[t].y);
+                    if (!dd_is_zero(xt)) {
+                        v0 = dd_sub(v0, dd_mul(xt, tile_dd(T, lane, t)));
+                        v1 = dd_sub(v1, dd_mul(xt, tile_dd(T, 32 + lane, t)));
+                    }
+                }
+                __syncwarp();
+            }
+            __syncthreads();
+            if (fail) return;
+        }
+        if (warp == 0) {
+            // diagonal tile (p == c)
+            const double2 *T = trsv_sm + (c & 1) * TRSV_B * TRSV_LD;
+            const int nb = min(TRSV_B, a.n - r0);
+            for (int t = 0; t < nb; ++t) {
+                const int owner = t & 31;
+                dd_t mine = t < 32 ? v0 : v1;
+                if (lane == owner && !dd_is_zero(mine)) mine = dd_div(mine, tile_dd(T, t, t));
+                if (lane == owner) {
+                    if (t < 32) v0 = mine;
+                    else v1 = mine;
+                }
+                const dd_t xt = shfl_dd(mine, owner);
+                if (!dd_is_zero(xt)) {
+                    if (lane > t && lane < nb) v0 = dd_sub(v0, dd_mul(xt, tile_dd(T, lane, t)));
+                    if (32 + lane > t && 32 + lane < nb) v1 = dd_sub(v1, dd_mul(xt, tile_dd(T, 32 + lane, t)));
+                }
+            }
+            if (i0 < a.n) st_dd(a.x + i0, v0);
+            if (i1 < a.n) st_dd(a.x + i1, v1);
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) st_release_gpu(a.flags + c, a.epoch);
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(TRSV_THREADS) trsv_bwd_wave_kernel(TrsvArgs a) {
+    extern __shared__ double2 trsv_sm[];
+    double2 *xs = trsv_sm + 2 * TRSV_B * TRSV_LD;
+    __shared__ int fail;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) fail = 0;
+    for (int k = blockIdx.x; k < a.nblk; k += gridDim.x) {
+        const int c = a.nblk - 1 - k;
+        const int r0 = c * TRSV_B;
+        const int j0 = r0 + lane, j1 = r0 + 32 + lane;
+        dd_t v0 = dd_zero(), v1 = dd_zero();
+        if (warp == 0) {
+            if (j0 < a.n) v0 = ld_dd(a.x + j0);
+            if (j1 < a.n) v1 = ld_dd(a.x + j1);
+        }
+        // tiles T(i, j) = L(p*64 + i, r0 + j) for p = nblk-1 down to c
+        trsv_load_tile(trsv_sm, a, (a.nblk - 1) * TRSV_B, r0, tid, blockDim.x);
+        __syncthreads();
+        int s = 0;
+        for (int p = a.nblk - 1; p > c; --p, ++s) {
+            const double2 *T = trsv_sm + (s & 1) * TRSV_B * TRSV_LD;
+            if (warp != 0) {
+                trsv_load_tile(trsv_sm + ((s + 1) & 1) * TRSV_B * TRSV_LD, a, (p - 1) * TRSV_B, r0, tid - 32, blockDim.x - 32);
+            } else if (!trsv_wait(a, p)) {
+                if (lane == 0) fail = 1;
+            } else {
+                const int ib = min(TRSV_B, a.n - p * TRSV_B);
+                if (lane < ib) {
+                    const dd_t xa = ldcg_dd(a.x + p * TRSV_B + lane);
+                    xs[lane] = make_double2(xa.hi, xa.lo);
+                }
+                if (32 + lane < ib) {
+                    const dd_t xb = ldcg_dd(a.x + p * TRSV_B + 32 + lane);
+                    xs[32 + lane] = make_double2(xb.hi, xb.lo);
+                }
+                __syncwarp();
+                for (int t = ib - 1; t >= 0; --t) {
+                    const dd_t xt = dd_make(xs[t].x, xs[t].y);
+                    v0 = dd_sub(v0, dd_mul(tile_dd(T, t, lane), xt));
+                    v1 = dd_sub(v1, dd_mul(tile_dd(T, t, 32 + lane), xt));
+                }
+                __syncwarp();
+            }
+            __syncthreads();
+            if (fail) return;
+        }
+        if (warp == 0) {
+            const double2 *T = trsv_sm + (s & 1) * TRSV_B * TRSV_LD;
+            const int nb = min(TRSV_B, a.n - r0);
+            for (int t = nb - 1; t >= 0; --t) {
+                const int owner = t & 31;
+                dd_t mine = t < 32 ? v0 : v1;
+                if (lane == owner) {
+                    mine = dd_div(mine, tile_dd(T, t, t));
+                    if (t < 32) v0 = mine;
+                    else v1 = mine;
+                }
+                const dd_t xt = shfl_dd(mine, owner);
+                if (lane < t) v0 = dd_sub(v0, dd_mul(tile_dd(T, t, lane), xt));
+                if (32 + lane < t) v1 = dd_sub(v1, dd_mul(tile_dd(T, t, 32 + lane), xt));
+            }
+            if (j0 < a.n) st_dd(a.x + j0, v0);
+            if (j1 < a.n) st_dd(a.x + j1, v1);
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) st_release_gpu(a.flags + c, a.epoch);
+        }
+        __syncthreads();
+    }
+}
+
+// Co-resident CTAs of a wave kernel on the current device.
+static int trsv_grid_cap(const void *kernel) {
+    int dev = 0, sms = 0, per = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRSV_SMEM));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, TRSV_THREADS, TRSV_SMEM));
+    if (per < 1) throw Error(ERR_CUDA, "trsv: the wave kernel does not fit on an SM");
+    return per * sms;
+}
+
+void trsv_lower(cudaStream_t st, char trans, const dd_t *L, long lda, int n, dd_t *x, TrsvSync &sync) {
     if (n <= 0) return;
-    PROF_SCOPE("trsv", st);
+    if (trans != 'N' && trans != 'T') throw Error(ERR_ARG, "trsv: trans must be 'N' or 'T'");
     const int nblk = ceil_div(n, TRSV_B);
-    if (trans == 'N') {
-        for (int p = 0; p < nblk; ++p) {
-            trsv_fwd_kernel<<<nblk - p, TRSV_B, 0, st>>>(L, lda, n, x, p);
-            CK_LAUNCH();
-        }
-    } else {
-        for (int p = nblk - 1; p >= 0; --p) {
-            trsv_bwd_kernel<<<p + 1, TRSV_B, 0, st>>>(L, lda, n, x, p, nblk);
-            CK_LAUNCH();
-        }
-    }
+    if (nblk > sync.capacity || !sync.flags) throw Error(ERR_ARG, "trsv: progress flags hold fewer blocks than the solve needs");
+    PROF_SCOPE("trsv", st);
+    if (++sync.epoch <= 0) sync.epoch = 1;
+    TrsvArgs a{L, lda, n, nblk, sync.epoch, x, sync.flags, sync.flags + sync.capacity};
+    const void *k = trans == 'N' ? (const void *)trsv_fwd_wave_kernel : (const void *)trsv_bwd_wave_kernel;
+    static thread_local int cap[2][64] = {};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    int &cp = cap[trans == 'N' ? 0 : 1][dev & 63];
+    if (cp == 0) cp = trsv_grid_cap(k);
+    const int grid = std::min(nblk, cp);
+    void *args[] = {&a};
+    CK(cudaLaunchCooperativeKernel(k, grid, TRSV_THREADS, args, TRSV_SMEM, st));
+    CK_LAUNCH();
+}
+
+void trsv_check(cudaStream_t st, const TrsvSync &sync) {
+    if (!sync.flags) return;
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, sync.flags + sync.capacity, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (err != 0)
+        throw Error(ERR_CUDA, "trsv: a block waited more than 2 s for block " + std::to_string(err - 1) + " (solve abandoned)");
 }
 
 // ======================================================= triangular inverse

@@ -17,7 +17,19 @@ void gemm(cudaStream_t st, char ta, char tb, int mode, int M, int N, int K, cons
 // rdiag_dev holds POTRF_NB dd of scratch.
 void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag_dev);
 void zero_upper(cudaStream_t st, dd_t *A, long lda, int n);
-void trsv_lower(cudaStream_t st, char trans, const dd_t *L, long lda, int n, dd_t *x);
+// Progress words of the one-launch triangular solve: one flag per 64-entry
+// block (the epoch of the solve that finished it), then an error word.
+// The owner zeroes them once; the epoch advances with every solve.
+struct TrsvSync {
+    int *flags = nullptr; // capacity flags + 1 error word
+    int capacity = 0;
+    int epoch = 0;
+};
+// x = L^-1 x ('N') or L^-T x ('T'), L lower, as Rtrsv("Lower", trans, "NonUnit").
+void trsv_lower(cudaStream_t st, char trans, const dd_t *L, long lda, int n, dd_t *x, TrsvSync &sync);
+// Throws when a solve since the flags were zeroed gave up waiting
+// (synchronises st).
+void trsv_check(cudaStream_t st, const TrsvSync &sync);
 void inv_lower(cudaStream_t st, const dd_t *L, long lda, int n, dd_t *X, long ldx);
 void trmm_lt(cudaStream_t st, const dd_t *M, long ldm, int n, dd_t *B, long ldb);
 void symmetrize(cudaStream_t st, dd_t *A, int n);

@@ -505,8 +505,9 @@ int sddd_Rpotrf(sddd_ctx *ctx, long n, sddd_dd *A, long lda) {
 int sddd_Rtrsv(sddd_ctx *ctx, char trans, long n, sddd_dd *L, long lda, sddd_dd *x) {
     return guarded(ctx, [&] {
         if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
-        sddd::trsv_lower(ctx->c->stream, trans, reinterpret_cast<dd_t *>(L), lda, (int)n, reinterpret_cast<dd_t *>(x));
-        CK(cudaStreamSynchronize(ctx->c->stream));
+        sddd::TrsvSync &sync = sddd::trsv_sync(*ctx->c, (int)n);
+        sddd::trsv_lower(ctx->c->stream, trans, reinterpret_cast<dd_t *>(L), lda, (int)n, reinterpret_cast<dd_t *>(x), sync);
+        sddd::trsv_check(ctx->c->stream, sync);
         return SDDD_OK;
     });
 }

@@ -42,6 +42,17 @@ Context::~Context() {
     if (stream) cudaStreamDestroy(stream);
 }
 
+TrsvSync &trsv_sync(Context &c, int n) {
+    const int nblk = (int)ceil_div(n, 64);
+    if (nblk > c.trsv.capacity || !c.trsv.flags) {
+        CK(cudaStreamSynchronize(c.stream));
+        c.trsv_flags.alloc((size_t)nblk + 1);
+        CK(cudaMemsetAsync(c.trsv_flags.p, 0, sizeof(int) * ((size_t)nblk + 1), c.stream));
+        c.trsv = TrsvSync{c.trsv_flags.p, nblk, 0};
+    }
+    return c.trsv;
+}
+
 Context *create_context(int device) {
     int count = 0;
     CK(cudaGetDeviceCount(&count));

@@ -8,6 +8,7 @@
 #include <string>
 #include <vector>
 
+#include "blas.h"
 #include "common.cuh"
 #include "problem.h"
 
@@ -147,6 +148,8 @@ struct Context {
     DBuf<dd_t> red;    // reduction scratch
     DBuf<int> info;
     DBuf<dd_t> rdiag;
+    DBuf<int> trsv_flags; // progress words of the one-launch triangular solve
+    TrsvSync trsv;
     std::vector<dd_t> h_scal;
     // algorithmic dd-flop counts of one Make_bMat and one Cholesky of B
     double schur_flops = 0, chol_flops = 0;
@@ -156,6 +159,8 @@ struct Context {
 Context *create_context(int device);
 void upload_problem(Context &c, Problem &&p);
 void alloc_state(Context &c);
+// The triangular-solve progress words, grown (and zeroed) to cover order n.
+TrsvSync &trsv_sync(Context &c, int n);
 
 // Host<->device for spaces laid out as the C-ABI defines: SDP blocks
 // concatenated, each n_l x n_l column-major.

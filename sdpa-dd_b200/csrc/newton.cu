@@ -173,8 +173,10 @@ int schur_factor(Context &c) {
 
 void solve_dy(Context &c) {
     CK(cudaMemcpyAsync(c.Dy.p, c.g.p, sizeof(dd_t) * c.m, cudaMemcpyDeviceToDevice, c.stream));
-    trsv_lower(c.stream, 'N', c.B.p, c.m, c.m, c.Dy.p);
-    trsv_lower(c.stream, 'T', c.B.p, c.m, c.m, c.Dy.p);
+    TrsvSync &sync = trsv_sync(c, c.m);
+    trsv_lower(c.stream, 'N', c.B.p, c.m, c.m, c.Dy.p, sync);
+    trsv_lower(c.stream, 'T', c.B.p, c.m, c.m, c.Dy.p, sync);
+    trsv_check(c.stream, sync);
 }
 
 void make_dz_dx(Context &c, bool dual_infeasible) {

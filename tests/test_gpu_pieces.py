@@ -130,6 +130,29 @@ def test_device_potrf_trsv_match(ctx, oracle_lib, n):
         assert same(from_dev(dx, n), x), tr
 
 
+@pytest.mark.parametrize("n,lda", [(300, 320), (9800, 9800)])
+def test_device_trsv_wavefront_matches_rtrsv(ctx, oracle_lib, n, lda):
+    """The one-launch solve with more 64-entry blocks than co-resident CTAs
+    (9800 = 153 full blocks + 8), a leading dimension above n and zero
+    right-hand-side entries (the forward loop's skip)."""
+    rng = np.random.default_rng(n)
+    L = np.zeros(lda * n, DD)
+    for j in range(n):
+        col = L[j * lda:(j + 1) * lda]
+        col["hi"][j] = 1.0 + rng.random()
+        col["hi"][j + 1:n] = rng.standard_normal(n - j - 1) / np.sqrt(n)
+        col["lo"][j:n] = col["hi"][j:n] * rng.uniform(-1, 1, n - j) * 1e-17
+    dL = to_dev(L)
+    for tr in ("N", "T"):
+        b = rand_dd(rng, n)
+        b[rng.random(n) < 0.05] = (0.0, 0.0)
+        x = b.copy()
+        oracle_lib.o_trsv(ctypes.c_char(tr.encode()), ctypes.c_long(n), ptr(L), ctypes.c_long(lda), ptr(x))
+        dx = to_dev(b)
+        assert ctx.L.sddd_Rtrsv(ctx.h, tr.encode(), n, ctypes.c_void_p(dL.data_ptr()), lda, ctypes.c_void_p(dx.data_ptr())) == 0
+        assert same(from_dev(dx, n), x), tr
+
+
 def test_device_potrf_reports_failing_column(ctx, oracle_lib):
     rng = np.random.default_rng(9)
     n = 150
