@@ -203,6 +203,8 @@ def run_ours(args, world, rank, local):
     workdir.mkdir(exist_ok=True)
     data, param_path = write_workload(WORKLOAD, workdir)
     ctx = sddd.Context(local)
+    if args.tc and L.sddd_set_tc_split(ctx.h, args.tc) != 0:
+        raise RuntimeError(L.sddd_last_error(ctx.h).decode())
     t0 = time.perf_counter()
     ctx.read_problem(data, sparse=True, kappa=1.2)
     setup_s = time.perf_counter() - t0
@@ -248,7 +250,7 @@ def run_ours(args, world, rank, local):
     clk = clocks.stop() if clocks else None
     ms = ev0.elapsed_time(ev1)
     kern = {}
-    for name in ("potrf_trailing_update", "potrf_panel", "potrf_diag", "trsv", "schur_build", "min_eig"):
+    for name in ("potrf_trailing_update", "potrf_trailing_update_tc", "potrf_panel", "potrf_diag", "trsv", "schur_build", "min_eig"):
         t = ctypes.c_double()
         n = ctypes.c_long()
         L.sddd_profile_read(ctx.h, name.encode(), ctypes.byref(t), ctypes.byref(n))
@@ -342,6 +344,8 @@ def profile_case(args):
     dd[:, 0] = A.T.reshape(-1)  # column-major
     del G, A
     with sddd.Context(0) as ctx:
+        if args.tc and L.sddd_set_tc_split(ctx.h, args.tc) != 0:
+            raise RuntimeError(L.sddd_last_error(ctx.h).decode())
         torch.cuda.synchronize()
         t = time.perf_counter()
         info = L.sddd_Rpotrf(ctx.h, m, ctypes.c_void_p(dd.data_ptr()), m)
@@ -359,6 +363,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", choices=["potrf"], help="run one kernel-level case for an ncu capture and exit")
     ap.add_argument("--m", type=int, default=4096)
+    ap.add_argument("--tc", type=int, default=0, help="slices of the tensor-core split Cholesky (8..16; 0 = plain dd)")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case(args)

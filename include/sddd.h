@@ -160,6 +160,20 @@ int sddd_work(const sddd_ctx *ctx, double *schur_ddflops, double *chol_ddflops);
 /* Measured FP64 fused multiply-add throughput of the current device (GFLOP/s). */
 int sddd_fp64_peak(sddd_ctx *ctx, double *gflops);
 
+/* -- tensor-core split (no counterpart in the reference) --
+ * With slices in 8..16 the Cholesky of the Schur matrix B (sddd_schur_factor,
+ * sddd_Rpotrf, whole solves) runs its trailing updates C -= P P^T as
+ * products of signed 7-bit integer slices of the dd operands on the INT8
+ * tensor cores, exact in int32, rebuilt in dd: each value is carried to
+ * 7*slices+1 bits of its row's largest entry (16 slices: 113 bits).  The
+ * diagonal blocks, the panel solves and everything else stay in plain dd.
+ * 0 (the default) keeps the reference's operation order, bit for bit. */
+int sddd_set_tc_split(sddd_ctx *ctx, int slices);
+int sddd_get_tc_split(const sddd_ctx *ctx);
+/* C(i,j) -= sum_k P(i,k) P(j,k) for i >= j (device pointers, column-major,
+ * P n x k with k <= 64) through the same slice products. */
+int sddd_Rsyrk_tc(sddd_ctx *ctx, long n, long k, const sddd_dd *P, long ldp, sddd_dd *C, long ldc, int slices);
+
 /* -- dd kernels on device memory (MPLAPACK-like; pointers are device
  *    pointers to column-major sddd_dd) -- */
 int sddd_Rgemm(sddd_ctx *ctx, char transa, char transb, long m, long n, long k, sddd_dd *A, long lda, sddd_dd *B, long ldb, sddd_dd *C, long ldc);

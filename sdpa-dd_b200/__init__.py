@@ -87,6 +87,9 @@ def lib() -> ctypes.CDLL:
         "sddd_Rgemm": (ci, [vp, cc, cc, cl, cl, cl, vp, cl, vp, cl, vp, cl]),
         "sddd_Rpotrf": (ci, [vp, cl, vp, cl]),
         "sddd_Rtrsv": (ci, [vp, cc, cl, vp, cl, vp]),
+        "sddd_set_tc_split": (ci, [vp, ci]),
+        "sddd_get_tc_split": (ci, [vp]),
+        "sddd_Rsyrk_tc": (ci, [vp, cl, cl, vp, cl, vp, cl, ci]),
         "sddd_dd_op": (ci, [vp, ci, cl, vp, vp, vp]),
         "sddd_host_dd_op": (ci, [ci, cl, vp, vp, vp]),
         "sddd_host_dd_read": (ci, [ctypes.c_char_p, vp]),

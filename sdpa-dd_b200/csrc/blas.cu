@@ -18,6 +18,7 @@
 // The blocking below (tiles, panels) is the B200 schedule; it never
 // reorders the operations that land on one entry.
 #include "blas.h"
+#include "ozaki.h"
 #include "prof.h"
 
 #include <algorithm>
@@ -257,7 +258,7 @@ __global__ void potrf_panel_kernel(dd_t *A, long lda, int n, int nb, int c0, con
 // diagonal block, solve the rows below, then subtract the panel's outer
 // product from the trailing lower triangle (GEMM_SUB keeps each entry's
 // k-order).  info is a device int; 0 on success, else the failing column.
-void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag_dev) {
+void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag_dev, OzakiWork *tc) {
     if (n <= 0) return;
     static bool attr = false;
     const int nbmax = POTRF_NB;
@@ -285,8 +286,13 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
         }
         dd_t *panel = A + (c0 + nb) + lda * (long)c0;
         dd_t *trail = A + (c0 + nb) + lda * (long)(c0 + nb);
-        PROF_SCOPE("potrf_trailing_update", st);
-        gemm(st, 'N', 'T', GEMM_SUB, below, below, nb, panel, lda, 0, panel, lda, 0, trail, lda, 0, 1, true);
+        if (tc) {
+            PROF_SCOPE("potrf_trailing_update_tc", st);
+            ozaki_syrk_sub_lower(st, panel, lda, below, nb, trail, lda, *tc);
+        } else {
+            PROF_SCOPE("potrf_trailing_update", st);
+            gemm(st, 'N', 'T', GEMM_SUB, below, below, nb, panel, lda, 0, panel, lda, 0, trail, lda, 0, 1, true);
+        }
     }
 }
 

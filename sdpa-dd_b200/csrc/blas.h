@@ -5,6 +5,8 @@
 
 namespace sddd {
 
+struct OzakiWork;
+
 enum GemmMode { GEMM_STORE = 0, GEMM_SUB = 1, GEMM_ACC = 2 };
 constexpr int POTRF_NB = 64;
 
@@ -14,8 +16,9 @@ constexpr int POTRF_NB = 64;
 void gemm(cudaStream_t st, char ta, char tb, int mode, int M, int N, int K, const dd_t *A, long lda, long sA, const dd_t *B, long ldb, long sB,
           dd_t *C, long ldc, long sC, int batch, bool lower);
 // In-place lower Cholesky; *info_dev = 0 or the failing 1-based column.
-// rdiag_dev holds POTRF_NB dd of scratch.
-void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag_dev);
+// rdiag_dev holds POTRF_NB dd of scratch.  With tc, the trailing updates
+// run as tensor-core slice products (ozaki.h) instead of dd GEMMs.
+void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag_dev, OzakiWork *tc = nullptr);
 void zero_upper(cudaStream_t st, dd_t *A, long lda, int n);
 // Progress words of the one-launch triangular solve: one flag per 64-entry
 // block (the epoch of the solve that finished it), then an error word.

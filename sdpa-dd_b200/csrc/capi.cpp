@@ -1,6 +1,7 @@
 // extern "C" boundary (include/sddd.h) over the device solver.
 #include "../../include/sddd.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <ctime>
@@ -494,11 +495,40 @@ int sddd_Rpotrf(sddd_ctx *ctx, long n, sddd_dd *A, long lda) {
         if (!c.info.p) c.info.alloc(4);
         if (!c.rdiag.p) c.rdiag.alloc(256);
         CK(cudaMemsetAsync(c.info.p, 0, sizeof(int), c.stream));
-        sddd::potrf(c.stream, reinterpret_cast<dd_t *>(A), lda, (int)n, c.info.p, c.rdiag.p);
+        sddd::OzakiWork *tc = c.tc_slices > 0 ? &sddd::tc_work(c, (int)n, c.tc_slices) : nullptr;
+        sddd::potrf(c.stream, reinterpret_cast<dd_t *>(A), lda, (int)n, c.info.p, c.rdiag.p, tc);
         int info = 0;
         CK(cudaMemcpyAsync(&info, c.info.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
         CK(cudaStreamSynchronize(c.stream));
+        if (tc) sddd::ozaki_check(c.stream, *tc);
         return info;
+    });
+}
+
+int sddd_set_tc_split(sddd_ctx *ctx, int slices) {
+    if (!ctx || !ctx->c) return SDDD_ERR_ARG;
+    if (slices != 0 && (slices < 8 || slices > sddd::OZ_MAX_SLICES)) {
+        ctx->err = "sddd_set_tc_split: slices must be 0 (off) or 8..16";
+        return SDDD_ERR_ARG;
+    }
+    ctx->c->tc_slices = slices;
+    return SDDD_OK;
+}
+
+int sddd_get_tc_split(const sddd_ctx *ctx) { return (ctx && ctx->c) ? ctx->c->tc_slices : SDDD_ERR_ARG; }
+
+int sddd_Rsyrk_tc(sddd_ctx *ctx, long n, long k, const sddd_dd *P, long ldp, sddd_dd *C, long ldc, int slices) {
+    return guarded(ctx, [&] {
+        if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
+        if (n < 0 || k < 0 || k > sddd::OZ_K || ldp < std::max(1L, n) || ldc < std::max(1L, n) || slices < 8 || slices > sddd::OZ_MAX_SLICES)
+            throw sddd::Error(SDDD_ERR_ARG, "sddd_Rsyrk_tc: need 0 <= k <= 64, ld >= n and 8 <= slices <= 16");
+        if (n == 0 || k == 0) return SDDD_OK;
+        sddd::Context &c = *ctx->c;
+        sddd::OzakiWork &w = sddd::tc_work(c, (int)n, slices);
+        sddd::ozaki_syrk_sub_lower(c.stream, reinterpret_cast<const dd_t *>(P), ldp, (int)n, (int)k, reinterpret_cast<dd_t *>(C), ldc, w);
+        sddd::ozaki_check(c.stream, w);
+        if (c.tc_slices > 0) c.tc.slices_used = c.tc_slices;
+        return SDDD_OK;
     });
 }
 

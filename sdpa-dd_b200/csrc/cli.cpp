@@ -31,6 +31,7 @@ void usage(const char *argv0) {
     std::printf("  -o  : output     :: -p  : parameter       \n");
     std::printf("  -pt : parameters , 0 default, 1 fast (unstable)\n");
     std::printf("                     2 slow (stable)         \n");
+    std::printf("  -tc : slices (8-16) of the tensor-core split Cholesky of the Schur matrix\n");
     std::printf("example2-1: %s -o example1.result -dd example1.dat\n", argv0);
     std::printf("example2-2: %s -ds example1.dat-s -o example2.result -p param.sdpa\n", argv0);
     std::printf("example2-3: %s -ds example1.dat-s -o example3.result -pt 2\n", argv0);
@@ -59,6 +60,8 @@ extern "C" int sddd_cli_main(int argc, char **argv) {
     double kappa = 1.2;
     int device = 0;
     if (const char *d = std::getenv("SDDD_DEVICE")) device = std::atoi(d);
+    int tc_slices = 0; // tensor-core split Cholesky of B (this build's extension)
+    if (const char *s = std::getenv("SDDD_TC_SLICES")) tc_slices = std::atoi(s);
     if (argc == 1) {
         usage(argv[0]);
         return 1;
@@ -84,6 +87,8 @@ extern "C" int sddd_cli_main(int argc, char **argv) {
             } else if (!std::strcmp(t, "-pt") && i + 1 < argc) {
                 ptype = pt_type(argv[++i]);
                 paraFile = nullptr;
+            } else if (!std::strcmp(t, "-tc") && i + 1 < argc) {
+                tc_slices = std::atoi(argv[++i]);
             }
         }
     } else {
@@ -134,6 +139,11 @@ extern "C" int sddd_cli_main(int argc, char **argv) {
     int rc = sddd_create(device, &ctx);
     if (rc != SDDD_OK) {
         std::fprintf(stderr, "%s\n", sddd_last_error(nullptr));
+        return 1;
+    }
+    if (tc_slices != 0 && sddd_set_tc_split(ctx, tc_slices) != SDDD_OK) {
+        std::fprintf(stderr, "%s\n", sddd_last_error(ctx));
+        sddd_destroy(ctx);
         return 1;
     }
     struct Closer {

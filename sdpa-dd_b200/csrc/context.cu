@@ -42,6 +42,25 @@ Context::~Context() {
     if (stream) cudaStreamDestroy(stream);
 }
 
+OzakiWork &tc_work(Context &c, int n, int slices) {
+    const int rows = (int)(ceil_div(n, OZ_ROWS_A) * OZ_ROWS_A);
+    if (rows > c.tc.row_cap || !c.tc.slices) {
+        CK(cudaStreamSynchronize(c.stream));
+        c.tc_slice_buf.alloc((size_t)OZ_MAX_SLICES * rows * OZ_K);
+        c.tc_exps.alloc((size_t)rows);
+        if (!c.tc_err.p) {
+            c.tc_err.alloc(1);
+            CK(cudaMemsetAsync(c.tc_err.p, 0, sizeof(int), c.stream));
+        }
+        c.tc.slices = c.tc_slice_buf.p;
+        c.tc.exps = c.tc_exps.p;
+        c.tc.err = c.tc_err.p;
+        c.tc.row_cap = rows;
+    }
+    c.tc.slices_used = slices;
+    return c.tc;
+}
+
 TrsvSync &trsv_sync(Context &c, int n) {
     const int nblk = (int)ceil_div(n, 64);
     if (nblk > c.trsv.capacity || !c.trsv.flags) {

@@ -10,6 +10,7 @@
 
 #include "blas.h"
 #include "common.cuh"
+#include "ozaki.h"
 #include "problem.h"
 
 namespace sddd {
@@ -150,6 +151,12 @@ struct Context {
     DBuf<dd_t> rdiag;
     DBuf<int> trsv_flags; // progress words of the one-launch triangular solve
     TrsvSync trsv;
+    // tensor-core split of the Cholesky trailing updates of B: slices per
+    // value (8..16), 0 = plain dd GEMMs (the reference's operation order)
+    int tc_slices = 0;
+    DBuf<int8_t> tc_slice_buf;
+    DBuf<int> tc_exps, tc_err;
+    OzakiWork tc;
     std::vector<dd_t> h_scal;
     // algorithmic dd-flop counts of one Make_bMat and one Cholesky of B
     double schur_flops = 0, chol_flops = 0;
@@ -161,6 +168,9 @@ void upload_problem(Context &c, Problem &&p);
 void alloc_state(Context &c);
 // The triangular-solve progress words, grown (and zeroed) to cover order n.
 TrsvSync &trsv_sync(Context &c, int n);
+// The split workspace for an order-n factorisation with `slices` slices
+// (grown as needed).
+OzakiWork &tc_work(Context &c, int n, int slices);
 
 // Host<->device for spaces laid out as the C-ABI defines: SDP blocks
 // concatenated, each n_l x n_l column-major.

@@ -164,10 +164,12 @@ void make_rhs(Context &c, bool corrector, dd_t beta_mu, bool dual_infeasible) {
 
 int schur_factor(Context &c) {
     CK(cudaMemsetAsync(c.info.p, 0, sizeof(int), c.stream));
-    potrf(c.stream, c.B.p, c.m, c.m, c.info.p, c.rdiag.p);
+    OzakiWork *tc = c.tc_slices > 0 ? &tc_work(c, c.m, c.tc_slices) : nullptr;
+    potrf(c.stream, c.B.p, c.m, c.m, c.info.p, c.rdiag.p, tc);
     int info = 0;
     CK(cudaMemcpyAsync(&info, c.info.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
+    if (tc) ozaki_check(c.stream, *tc);
     return info;
 }
 

@@ -1,0 +1,31 @@
+// Tensor-core split of the Cholesky trailing update: C(lower) -= P P^T with
+// dd operands cut into signed 7-bit integer slices (an Ozaki-style
+// error-free split) and multiplied on the INT8 tensor cores (tcgen05,
+// kind::i8) with exact int32 accumulation, then rebuilt in dd.
+#pragma once
+#include "common.cuh"
+
+namespace sddd {
+
+constexpr int OZ_MAX_SLICES = 16;
+constexpr int OZ_K = 64;        // panel width the split handles (K of the update)
+constexpr int OZ_ROWS_A = 128;  // output tile rows (MMA M)
+constexpr int OZ_COLS_B = 32;   // output tile columns (MMA N)
+
+// Device workspace of the split: slices for `row_cap` rows (a multiple of
+// 128), row exponents and an error word.
+struct OzakiWork {
+    int8_t *slices = nullptr; // OZ_MAX_SLICES x row_cap x 64 bytes, tiled
+    int *exps = nullptr;      // row_cap
+    int *err = nullptr;       // 0, or the code of a wait that gave up
+    int row_cap = 0;
+    int slices_used = 16;     // 7-bit slices per value (8..16)
+};
+
+// C(i, j) -= sum_k P(i, k) P(j, k) for rows/cols < n with i >= j; P is
+// n x k (k <= 64) column-major with leading dimension ldp, C n x n with ldc.
+void ozaki_syrk_sub_lower(cudaStream_t st, const dd_t *P, long ldp, int n, int k, dd_t *C, long ldc, OzakiWork &w);
+// Throws when a launch since the last check gave up waiting (synchronises st).
+void ozaki_check(cudaStream_t st, const OzakiWork &w);
+
+} // namespace sddd
