@@ -241,6 +241,87 @@ __device__ __forceinline__ double oz_combine(const int32_t *a0, const int32_t *a
     return __ll2double_rn(v) * scale;
 }
 
+// 2^e as a double for -1022 <= e <= 1023 (built from its bits)
+__device__ __forceinline__ double oz_pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+
+// Drains round R (diagonals 2 + 8R .. 9 + 8R) for this thread's 16 columns
+// into the dd accumulator (R = 0 sets it, R = 1 adds to it).
+template <int R>
+__device__ __forceinline__ void oz_drain(const OzArgs &a, uint32_t lane_base, double *acc_hi, double *acc_lo) {
+    constexpr int D0 = 2 + 8 * R;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        double g[2][8];
+#pragma unroll
+        for (int gi = 0; gi < 2; ++gi) {
+            int32_t v[4][8];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int slot = 4 * gi + u;
+                if (D0 + slot <= a.ns + 1) {
+                    tc_ld8(lane_base + (uint32_t)(R * 256 + slot * 32 + 8 * half), v[u]);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) v[u][c] = 0;
+                }
+            }
+            tc_wait_ld();
+            // group value (2^21 A_d + 2^14 A_d+1 + 2^7 A_d+2 + A_d+3) 2^-7(d+3)
+            const double sc = oz_pow2(-7 * (D0 + 4 * gi + 3));
+#pragma unroll
+            for (int c = 0; c < 8; ++c) g[gi][c] = oz_combine(v[0], v[1], v[2], v[3], c, sc);
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int cc = 8 * half + c;
+            double e, s = ddm::two_sum(g[0][c], g[1][c], e); // exact: 72 bits at most
+            if (R == 0) {
+                acc_hi[cc] = s;
+                acc_lo[cc] = e;
+            } else { // accurate dd addition of (s, e)
+                double t1, t2, s2;
+                double s1 = ddm::two_sum(acc_hi[cc], s, s2);
+                t1 = ddm::two_sum(acc_lo[cc], e, t2);
+                s2 += t1;
+                s1 = ddm::fast_two_sum(s1, s2, s2);
+                s2 += t2;
+                acc_hi[cc] = ddm::fast_two_sum(s1, s2, acc_lo[cc]);
+            }
+        }
+    }
+}
+
+// C(i, jb + c) -= 2^(e_i + e_j) acc[c] for c in [c0, c0 + 8) (cv: C prefetched)
+__device__ __forceinline__ void oz_update8(const OzArgs &a, int i, int jb, int c0, int ei, const double *acc_hi, const double *acc_lo,
+                                           const double2 *cv) {
+    const int4 e0 = *reinterpret_cast<const int4 *>(a.exps + jb + c0), e1 = *reinterpret_cast<const int4 *>(a.exps + jb + c0 + 4);
+    const int ej[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const int j = jb + c0 + c;
+        if (i < a.n && j < a.n && j <= i) {
+            const int sc = ei + ej[c];
+            dd_t p;
+            if (sc >= -1022 && sc <= 1023) {
+                const double pw = oz_pow2(sc);
+                p = dd_make(acc_hi[c0 + c] * pw, acc_lo[c0 + c] * pw);
+            } else {
+                p = dd_make(ldexp(acc_hi[c0 + c], sc), ldexp(acc_lo[c0 + c], sc));
+            }
+            const dd_t r = dd_sub(dd_make(cv[c].x, cv[c].y), p);
+            __stcs(reinterpret_cast<double2 *>(a.C + i + a.ldc * (long)j), make_double2(r.hi, r.lo));
+        }
+    }
+}
+
+__device__ __forceinline__ void oz_load8(const OzArgs &a, int i, int jb, int c0, double2 *cv) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const int j = jb + c0 + c;
+        cv[c] = (i < a.n && j < a.n && j <= i) ? __ldcs(reinterpret_cast<const double2 *>(a.C + i + a.ldc * (long)j)) : make_double2(0.0, 0.0);
+    }
+}
+
 __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_end) {
     volatile int *abort_flag = &S.abort_flag;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -249,81 +330,39 @@ __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_e
     const uint32_t lane_base = S.tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(16 * h);
     int I, J;
     oz_tile_at(t_begin, a.nI, a.nJ, I, J);
-    uint32_t nfull[2] = {0, 0};
+    uint32_t ph = 0; // parity of tfull[0] and tfull[1] (they complete in step)
+    // lane 0 waits; the warp follows its outcome (the tensor-memory loads
+    // are warp-collective)
+    auto wait_full = [&](int r) {
+        int okw = 1;
+        if (lane == 0) okw = oz_wait(&S.tfull[r], ph, abort_flag, a.err, 6) ? 1 : 0;
+        return __shfl_sync(0xffffffffu, okw, 0) != 0;
+    };
+    auto release = [&](int r) {
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&S.tempty[r]);
+    };
     for (long t = t_begin; t < t_end; ++t) {
-        double acc_hi[16], acc_lo[16];
-        bool ok = true;
-        for (int r = 0; r < 2; ++r) {
-            // lane 0 waits; the warp follows its outcome (the tensor-memory
-            // loads below are warp-collective)
-            int okw = 1;
-            if (lane == 0) okw = oz_wait(&S.tfull[r], nfull[r] & 1, abort_flag, a.err, 6) ? 1 : 0;
-            ok = __shfl_sync(0xffffffffu, okw, 0) != 0;
-            ++nfull[r];
-            if (!ok) break;
-            tc_fence_after();
-            // 8 columns at a time: the round's 8 diagonals (x8 loads), then
-            // per column the two exact group values and their dd sum
-#pragma unroll
-            for (int half = 0; half < 2; ++half) {
-                double g[2][8];
-#pragma unroll
-                for (int gi = 0; gi < 2; ++gi) {
-                    int32_t v[4][8];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int slot = 4 * gi + u, d = 2 + 8 * r + slot;
-                        if (d <= a.ns + 1) {
-                            tc_ld8(lane_base + (uint32_t)(r * 256 + slot * 32 + 8 * half), v[u]);
-                        } else {
-#pragma unroll
-                            for (int c = 0; c < 8; ++c) v[u][c] = 0;
-                        }
-                    }
-                    tc_wait_ld();
-                    // group value (2^21 A_d0 + ... + A_d0+3) 2^-7(d0+3), d0 = 2 + 8r + 4gi
-                    const double sc = ldexp(1.0, -7 * (2 + 8 * r + 4 * gi + 3));
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) g[gi][c] = oz_combine(v[0], v[1], v[2], v[3], c, sc);
-                }
-#pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                    const int cc = 8 * half + c;
-                    double e, s = ddm::two_sum(g[0][c], g[1][c], e); // exact: 72 bits at most
-                    if (r == 0) {
-                        acc_hi[cc] = s;
-                        acc_lo[cc] = e;
-                    } else { // accurate dd addition of (s, e)
-                        double t1, t2, s2;
-                        double s1 = ddm::two_sum(acc_hi[cc], s, s2);
-                        t1 = ddm::two_sum(acc_lo[cc], e, t2);
-                        s2 += t1;
-                        s1 = ddm::fast_two_sum(s1, s2, s2);
-                        s2 += t2;
-                        acc_hi[cc] = ddm::fast_two_sum(s1, s2, acc_lo[cc]);
-                    }
-                }
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&S.tempty[r]);
-        }
-        if (!ok) break;
         const int i = I * OZ_ROWS_A + row;
         const int jb = J * OZ_COLS_B + 16 * h;
-        if (i < a.n) {
-            const int ei = a.exps[i];
-#pragma unroll
-            for (int c = 0; c < 16; ++c) {
-                const int j = jb + c;
-                if (j < a.n && j <= i) {
-                    const int sc = ei + a.exps[j];
-                    const dd_t p = dd_make(ldexp(acc_hi[c], sc), ldexp(acc_lo[c], sc));
-                    dd_t *cp = a.C + i + a.ldc * (long)j;
-                    st_dd(cp, dd_sub(ld_dd(cp), p));
-                }
-            }
-        }
+        const int ei = a.exps[i]; // scale exponent of the row (padded rows hold 0)
+        double acc_hi[16], acc_lo[16];
+        double2 cv[8];
+        if (!wait_full(0)) break;
+        tc_fence_after();
+        oz_drain<0>(a, lane_base, acc_hi, acc_lo);
+        release(0);
+        if (!wait_full(1)) break;
+        tc_fence_after();
+        oz_drain<1>(a, lane_base, acc_hi, acc_lo);
+        release(1);
+        ph ^= 1u;
+        // the next tile's MMAs run while C is read and written
+        oz_load8(a, i, jb, 0, cv);
+        oz_update8(a, i, jb, 0, ei, acc_hi, acc_lo, cv);
+        oz_load8(a, i, jb, 8, cv);
+        oz_update8(a, i, jb, 8, ei, acc_hi, acc_lo, cv);
         oz_tile_next(a.nJ, I, J);
     }
 }
