@@ -153,17 +153,65 @@ struct OzShared {
     int abort_flag;
 };
 
+// MMAs of round R into its tensor-memory buffer: for each diagonal d of the
+// round, the slice pairs (s, d - s) over the two 32-byte K steps; the first
+// MMA of a diagonal overwrites, the others accumulate.  descA/descB address
+// slice 1 of the A and B operands; slices are OZ_A_BYTES / OZ_B_BYTES apart.
+template <int R, int NS>
+__device__ __forceinline__ void oz_issue_round(uint32_t tmem, uint64_t descA, uint64_t descB) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const int d = 2 + 8 * R + u;
+        if (d <= NS + 1) {
+            const uint32_t dcol = tmem + (uint32_t)(R * 256 + u * 32);
+#pragma unroll
+            for (int s = 1; s <= NS; ++s) {
+                const int t = d - s;
+                if (t >= 1 && t <= NS) {
+#pragma unroll
+                    for (int kk = 0; kk < 2; ++kk) {
+                        const uint64_t da = descA + (uint64_t)(((s - 1) * OZ_A_BYTES + kk * 256) >> 4);
+                        const uint64_t db = descB + (uint64_t)(((t - 1) * OZ_B_BYTES + kk * 256) >> 4);
+                        const int s_first = d - NS > 1 ? d - NS : 1;
+                        tc_mma_i8(dcol, da, db, (s == s_first && kk == 0) ? 0u : 1u);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// The same for a slice count known only at run time.
+__device__ __forceinline__ void oz_issue_round_rt(int r, int ns, uint32_t tmem, uint64_t descA, uint64_t descB) {
+    for (int u = 0; u < 8; ++u) {
+        const int d = 2 + 8 * r + u;
+        if (d > ns + 1) break;
+        const uint32_t dcol = tmem + (uint32_t)(r * 256 + u * 32);
+        uint32_t acc = 0;
+        const int s_lo = max(1, d - ns), s_hi = min(ns, d - 1);
+        for (int s = s_lo; s <= s_hi; ++s) {
+            const int t = d - s;
+            for (int kk = 0; kk < 2; ++kk) {
+                tc_mma_i8(dcol, descA + (uint64_t)(((s - 1) * OZ_A_BYTES + kk * 256) >> 4), descB + (uint64_t)(((t - 1) * OZ_B_BYTES + kk * 256) >> 4),
+                          acc);
+                acc = 1;
+            }
+        }
+    }
+}
+
 __device__ void oz_producer(const OzArgs &a, OzShared &S, uint8_t *smA, uint8_t *smB, long t_begin, long t_end) {
     volatile int *abort_flag = &S.abort_flag;
     int I, J;
     oz_tile_at(t_begin, a.nI, a.nJ, I, J);
-    int In = I, Jn = J;
     auto issue_B = [&](int jb, int buf) {
         mbar_expect_tx(&S.barB[buf], (uint32_t)(a.ns * OZ_B_BYTES));
         for (int s = 0; s < a.ns; ++s)
             bulk_g2s(smB + (size_t)buf * OZ_MAX_SLICES * OZ_B_BYTES + (size_t)s * OZ_B_BYTES, a.slices + s * a.slice_stride + (long)jb * OZ_B_BYTES,
                      OZ_B_BYTES, &S.barB[buf]);
     };
+    const uint64_t descA = oz_desc(smem_u32(smA));
+    const uint64_t descB0 = oz_desc(smem_u32(smB)), descB1 = oz_desc(smem_u32(smB + (size_t)OZ_MAX_SLICES * OZ_B_BYTES));
     // phase parities, one bit per barrier of a pair; pending copies likewise
     uint32_t phA = 0, phB = 0, phFree = 0, phEmpty = 0, pendB = 0;
     int curA = -1;
@@ -174,17 +222,14 @@ __device__ void oz_producer(const OzArgs &a, OzShared &S, uint8_t *smA, uint8_t 
     bool ok = true;
     for (long t = t_begin; t < t_end && ok; ++t, ++n) {
         const int b = (int)(n & 1);
-        if (n >= 1) { // tile n-1 done: its B buffer and the A slices are free
-            ok = oz_wait(&S.bfree[b ^ 1], (phFree >> (b ^ 1)) & 1u, abort_flag, a.err, 1);
-            phFree ^= 1u << (b ^ 1);
-            if (!ok) break;
-        }
-        oz_tile_next(a.nJ, In, Jn);
-        if (t + 1 < t_end) {
-            issue_B(Jn, b ^ 1);
-            pendB |= 1u << (b ^ 1);
-        }
+        bool prev_done = n == 0; // tile n-1 complete (its B buffer and A free)
         if (I != curA) {
+            if (!prev_done) {
+                ok = oz_wait(&S.bfree[b ^ 1], (phFree >> (b ^ 1)) & 1u, abort_flag, a.err, 1);
+                phFree ^= 1u << (b ^ 1);
+                if (!ok) break;
+                prev_done = true;
+            }
             mbar_expect_tx(&S.barA, (uint32_t)(a.ns * OZ_A_BYTES));
             for (int s = 0; s < a.ns; ++s)
                 bulk_g2s(smA + (size_t)s * OZ_A_BYTES, a.slices + s * a.slice_stride + (long)I * OZ_A_BYTES, OZ_A_BYTES, &S.barA);
@@ -199,33 +244,36 @@ __device__ void oz_producer(const OzArgs &a, OzShared &S, uint8_t *smA, uint8_t 
         phB ^= 1u << b;
         if (!ok) break;
         pendB &= ~(1u << b);
-        const uint32_t a_base = smem_u32(smA);
-        const uint32_t b_base = smem_u32(smB + (size_t)b * OZ_MAX_SLICES * OZ_B_BYTES);
+        const uint64_t descB = b ? descB1 : descB0;
         for (int r = 0; r < 2 && ok; ++r) {
             ok = oz_wait(&S.tempty[r], ((phEmpty >> r) & 1u) ^ 1u, abort_flag, a.err, 4);
             phEmpty ^= 1u << r;
             if (!ok) break;
             tc_fence_after();
-            for (int u = 0; u < 8; ++u) {
-                const int d = 2 + 8 * r + u; // slice indices s + t = d (1-based)
-                if (d > a.ns + 1) break;
-                const uint32_t dcol = S.tmem + (uint32_t)(r * 256 + u * 32);
-                uint32_t acc = 0;
-                const int s_lo = max(1, d - a.ns), s_hi = min(a.ns, d - 1);
-                for (int s = s_lo; s <= s_hi; ++s) {
-                    const int tt = d - s;
-                    for (int kk = 0; kk < 2; ++kk) {
-                        const uint64_t da = oz_desc(a_base + (uint32_t)((s - 1) * OZ_A_BYTES + kk * 256));
-                        const uint64_t db = oz_desc(b_base + (uint32_t)((tt - 1) * OZ_B_BYTES + kk * 256));
-                        tc_mma_i8(dcol, da, db, acc);
-                        acc = 1;
-                    }
-                }
+            if (a.ns == OZ_MAX_SLICES) {
+                if (r == 0)
+                    oz_issue_round<0, OZ_MAX_SLICES>(S.tmem, descA, descB);
+                else
+                    oz_issue_round<1, OZ_MAX_SLICES>(S.tmem, descA, descB);
+            } else {
+                oz_issue_round_rt(r, a.ns, S.tmem, descA, descB);
             }
             tc_commit(&S.tfull[r]);
         }
         if (!ok) break;
         tc_commit(&S.bfree[b]);
+        // next tile's B into the other buffer, once tile n-1 has released it
+        int In = I, Jn = J;
+        oz_tile_next(a.nJ, In, Jn);
+        if (t + 1 < t_end) {
+            if (!prev_done) {
+                ok = oz_wait(&S.bfree[b ^ 1], (phFree >> (b ^ 1)) & 1u, abort_flag, a.err, 1);
+                phFree ^= 1u << (b ^ 1);
+                if (!ok) break;
+            }
+            issue_B(Jn, b ^ 1);
+            pendB |= 1u << (b ^ 1);
+        }
         I = In;
         J = Jn;
     }
