@@ -12,6 +12,12 @@ solves), step lengths, update and residuals.  The metric is dd-GFLOP/s of
 the Schur build plus the Cholesky of B (the algorithmic counts of
 sddd_work: m^3/3 for the Cholesky), over the whole step time.
 
+The headline runs the tensor-core split form (--tc, default 16 slices: the
+Cholesky trailing updates as INT8 slice products on tcgen05); the same
+passes in the plain dd form (the reference's operation order, bit for bit)
+are timed beside it ("plain_dd"), and both forms solve the problem from the
+standard initial point to relative gap 1e-25 ("solve_to_gap", wall clock).
+
 One JSON line on rank 0.  Multi-GPU runs are replicas (the single solve
 does not shard): every rank solves its own copy, value sums the ranks' work
 over the slowest rank's time.  --impl reference times the reference build
@@ -193,18 +199,18 @@ def run_reference(args, world, rank):
     return 0
 
 
+KERNELS = ("potrf_trailing_update", "potrf_trailing_update_tc", "potrf_panel", "potrf_diag", "trsv", "schur_build", "min_eig")
+
+
 def run_ours(args, world, rank, local):
     sddd = load_pkg()
     L = sddd.lib()
-    import numpy as np
     import torch
     torch.cuda.set_device(local)
     workdir = pathlib.Path(tempfile.gettempdir()) / f"sddd_bench_{os.getuid()}_{local}"
     workdir.mkdir(exist_ok=True)
     data, param_path = write_workload(WORKLOAD, workdir)
     ctx = sddd.Context(local)
-    if args.tc and L.sddd_set_tc_split(ctx.h, args.tc) != 0:
-        raise RuntimeError(L.sddd_last_error(ctx.h).decode())
     t0 = time.perf_counter()
     ctx.read_problem(data, sparse=True, kappa=1.2)
     setup_s = time.perf_counter() - t0
@@ -214,6 +220,10 @@ def run_ours(args, world, rank, local):
     step_flops = schur.value + chol.value
     par = sddd.param(param_path)
     stream = torch.cuda.ExternalStream(L.sddd_stream(ctx.h))
+
+    def set_tc(slices):
+        if L.sddd_set_tc_split(ctx.h, slices) != 0:
+            raise RuntimeError(L.sddd_last_error(ctx.h).decode())
 
     def restart():
         ctx.call("sddd_solver_start", ctypes.byref(par))
@@ -228,37 +238,42 @@ def run_ours(args, world, rank, local):
             if rc != 0:
                 raise RuntimeError(f"solver stopped at its first iteration (rc={rc})")
 
-    restart()
-    for _ in range(args.warmup):
-        iterate()
-    # ---- device-resident timed region
-    barrier(world)
-    torch.cuda.synchronize()
-    clocks = Clocks(local) if rank == 0 else None
-    L.sddd_profile(ctx.h, 1)
-    L.sddd_profile_reset(ctx.h)
-    launches0 = L.sddd_launch_count()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        iterate()
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    launches = L.sddd_launch_count() - launches0
-    barrier(world)
-    clk = clocks.stop() if clocks else None
-    ms = ev0.elapsed_time(ev1)
-    kern = {}
-    for name in ("potrf_trailing_update", "potrf_trailing_update_tc", "potrf_panel", "potrf_diag", "trsv", "schur_build", "min_eig"):
-        t = ctypes.c_double()
-        n = ctypes.c_long()
-        L.sddd_profile_read(ctx.h, name.encode(), ctypes.byref(t), ctypes.byref(n))
-        kern[name] = (t.value, n.value)
-    L.sddd_profile(ctx.h, 0)
-    ms_max = allmax(world, ms)
+    def timed_passes(steps, warmup, clocks=False):
+        """device time of `steps` main-loop passes (max over ranks), the
+        per-kernel times and the kernel launches inside the region"""
+        restart()
+        for _ in range(warmup):
+            iterate()
+        barrier(world)
+        torch.cuda.synchronize()
+        clk = Clocks(local) if (clocks and rank == 0) else None
+        L.sddd_profile(ctx.h, 1)
+        L.sddd_profile_reset(ctx.h)
+        launches0 = L.sddd_launch_count()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            iterate()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        launches = L.sddd_launch_count() - launches0
+        barrier(world)
+        clk_res = clk.stop() if clk else None
+        kern = {}
+        for name in KERNELS:
+            t = ctypes.c_double()
+            n = ctypes.c_long()
+            L.sddd_profile_read(ctx.h, name.encode(), ctypes.byref(t), ctypes.byref(n))
+            kern[name] = (t.value, n.value)
+        L.sddd_profile(ctx.h, 0)
+        return allmax(world, ev0.elapsed_time(ev1)), kern, launches, clk_res
+
+    # ---- headline: the tensor-core split form, device-resident
+    set_tc(args.tc)
+    ms_max, kern, launches, clk = timed_passes(args.steps, args.warmup, clocks=True)
     value = world * args.steps * step_flops / (ms_max * 1e-3) / 1e9
-    # ---- end to end through the C ABI with host buffers
+    # ---- end to end through the C ABI with host buffers (same form)
     n_space = L.sddd_space_len(ctx.h)
     m = ctx.m
     X = torch.empty(2 * n_space, dtype=torch.float64).pin_memory()
@@ -282,18 +297,73 @@ def run_ours(args, world, rank, local):
     barrier(world)
     e2e_ms = allmax(world, e0.elapsed_time(e1))
     e2e_value = world * args.steps * step_flops / (e2e_ms * 1e-3) / 1e9
-    # ---- roofline of the dominant kernel (Cholesky trailing update)
+    # ---- the plain dd form (the reference's operation order) on the same passes
+    plain = None
+    if args.tc:
+        set_tc(0)
+        p_ms, p_kern, _, _ = timed_passes(args.steps, 1)
+        plain = {"value": world * args.steps * step_flops / (p_ms * 1e-3) / 1e9, "ms_per_step": p_ms / args.steps,
+                 "kernel_ms_per_step": {k: v[0] / args.steps for k, v in p_kern.items()}}
+        set_tc(args.tc)
+    # ---- time to relative gap 1e-25 from the standard initial point
+    solves = None
+    if not args.no_solve:
+        solves = {}
+        for label, slices in (("tc_split", args.tc), ("plain", 0)):
+            if label == "tc_split" and not args.tc:
+                continue
+            set_tc(slices)
+            barrier(world)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            r = ctx.solve(par)
+            torch.cuda.synchronize()
+            dt = allmax(world, (time.perf_counter() - t1) * 1e3) / 1e3
+            solves[label] = {"seconds": dt, "iterations": r.iterations, "phase": sddd.PHASES[r.phase],
+                             "relative_gap": r.relative_gap.hi, "objValPrimal": r.objValPrimal.hi}
+        set_tc(args.tc)
+        if "tc_split" in solves:
+            solves["speedup_tc_over_plain"] = solves["plain"]["seconds"] / solves["tc_split"]["seconds"]
+    # ---- roofline of the dominant kernel
     tr_fl, tr_launch = trailing_flops(m)
-    t_ms, t_n = kern["potrf_trailing_update"]
     fp64 = ctypes.c_double()
     L.sddd_fp64_peak(ctx.h, ctypes.byref(fp64))
-    # one dd multiply-subtract = 2 dd-flops = 20 FP64 instructions
-    peak_dd = fp64.value / 20.0
-    achieved = (tr_fl * args.steps) / (t_ms * 1e-3) / 1e9 if t_ms > 0 else None
-    traffic = None
-    tfile = ROOT / "profiles" / "potrf_trailing_update_traffic.json"
-    if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get("bytes_per_launch")
+    peak_dd = fp64.value / 20.0  # one dd multiply-subtract = 2 dd-flops = 20 FP64 instructions
+    peaks = {}
+    pfile = ROOT / "MEASURED_PEAKS.json"
+    if pfile.exists():
+        peaks = json.loads(pfile.read_text())
+    if args.tc:
+        t_ms, t_n = kern["potrf_trailing_update_tc"]
+        pairs = args.tc * (args.tc + 1) // 2
+        int8_ops = tr_fl * pairs  # entries x 64 (= tr_fl / 2) x pairs x 2 ops
+        achieved = (int8_ops * args.steps) / (t_ms * 1e-3) / 1e12 if t_ms > 0 else None
+        bf16 = peaks.get("bf16_tflops")
+        peak = 2.0 * bf16 if bf16 else 2.0 * 1590.0
+        traffic = None
+        tfile = ROOT / "profiles" / "ozaki_syrk_traffic.json"
+        if tfile.exists():
+            bpe = json.loads(tfile.read_text()).get("bytes_per_entry")
+            if bpe:
+                traffic = bpe * (tr_fl / 128.0) / tr_launch
+        roofline = {"kernel": "potrf_trailing_update_tc (ozaki_split + ozaki_syrk: INT8 slice products on tcgen05)", "bound": "tensor",
+                    "achieved": achieved, "peak": peak, "unit": "TOPS (int8)", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                    "peak_source": ("2 x measured dense bf16 burst (MEASURED_PEAKS.json bf16_tflops %.0f): the part's dense int8 rate is twice its bf16 rate"
+                                    % bf16) if bf16 else "2 x fallback bf16 1590 TFLOP/s",
+                    "slices": args.tc, "pairs": pairs, "launches_per_step": t_n / args.steps, "int8_ops_per_launch": int8_ops / tr_launch,
+                    "dd_equivalent_gflops": (tr_fl * args.steps) / (t_ms * 1e-3) / 1e9 if t_ms > 0 else None,
+                    "plain_fp64_ceiling_dd_gflops": peak_dd}
+    else:
+        t_ms, t_n = kern["potrf_trailing_update"]
+        achieved = (tr_fl * args.steps) / (t_ms * 1e-3) / 1e9 if t_ms > 0 else None
+        traffic = None
+        tfile = ROOT / "profiles" / "potrf_trailing_update_traffic.json"
+        if tfile.exists():
+            traffic = json.loads(tfile.read_text()).get("bytes_per_launch")
+        roofline = {"kernel": "potrf_trailing_update", "bound": "fp64", "achieved": achieved, "peak": peak_dd, "unit": "dd-GFLOP/s",
+                    "frac": (achieved / peak_dd) if achieved and peak_dd else None, "traffic": traffic,
+                    "peak_source": f"measured FP64 FMA rate {fp64.value:.0f} GFLOP/s / 20 FP64 instructions per dd multiply-add pair (2 dd-flops)",
+                    "launches_per_step": t_n / args.steps, "ddflops_per_launch": tr_fl / tr_launch}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -308,17 +378,17 @@ def run_ours(args, world, rank, local):
             "metric": "Schur+Chol dd-GFLOP/s per Newton iteration",
             "value": value, "unit": "dd-GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "dd (f64 pairs)", "data": "synthetic",
+            "dtype": "dd (f64 pairs); Cholesky trailing updates as int8 slice products" if args.tc else "dd (f64 pairs)", "data": "synthetic",
             "config": {"workload": f"theta-shaped SDP nv={WORKLOAD['nv']} p={WORKLOAD['p']} seed={WORKLOAD['seed']}", "m": m,
                        "block": ctx.sizes, "step": "one main-loop pass (predictor+corrector Newton, step length, update)",
+                       "form": f"tensor-core split, {args.tc} slices" if args.tc else "plain dd",
                        "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (Schur matrix %.2f GB)" % (16.0 * m * m / 1e9),
                        "eps": EPS, "setup_s": setup_s},
             "step_ddflops": {"schur": schur.value, "cholesky": chol.value},
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()},
-            "roofline": {"kernel": "potrf_trailing_update", "bound": "fp64", "achieved": achieved, "peak": peak_dd, "unit": "dd-GFLOP/s",
-                         "frac": (achieved / peak_dd) if achieved and peak_dd else None, "traffic": traffic,
-                         "peak_source": f"measured FP64 FMA rate {fp64.value:.0f} GFLOP/s / 20 FP64 instructions per dd multiply-add pair (2 dd-flops)",
-                         "launches_per_step": t_n / args.steps, "ddflops_per_launch": tr_fl / tr_launch},
+            "plain_dd": plain,
+            "solve_to_gap": solves,
+            "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "dd-GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
@@ -363,7 +433,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", choices=["potrf"], help="run one kernel-level case for an ncu capture and exit")
     ap.add_argument("--m", type=int, default=4096)
-    ap.add_argument("--tc", type=int, default=0, help="slices of the tensor-core split Cholesky (8..16; 0 = plain dd)")
+    ap.add_argument("--tc", type=int, default=16, help="slices of the tensor-core split Cholesky (8..16; 0 = plain dd only)")
+    ap.add_argument("--no-solve", action="store_true", help="skip the two solves to relative gap 1e-25")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case(args)
