@@ -153,52 +153,72 @@ void gemm(cudaStream_t st, char ta, char tb, int mode, int M, int N, int K, cons
 // shared memory (lower triangle).  On a non-positive or NaN pivot the
 // 1-based global column goes to *info and the block stops (Rpotrf2's n=1
 // test, mplapack/Rpotrf2.cpp).  1/L(j,j) for the panel goes to rdiag.
-__global__ void potrf_diag_kernel(dd_t *A, long lda, int nb, int c0, int *info, dd_t *rdiag) {
+// Step k: warp 0 takes column k+1 through its step-k update, its pivot
+// (sqrt, reciprocal) and its scaling, while the other warps apply the
+// step-k update to columns k+2 and beyond; one barrier per step.  Every
+// entry sees the same operations in the same order as the column-by-column
+// form: x(i,j) -= L(j,k) L(i,k) for k ascending, then the scaling.
+constexpr int DIAG_THREADS = 1024;
+__global__ void __launch_bounds__(DIAG_THREADS) potrf_diag_kernel(dd_t *A, long lda, int nb, int c0, int *info, dd_t *rdiag) {
     extern __shared__ double2 sm[];
-    double2 *S = sm;                // nb x nb, column-major
-    __shared__ double2 rk;
+    double2 *S = sm; // nb x nb, column-major
     __shared__ int fail;
     if (*info != 0) return;
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     for (int e = tid; e < nb * nb; e += nt) {
         int i = e % nb, j = e / nb;
         S[e] = (i >= j) ? *reinterpret_cast<const double2 *>(A + (c0 + i) + lda * (long)(c0 + j)) : make_double2(0.0, 0.0);
     }
+    if (tid == 0) fail = 0;
     __syncthreads();
-    for (int k = 0; k < nb; ++k) {
-        if (tid == 0) {
-            dd_t d = dd_make(S[k + nb * k].x, S[k + nb * k].y);
+    auto at = [&](int i, int j) -> dd_t {
+        const double2 v = S[i + nb * j];
+        return dd_make(v.x, v.y);
+    };
+    auto put = [&](int i, int j, dd_t x) { S[i + nb * j] = make_double2(x.hi, x.lo); };
+    // warp 0: pivot of column col (sqrt, 1/L) and the scaling below it
+    auto finish_column = [&](int col) {
+        int bad = 0;
+        double rh = 0.0, rl = 0.0;
+        if (lane == 0) {
+            const dd_t d = at(col, col);
             if (dd_le_d(d, 0.0) || dd_isnan(d)) {
+                bad = 1;
                 fail = 1;
-                *info = c0 + k + 1;
+                *info = c0 + col + 1;
             } else {
-                dd_t l = dd_sqrt(d);
-                S[k + nb * k] = make_double2(l.hi, l.lo);
-                dd_t r = dd_div(dd_from(1.0), l);
-                rk = make_double2(r.hi, r.lo);
-                rdiag[k] = r;
-                fail = 0;
+                const dd_t l = dd_sqrt(d);
+                put(col, col, l);
+                const dd_t r = dd_div(dd_from(1.0), l);
+                rdiag[col] = r;
+                rh = r.hi;
+                rl = r.lo;
+            }
+        }
+        if (__shfl_sync(0xffffffffu, bad, 0)) return;
+        const dd_t r = dd_make(__shfl_sync(0xffffffffu, rh, 0), __shfl_sync(0xffffffffu, rl, 0));
+        for (int i = col + 1 + lane; i < nb; i += 32) put(i, col, dd_mul(r, at(i, col)));
+        __syncwarp();
+    };
+    if (warp == 0) finish_column(0);
+    __syncthreads();
+    if (fail) return;
+    for (int k = 0; k + 1 < nb; ++k) {
+        if (warp == 0) {
+            const dd_t l = at(k + 1, k);
+            for (int i = k + 1 + lane; i < nb; i += 32) put(i, k + 1, dd_sub(at(i, k + 1), dd_mul(l, at(i, k))));
+            __syncwarp();
+            finish_column(k + 1);
+        } else {
+            const int w = nb - k - 2;
+            for (int p = tid - 32; p < w * w; p += nt - 32) {
+                const int i = k + 2 + p % w, j = k + 2 + p / w;
+                if (i < j) continue;
+                put(i, j, dd_sub(at(i, j), dd_mul(at(j, k), at(i, k))));
             }
         }
         __syncthreads();
         if (fail) return;
-        const dd_t r = dd_make(rk.x, rk.y);
-        for (int i = k + 1 + tid; i < nb; i += nt) {
-            double2 v = S[i + nb * k];
-            dd_t x = dd_mul(r, dd_make(v.x, v.y));
-            S[i + nb * k] = make_double2(x.hi, x.lo);
-        }
-        __syncthreads();
-        // trailing update of the block: (i, j) with k < j <= i < nb
-        const int w = nb - 1 - k;
-        for (int p = tid; p < w * w; p += nt) {
-            int i = k + 1 + p % w, j = k + 1 + p / w;
-            if (i < j) continue;
-            double2 xi = S[i + nb * k], xj = S[j + nb * k], v = S[i + nb * j];
-            dd_t y = dd_sub(dd_make(v.x, v.y), dd_mul(dd_make(xj.x, xj.y), dd_make(xi.x, xi.y)));
-            S[i + nb * j] = make_double2(y.hi, y.lo);
-        }
-        __syncthreads();
     }
     for (int e = tid; e < nb * nb; e += nt) {
         int i = e % nb, j = e / nb;
@@ -206,16 +226,19 @@ __global__ void potrf_diag_kernel(dd_t *A, long lda, int nb, int c0, int *info, 
     }
 }
 
-// Panel rows below the diagonal block: each CTA takes PR rows and solves
-// them against L11 in shared memory, column by column (Rtrsm "Right",
-// "Lower", "Transpose": x(i,j) -= L(j,k) x(i,k) for k < j, then
-// x(i,j) *= 1/L(j,j)).
-constexpr int PANEL_ROWS = 64;
-__global__ void potrf_panel_kernel(dd_t *A, long lda, int n, int nb, int c0, const int *info, const dd_t *rdiag) {
+// Panel rows below the diagonal block: each CTA takes PANEL_ROWS rows and
+// solves them against L11 in shared memory (Rtrsm "Right", "Lower",
+// "Transpose": x(i,j) -= L(j,k) x(i,k) for k < j, then x(i,j) *= 1/L(j,j)).
+// Each thread owns fixed entries; at step k it subtracts column k's term
+// from its entries right of k and, for column k+1, applies the scaling at
+// once (the entry is final then): one barrier per step.
+constexpr int PANEL_ROWS = 32;
+constexpr int PANEL_THREADS = 512;
+__global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, long lda, int n, int nb, int c0, const int *info, const dd_t *rdiag) {
     extern __shared__ double2 sm[];
-    double2 *L11 = sm;               // nb x nb
-    double2 *P = sm + nb * nb;       // PANEL_ROWS x nb, column-major ld PANEL_ROWS
-    double2 *R = P + PANEL_ROWS * nb; // nb reciprocals
+    double2 *L11 = sm;                 // nb x nb
+    double2 *P = sm + nb * nb;         // PANEL_ROWS x nb, column-major ld PANEL_ROWS
+    double2 *R = P + PANEL_ROWS * nb;  // nb reciprocals
     if (*info != 0) return;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int r0 = c0 + nb + blockIdx.x * PANEL_ROWS;
@@ -231,20 +254,23 @@ __global__ void potrf_panel_kernel(dd_t *A, long lda, int n, int nb, int c0, con
     }
     for (int e = tid; e < nb; e += nt) R[e] = make_double2(rdiag[e].hi, rdiag[e].lo);
     __syncthreads();
-    for (int k = 0; k < nb; ++k) {
-        const dd_t r = dd_make(R[k].x, R[k].y);
-        for (int i = tid; i < rows; i += nt) {
-            double2 v = P[i + PANEL_ROWS * k];
-            dd_t x = dd_mul(r, dd_make(v.x, v.y));
-            P[i + PANEL_ROWS * k] = make_double2(x.hi, x.lo);
+    auto rk = [&](int k) { return dd_make(R[k].x, R[k].y); };
+    // column 0: scaling only
+    for (int e = tid; e < PANEL_ROWS; e += nt)
+        if (e < rows) {
+            const double2 v = P[e];
+            const dd_t x = dd_mul(rk(0), dd_make(v.x, v.y));
+            P[e] = make_double2(x.hi, x.lo);
         }
-        __syncthreads();
-        const int w = nb - 1 - k;
-        for (int e = tid; e < rows * w; e += nt) {
-            int i = e % rows, j = k + 1 + e / rows;
-            double2 ljk = L11[j + nb * k], xik = P[i + PANEL_ROWS * k], v = P[i + PANEL_ROWS * j];
+    __syncthreads();
+    for (int k = 0; k + 1 < nb; ++k) {
+        for (int e = tid; e < PANEL_ROWS * nb; e += nt) {
+            const int i = e % PANEL_ROWS, j = e / PANEL_ROWS;
+            if (j <= k || i >= rows) continue;
+            const double2 ljk = L11[j + nb * k], xik = P[i + PANEL_ROWS * k], v = P[e];
             dd_t y = dd_sub(dd_make(v.x, v.y), dd_mul(dd_make(ljk.x, ljk.y), dd_make(xik.x, xik.y)));
-            P[i + PANEL_ROWS * j] = make_double2(y.hi, y.lo);
+            if (j == k + 1) y = dd_mul(rk(k + 1), y);
+            P[e] = make_double2(y.hi, y.lo);
         }
         __syncthreads();
     }
@@ -273,14 +299,14 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
         const int nb = std::min(nbmax, n - c0);
         {
             PROF_SCOPE("potrf_diag", st);
-            potrf_diag_kernel<<<1, 256, sizeof(double2) * nb * nb, st>>>(A, lda, nb, c0, info_dev, rdiag_dev);
+            potrf_diag_kernel<<<1, DIAG_THREADS, sizeof(double2) * nb * nb, st>>>(A, lda, nb, c0, info_dev, rdiag_dev);
             CK_LAUNCH();
         }
         const int below = n - c0 - nb;
         if (below <= 0) break;
         {
             PROF_SCOPE("potrf_panel", st);
-            potrf_panel_kernel<<<ceil_div(below, PANEL_ROWS), 256, sizeof(double2) * (nb * nb + PANEL_ROWS * nb + nb), st>>>(A, lda, n, nb, c0, info_dev,
+            potrf_panel_kernel<<<ceil_div(below, PANEL_ROWS), PANEL_THREADS, sizeof(double2) * (nb * nb + PANEL_ROWS * nb + nb), st>>>(A, lda, n, nb, c0, info_dev,
                                                                                                                           rdiag_dev);
             CK_LAUNCH();
         }
