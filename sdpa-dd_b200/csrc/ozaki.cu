@@ -23,8 +23,8 @@
 // it walks the columns).  Warp 0 lane 0 stages operands with bulk copies
 // (cp.async.bulk, no multicast) and issues the MMAs; warps 1-8 drain tensor
 // memory.  Tensor memory holds two rounds of eight diagonal accumulators
-// (8 x 32 columns each): round 0 (d = 2..9) of the next tile is issued while
-// round 1 (d = 10..17) of the current one is being drained.
+// (8 x 32 columns each): round 0 (d = 10..17) of the next tile is issued
+// while round 1 (d = 2..9) of the current one is being drained.
 // Operand layout in global and shared memory: per slice, 8-row groups of
 // 512 bytes, each four 128-byte core matrices (8 rows x 16 K-bytes): the
 // K-major, non-swizzled canonical layout of the MMA's shared-memory
@@ -117,6 +117,11 @@ __device__ __forceinline__ uint64_t oz_desc(uint32_t saddr) {
     return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(512 >> 4) << 32) | (1ull << 46);
 }
 
+// First diagonal of round r.  Round 0 takes the small diagonals 10..17 (200
+// of the 272 MMAs of a 16-slice tile), round 1 the large ones 2..9: the
+// epilogue's C update then overlaps the long round 0 of the next tile.
+__host__ __device__ constexpr int oz_round_d0(int r) { return r == 0 ? 10 : 2; }
+
 struct OzArgs {
     const int8_t *slices;
     long slice_stride; // bytes between slices
@@ -161,7 +166,7 @@ template <int R, int NS>
 __device__ __forceinline__ void oz_issue_round(uint32_t tmem, uint64_t descA, uint64_t descB) {
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-        const int d = 2 + 8 * R + u;
+        const int d = oz_round_d0(R) + u;
         if (d <= NS + 1) {
             const uint32_t dcol = tmem + (uint32_t)(R * 256 + u * 32);
 #pragma unroll
@@ -184,7 +189,7 @@ __device__ __forceinline__ void oz_issue_round(uint32_t tmem, uint64_t descA, ui
 // The same for a slice count known only at run time.
 __device__ __forceinline__ void oz_issue_round_rt(int r, int ns, uint32_t tmem, uint64_t descA, uint64_t descB) {
     for (int u = 0; u < 8; ++u) {
-        const int d = 2 + 8 * r + u;
+        const int d = oz_round_d0(r) + u;
         if (d > ns + 1) break;
         const uint32_t dcol = tmem + (uint32_t)(r * 256 + u * 32);
         uint32_t acc = 0;
@@ -292,11 +297,11 @@ __device__ __forceinline__ double oz_combine(const int32_t *a0, const int32_t *a
 // 2^e as a double for -1022 <= e <= 1023 (built from its bits)
 __device__ __forceinline__ double oz_pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
 
-// Drains round R (diagonals 2 + 8R .. 9 + 8R) for this thread's 16 columns
+// Drains round R (its 8 diagonals from oz_round_d0(R)) for this thread's 16 columns
 // into the dd accumulator (R = 0 sets it, R = 1 adds to it).
 template <int R>
 __device__ __forceinline__ void oz_drain(const OzArgs &a, uint32_t lane_base, double *acc_hi, double *acc_lo) {
-    constexpr int D0 = 2 + 8 * R;
+    constexpr int D0 = oz_round_d0(R);
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
         double g[2][8];
