@@ -126,7 +126,8 @@ int sddd_residuals(sddd_ctx *ctx, sddd_dd *norm_primal, sddd_dd *norm_dual);
 /* Inner products: 0 C.X, 1 b.y, 2 X.Z, 3 C.Dx, 4 b.Dy, 5 X.Dz, 6 Dx.Z, 7 Dx.Dz */
 int sddd_inner(sddd_ctx *ctx, int which, sddd_dd *out);
 /* Device arrays to host: 0 X 1 Z 2 y 3 invCholX 4 invCholZ 5 invZ 6 B
- * 7 g 8 Dx 9 Dy 10 Dz 11 dual residual 12 primal residual.  Returns the
+ * 7 g 8 Dx 9 Dy 10 Dz 11 dual residual 12 primal residual, after
+ * sddd_adjoint 13 its u 14 its R.  Returns the
  * number of dd written (with out == NULL: the number it would write). */
 long sddd_get(sddd_ctx *ctx, int what, sddd_dd *out);
 int sddd_set(sddd_ctx *ctx, int what, const sddd_dd *in);
@@ -142,6 +143,34 @@ int sddd_iterate(sddd_ctx *ctx);
 int sddd_solver_result(sddd_ctx *ctx, sddd_result *out);
 /* The reference's command line (sdpa_main.cpp:493-672). */
 int sddd_cli_main(int argc, char **argv);
+
+/* -- adjoint of a finished solve (no counterpart in the reference) --
+ * Gradients with respect to the file's data c, F_0, F_1..F_m at the
+ * context's current iterate (normally where sddd_solve stopped), for
+ * weights on the outputs: g_x on x (m), g_Y on Y and g_X on X (block
+ * spaces), g_obj on the optimal value c.x; host arrays, NULL = zero.
+ * It differentiates the central-path equations at the iterate (the same
+ * HKM linearisation the solver's Schur matrix B comes from), builds and
+ * factors B there and solves with it once; as the gap goes to zero the
+ * result tends to the derivative of the optimal solution, and for g_obj to
+ * the envelope gradient (x, Y, -x_k Y).  A matrix gradient G is the
+ * symmetric one: d(value) = sum_ij G_ij dF_ij for a symmetric change dF
+ * (an off-diagonal entry listed once in the file moves F_ij and F_ji, so
+ * its derivative is 2 G_ij).  Outputs: grad_c (m) and grad_F0 (block space),
+ * each may be NULL.  Returns > 0 (failing column) when B is not positive
+ * definite at the iterate.  Overwrites the Newton direction and B.
+ * Accuracy: for g_obj the result agrees with sixth-order finite
+ * differences of whole solves to ~1e-20 and with the envelope gradient to
+ * ~1e-19 at gap 1e-25.  The weights on x, Y and X give the linearisation at
+ * the iterate itself: the solver stops off the central path, and there the
+ * HKM form couples the range and null spaces of X differently from the
+ * optimum, so these solution gradients can differ from the optimal
+ * solution's derivative by 1e-6 (Y) to 1e-1 (x) relative.
+ * sddd_adjoint_grad_F then gives the gradient for F_k, k = 1..m, from the
+ * same adjoint.  sddd_get 13 and 14 return its vector u = B^-1 (...) and
+ * the matrix R (grad_F0 = -R, grad_F_k = -u_k Y + x_k R). */
+int sddd_adjoint(sddd_ctx *ctx, const sddd_dd *g_x, const sddd_dd *g_Y, const sddd_dd *g_X, sddd_dd g_obj, sddd_dd *grad_c, sddd_dd *grad_F0);
+int sddd_adjoint_grad_F(sddd_ctx *ctx, int k, sddd_dd *grad_Fk);
 
 /* -- measurement -- */
 /* Kernels this library has launched in this process so far. */

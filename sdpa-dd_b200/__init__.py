@@ -101,6 +101,8 @@ def lib() -> ctypes.CDLL:
         "sddd_profile_reset": (ci, [vp]),
         "sddd_work": (ci, [vp, ctypes.POINTER(cd), ctypes.POINTER(cd)]),
         "sddd_fp64_peak": (ci, [vp, ctypes.POINTER(cd)]),
+        "sddd_adjoint": (ci, [vp, vp, vp, vp, SdddDD, vp, vp]),
+        "sddd_adjoint_grad_F": (ci, [vp, ci, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -122,7 +124,7 @@ class Context:
     """One device context (sddd_create) with its resident problem."""
 
     GET = {"X": 0, "Z": 1, "y": 2, "invCholX": 3, "invCholZ": 4, "invZ": 5, "B": 6, "g": 7, "Dx": 8, "Dy": 9, "Dz": 10,
-           "dualMat": 11, "primalVec": 12}
+           "dualMat": 11, "primalVec": 12, "adj_u": 13, "adj_R": 14}
 
     def __init__(self, device: int = 0):
         self.L = lib()
@@ -155,6 +157,40 @@ class Context:
         self._check(self.L.sddd_dims(self.h, ctypes.byref(m), ctypes.byref(ns), ctypes.byref(nd), _ptr(sizes), 4096), "dims")
         self.m, self.nsdp, self.ndim = m.value, ns.value, nd.value
         self.sizes = [int(x) for x in sizes[: self.nsdp]]
+
+    def _dims(self):
+        m, ns, nd = ctypes.c_int(), ctypes.c_int(), ctypes.c_long()
+        sizes = np.zeros(4096, np.int32)
+        self._check(self.L.sddd_dims(self.h, ctypes.byref(m), ctypes.byref(ns), ctypes.byref(nd), _ptr(sizes), 4096), "dims")
+        self.m, self.nsdp, self.ndim = m.value, ns.value, nd.value
+        self.sizes = [int(x) for x in sizes[: self.nsdp]]
+
+    def upload(self, m, block_struct, b, k, blk, i, j, val, kappa=1.2):
+        """sddd_upload_problem: entries (k, blk, i, j, val) as in a .dat-s
+        file (k = 0 is F_0; 1-based block, row, column); b and val are dd."""
+        bs = np.ascontiguousarray(block_struct, np.int32)
+        b = np.ascontiguousarray(b, DD)
+        k, blk, i, j = (np.ascontiguousarray(a, np.int32) for a in (k, blk, i, j))
+        val = np.ascontiguousarray(val, DD)
+        self._check(self.L.sddd_upload_problem(self.h, int(m), len(bs), _ptr(bs), _ptr(b), len(val), _ptr(k), _ptr(blk), _ptr(i), _ptr(j),
+                                               _ptr(val), kappa), "upload_problem")
+        self._dims()
+
+    def adjoint(self, g_x=None, g_Y=None, g_X=None, g_obj=(0.0, 0.0)):
+        """sddd_adjoint at the current iterate; returns (grad_c, grad_F0)
+        as dd arrays (grad_F0 a block space)."""
+        keep = [None if a is None else np.ascontiguousarray(a, DD) for a in (g_x, g_Y, g_X)]
+        gc = np.zeros(self.m, DD)
+        gF0 = np.zeros(self.L.sddd_space_len(self.h), DD)
+        self._check(self.L.sddd_adjoint(self.h, *[None if a is None else _ptr(a) for a in keep], SdddDD(*g_obj), _ptr(gc), _ptr(gF0)),
+                    "adjoint")
+        return gc, gF0
+
+    def adjoint_grad_F(self, k):
+        """Gradient with respect to F_k (k = 1..m) from the last adjoint."""
+        out = np.zeros(self.L.sddd_space_len(self.h), DD)
+        self._check(self.L.sddd_adjoint_grad_F(self.h, int(k), _ptr(out)), "adjoint_grad_F")
+        return out
 
     def get(self, what):
         w = self.GET[what] if isinstance(what, str) else what

@@ -8,6 +8,7 @@
 #include <memory>
 #include <string>
 
+#include "adjoint.h"
 #include "blas.h"
 #include "capi_internal.h"
 #include "context.h"
@@ -337,6 +338,15 @@ static void *target_of(sddd::Context &c, int what, long &len) {
     case 10: len = L; return c.Dz.buf.p;
     case 11: len = L; return c.dualMat.buf.p;
     case 12: len = c.m; return c.primalVec.p;
+    case 13:
+    case 14:
+        if (!c.adj_valid) throw sddd::Error(SDDD_ERR_STATE, "no adjoint computed");
+        if (what == 13) {
+            len = c.m;
+            return c.adj_u.p;
+        }
+        len = L;
+        return c.adj_R.buf.p;
     default: throw sddd::Error(SDDD_ERR_ARG, "unknown array selector");
     }
 }
@@ -365,6 +375,37 @@ int sddd_set(sddd_ctx *ctx, int what, const sddd_dd *in) {
         void *p = target_of(c, what, len);
         CK(cudaMemcpyAsync(p, in, sizeof(dd_t) * len, cudaMemcpyHostToDevice, c.stream));
         CK(cudaStreamSynchronize(c.stream));
+        return SDDD_OK;
+    });
+}
+
+int sddd_adjoint(sddd_ctx *ctx, const sddd_dd *g_x, const sddd_dd *g_Y, const sddd_dd *g_X, sddd_dd g_obj, sddd_dd *grad_c, sddd_dd *grad_F0) {
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        const int info = sddd::adjoint(c, reinterpret_cast<const dd_t *>(g_x), reinterpret_cast<const dd_t *>(g_Y),
+                                       reinterpret_cast<const dd_t *>(g_X), D(g_obj));
+        if (info != 0) return info;
+        if (grad_c) {
+            sddd::adjoint_grad_c(c, D(g_obj), c.adj_v.p);
+            CK(cudaMemcpyAsync(grad_c, c.adj_v.p, sizeof(dd_t) * c.m, cudaMemcpyDeviceToHost, c.stream));
+        }
+        if (grad_F0) {
+            sddd::adjoint_grad_F0(c, c.adj_T.buf.p);
+            sddd::space_to_host(c, c.adj_T, reinterpret_cast<dd_t *>(grad_F0));
+        }
+        CK(cudaStreamSynchronize(c.stream));
+        return SDDD_OK;
+    });
+}
+
+int sddd_adjoint_grad_F(sddd_ctx *ctx, int k, sddd_dd *grad_Fk) {
+    if (!grad_Fk) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        if (!c.adj_valid) throw sddd::Error(SDDD_ERR_STATE, "no adjoint computed");
+        if (k < 1 || k > c.m) throw sddd::Error(SDDD_ERR_ARG, "constraint index out of range");
+        sddd::adjoint_grad_F(c, k - 1, c.adj_T.buf.p);
+        sddd::space_to_host(c, c.adj_T, reinterpret_cast<dd_t *>(grad_Fk));
         return SDDD_OK;
     });
 }

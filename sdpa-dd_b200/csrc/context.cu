@@ -334,6 +334,7 @@ void upload_problem(Context &c, Problem &&p) {
     c.b.upload(P.b, c.stream);
     alloc_state(c);
     CK(cudaStreamSynchronize(c.stream));
+    c.adj_valid = false;
     c.have_problem = true;
 }
 

@@ -158,6 +158,12 @@ struct Context {
     DBuf<int> tc_exps, tc_err;
     OzakiWork tc;
     std::vector<dd_t> h_scal;
+    // adjoint of the final iterate (adjoint.cu): u = B^-1 (g_y - A(g_Z')),
+    // the symmetric gradient R of the dual constraint's right-hand side,
+    // and work; allocated on first use
+    DBuf<dd_t> adj_u, adj_v, adj_x;
+    Space adj_R, adj_T;
+    bool adj_valid = false;
     // algorithmic dd-flop counts of one Make_bMat and one Cholesky of B
     double schur_flops = 0, chol_flops = 0;
     ~Context();

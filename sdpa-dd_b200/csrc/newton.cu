@@ -37,7 +37,7 @@ __global__ void constraint_inner_kernel(int m, const BlockView *views, const lon
     st_dd(out + i, dd_acc(dd_mul(MONE, ret), dd_mul(ONE, ld_dd(addv + i))));
 }
 
-static void constraint_inner(Context &c, const Space &M, const dd_t *addv, dd_t *out) {
+void constraint_inner(Context &c, const Space &M, const dd_t *addv, dd_t *out) {
     constraint_inner_kernel<<<ceil_div(c.m, 64), 64, 0, c.stream>>>(c.m, c.views.p, c.d_off.p, c.cb_ptr.p, c.cb_block.p, c.cb_t.p, M.buf.p, addv, out);
     CK_LAUNCH();
 }
@@ -72,7 +72,7 @@ __global__ void sum_yA_kernel(BlockView v, const dd_t *y, dd_t *out, int mode, c
     st_dd(out + e, r);
 }
 
-static void sum_yA(Context &c, const dd_t *y, Space &out, int mode, const Space *D, const Space *Z) {
+void sum_yA(Context &c, const dd_t *y, Space &out, int mode, const Space *D, const Space *Z) {
     for (int l = 0; l < c.nSDP; ++l) {
         const BlockDev &bd = *c.blocks[l];
         const long ne = (long)bd.n * bd.n;
@@ -133,7 +133,7 @@ bool compute_inverse(Context &c) {
 }
 
 // ------------------------------------------------------------ Newton step
-static void triple(Context &c, const Space &A, const Space &B, const Space &C, Space &out) {
+void triple(Context &c, const Space &A, const Space &B, const Space &C, Space &out) {
     // Jal::ns_jordan_triple_product: work = A B; out = work C (two Rgemm)
     for (int l = 0; l < c.nSDP; ++l) {
         const int n = c.sizes[l];

@@ -35,4 +35,13 @@ dd_t lambda_trace(Context &c, const Space &s, double lambda);
 // Jal::getMinEigen(L, D) over the SDP blocks (sdpa_jordan.cpp:55-88).
 dd_t min_eig(Context &c, const Space &L, const Space &D);
 
+// Building blocks shared with the adjoint (adjoint.cu):
+// out_k = -(A_k . M) + addv_k (InputData::multi_InnerProductToA, then the
+// callers' "v = -v + w").
+void constraint_inner(Context &c, const Space &M, const dd_t *addv, dd_t *out);
+// out = -sum_k y_k A_k (+ D) (mode 0) or C - Z - sum_k y_k A_k (mode 1).
+void sum_yA(Context &c, const dd_t *y, Space &out, int mode, const Space *D, const Space *Z);
+// out = A B C per block (Jal::ns_jordan_triple_product); uses W2.
+void triple(Context &c, const Space &A, const Space &B, const Space &C, Space &out);
+
 } // namespace sddd
