@@ -147,6 +147,61 @@ def cpu_reference(sample, warmup, steps, threads):
     return {"value": (schur + chol) * len(secs) / sum(secs) / 1e9, "m": out["m"], "threads": out["threads"], "pass_s": secs}, None
 
 
+BATCH = {"count": 256, "seed": 4, "cpu_sample": 8}
+
+
+def batch_measure(sddd, device, rank, world, args):
+    """The batched workload: 256 dense random SDPs (n ~ U[10,80], m ~
+    U[20,200], the dense_random construction), every one solved to relative
+    gap 1e-25 with the gradient of its optimal value with respect to c, on
+    one GPU through sddd_batch_*; beside it the reference build on a seeded
+    sample of the same problems, one single-thread process per core."""
+    P = problems()
+    probs = P.batch(BATCH["count"], seed=BATCH["seed"])
+    workdir = pathlib.Path(tempfile.gettempdir()) / f"sddd_batch_{os.getuid()}_{device}"
+    workdir.mkdir(exist_ok=True)
+    paths = []
+    for q, (n, m, text) in enumerate(probs):
+        path = workdir / f"b{q}.dat-s"
+        if not path.exists():
+            path.write_text(text)
+        paths.append((path, n, m))
+    param_path = P.write_param(str(workdir / "param.sdpa"), eps=EPS, max_iter=200)
+    par = sddd.param(param_path)
+    with sddd.Batch(device) as bt:
+        for path, n, m in paths:
+            bt.add_file(path, m, n * n)
+        barrier(world)
+        t = time.perf_counter()
+        res = bt.solve(par, with_grad=True)
+        dt = allmax(world, time.perf_counter() - t)
+    phases = [sddd.PHASES[r.phase] for r in res]
+    out = {"workload": f"{BATCH['count']} dense random SDPs, n ~ U[10,80], m ~ U[20,200], seed {BATCH['seed']}, gap {EPS:g}, with d(c.x)/dc",
+           "solves_per_s": world * len(res) / dt, "seconds": dt, "pdOPT": phases.count("pdOPT"),
+           "mean_iterations": sum(r.iterations for r in res) / len(res)}
+    exe = ROOT / "oracle" / "_ref" / "sdpa_dd"
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and exe.exists():
+        import concurrent.futures as cf
+        import random
+        pick = random.Random(0).sample(range(len(paths)), BATCH["cpu_sample"])
+        cores = os.cpu_count() or 1
+
+        def run(q):
+            path = paths[q][0]
+            t0 = time.perf_counter()
+            subprocess.run([str(exe), "-ds", str(path), "-o", str(path) + ".ref.out", "-p", param_path], capture_output=True,
+                           env=dict(os.environ, OMP_NUM_THREADS="1"), check=False)
+            return time.perf_counter() - t0
+
+        with cf.ThreadPoolExecutor(max_workers=min(cores, len(pick))) as ex:
+            secs = list(ex.map(run, pick))
+        mean_s = sum(secs) / len(secs)
+        out["cpu_reference"] = {"solves_per_s": cores / mean_s, "cores": cores, "kind": "reference",
+                                "sample": f"oracle/_ref sdpa_dd on {len(pick)} of the problems (seeded pick), one thread each; "
+                                          f"rate = cores / mean single-thread solve time ({mean_s:.2f} s), without gradients"}
+    return out
+
+
 def dist_init(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -364,6 +419,7 @@ def run_ours(args, world, rank, local):
                     "frac": (achieved / peak_dd) if achieved and peak_dd else None, "traffic": traffic,
                     "peak_source": f"measured FP64 FMA rate {fp64.value:.0f} GFLOP/s / 20 FP64 instructions per dd multiply-add pair (2 dd-flops)",
                     "launches_per_step": t_n / args.steps, "ddflops_per_launch": tr_fl / tr_launch}
+    batched = None if args.no_batch else batch_measure(sddd, local, rank, world, args)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -388,6 +444,7 @@ def run_ours(args, world, rank, local):
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()},
             "plain_dd": plain,
             "solve_to_gap": solves,
+            "batched": batched,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "dd-GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -435,6 +492,7 @@ def main():
     ap.add_argument("--m", type=int, default=4096)
     ap.add_argument("--tc", type=int, default=16, help="slices of the tensor-core split Cholesky (8..16; 0 = plain dd only)")
     ap.add_argument("--no-solve", action="store_true", help="skip the two solves to relative gap 1e-25")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched workload (256 small SDPs)")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case(args)

@@ -172,6 +172,32 @@ int sddd_cli_main(int argc, char **argv);
 int sddd_adjoint(sddd_ctx *ctx, const sddd_dd *g_x, const sddd_dd *g_Y, const sddd_dd *g_X, sddd_dd g_obj, sddd_dd *grad_c, sddd_dd *grad_F0);
 int sddd_adjoint_grad_F(sddd_ctx *ctx, int k, sddd_dd *grad_Fk);
 
+/* -- batches of independent problems (no counterpart in the reference) --
+ * Many SDPs solved on one GPU by a pool of `workers` host threads (<= 0:
+ * 32), each with its own context and stream, so the small kernels of many
+ * problems run at once.  Every problem is solved exactly as sddd_solve
+ * solves it (same iterates, bit for bit).  Problems are added from SDPA
+ * text or from memory (the arguments of sddd_read_problem /
+ * sddd_upload_problem); the add calls return the problem's index.
+ * sddd_batch_solve fills results[count] and, with with_grad != 0, the
+ * gradient of each optimal value with respect to its c (sddd_adjoint with
+ * g_obj = 1).  It returns the first problem error (< 0) after solving all
+ * others; sddd_batch_status gives each problem's (0, > 0 failing column of
+ * B at the adjoint, < 0 error).  Points and gradients are kept on the host:
+ * X and Z as block spaces of that problem, y and grad_c of length m. */
+typedef struct sddd_batch sddd_batch;
+int sddd_batch_create(int device, int workers, sddd_batch **out);
+int sddd_batch_destroy(sddd_batch *b);
+const char *sddd_batch_last_error(const sddd_batch *b);
+int sddd_batch_add_file(sddd_batch *b, const char *path, int sparse, double kappa);
+int sddd_batch_add_problem(sddd_batch *b, int m, int nblock, const int *block_struct, const sddd_dd *bvec, long nnz, const int *k, const int *blk,
+                           const int *i, const int *j, const sddd_dd *val, double kappa);
+int sddd_batch_count(const sddd_batch *b);
+int sddd_batch_solve(sddd_batch *b, const sddd_param *param, int with_grad, sddd_result *results);
+int sddd_batch_status(const sddd_batch *b, int index);
+int sddd_batch_get_point(const sddd_batch *b, int index, sddd_dd *X, sddd_dd *y, sddd_dd *Z);
+int sddd_batch_grad_c(const sddd_batch *b, int index, sddd_dd *grad_c);
+
 /* -- measurement -- */
 /* Kernels this library has launched in this process so far. */
 unsigned long long sddd_launch_count(void);

@@ -13,6 +13,10 @@
 #include <mpblas_dd.h>
 #include <mplapack_dd.h>
 
+#include <qd/qd_real.h>
+
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -482,5 +486,110 @@ int ref_phase(void *h) { return (int)((RefSolver *)h)->phase.value; }
 // Phase at the start of the last pass (before the step's updates).
 int ref_phase_at_step(void *h) { return ((RefSolver *)h)->phaseAtStep; }
 int ref_iteration(void *h) { return ((RefSolver *)h)->pIteration; }
+
+} // extern "C"
+
+// ----------------------------------------------------------------------
+// Quad-double (qd_real, QD 2.3.23, ~212 bits) error oracle: the same
+// quantities as the dd path computed in qd_real from the same dd inputs, so
+// that the error of a dd result can be stated against a value 2^-100 more
+// accurate.  qd values cross as 4 doubles per entry.
+namespace {
+inline qd_real ldq(const double *p) { return qd_real(p[0], p[1], p[2], p[3]); }
+inline void stq(double *p, const qd_real &v) {
+    for (int i = 0; i < 4; ++i) p[i] = v.x[i];
+}
+inline qd_real from_dd(const double *p) { return qd_real(dd_real(p[0], p[1])); }
+} // namespace
+
+extern "C" {
+
+// Lower Cholesky of the symmetric n x n dd matrix A (column-major, lower
+// triangle read) in qd; L receives n*n qd values (upper triangle zero).
+// Returns 0 or the 1-based failing column.
+long qd_potrf(long n, const double *A, double *L) {
+    std::vector<qd_real> a((size_t)n * n);
+    for (long j = 0; j < n; ++j)
+        for (long i = 0; i < n; ++i) a[i + n * j] = i >= j ? from_dd(A + 2 * (i + n * j)) : qd_real(0.0);
+    for (long j = 0; j < n; ++j) {
+        qd_real d = a[j + n * j];
+        for (long k = 0; k < j; ++k) d -= a[j + n * k] * a[j + n * k];
+        if (!(d > 0.0)) return j + 1;
+        d = sqrt(d);
+        a[j + n * j] = d;
+        for (long i = j + 1; i < n; ++i) {
+            qd_real v = a[i + n * j];
+            for (long k = 0; k < j; ++k) v -= a[i + n * k] * a[j + n * k];
+            a[i + n * j] = v / d;
+        }
+    }
+    for (size_t e = 0; e < a.size(); ++e) stq(L + 4 * e, a[e]);
+    return 0;
+}
+
+// x = (L L^T)^-1 b in qd for a qd lower factor L and a dd right-hand side.
+void qd_chol_solve(long n, const double *L, const double *b, double *x) {
+    std::vector<qd_real> v(n);
+    for (long i = 0; i < n; ++i) v[i] = from_dd(b + 2 * i);
+    for (long i = 0; i < n; ++i) {
+        for (long k = 0; k < i; ++k) v[i] -= ldq(L + 4 * (i + n * k)) * v[k];
+        v[i] /= ldq(L + 4 * (i + n * i));
+    }
+    for (long i = n - 1; i >= 0; --i) {
+        for (long k = i + 1; k < n; ++k) v[i] -= ldq(L + 4 * (k + n * i)) * v[k];
+        v[i] /= ldq(L + 4 * (i + n * i));
+    }
+    for (long i = 0; i < n; ++i) stq(x + 4 * i, v[i]);
+}
+
+// B_ij = A_j . (X A_i Zi) in qd for m dense symmetric n x n dd matrices A
+// (consecutive, column-major) and dd X, Zi: the Schur matrix of the F1
+// formula (sdpa_newton.cpp:895) without rounding.  B: m*m qd values.
+void qd_schur_dense(long n, long m, const double *A, const double *X, const double *Zi, double *B) {
+    const long nn = n * n;
+    std::vector<qd_real> x(nn), z(nn), a((size_t)m * nn), t(nn), g(nn);
+    for (long e = 0; e < nn; ++e) {
+        x[e] = from_dd(X + 2 * e);
+        z[e] = from_dd(Zi + 2 * e);
+    }
+    for (long e = 0; e < m * nn; ++e) a[e] = from_dd(A + 2 * e);
+    for (long i = 0; i < m; ++i) {
+        const qd_real *ai = a.data() + i * nn;
+        for (long c = 0; c < n; ++c) // t = A_i Zi
+            for (long r = 0; r < n; ++r) {
+                qd_real s = 0.0;
+                for (long k = 0; k < n; ++k) s += ai[r + n * k] * z[k + n * c];
+                t[r + n * c] = s;
+            }
+        for (long c = 0; c < n; ++c) // g = X t
+            for (long r = 0; r < n; ++r) {
+                qd_real s = 0.0;
+                for (long k = 0; k < n; ++k) s += x[r + n * k] * t[k + n * c];
+                g[r + n * c] = s;
+            }
+        for (long j = 0; j < m; ++j) {
+            const qd_real *aj = a.data() + j * nn;
+            qd_real s = 0.0;
+            for (long e = 0; e < nn; ++e) s += aj[e] * g[e];
+            stq(B + 4 * (i + m * j), s);
+        }
+    }
+}
+
+// out[0] = max_e |dd_e - qd_e|, out[1] = max_e |qd_e| (leading doubles),
+// over n entries; with lower != 0 only the lower triangle of the square
+// order-ord matrix counts.
+void qd_maxdiff(long n, const double *dd, const double *qd, int lower, long ord, double *out) {
+    double md = 0.0, mq = 0.0;
+    for (long e = 0; e < n; ++e) {
+        if (lower && (e % ord) < (e / ord)) continue;
+        const qd_real q = ldq(qd + 4 * e);
+        const qd_real d = from_dd(dd + 2 * e) - q;
+        md = std::max(md, std::fabs(d.x[0]));
+        mq = std::max(mq, std::fabs(q.x[0]));
+    }
+    out[0] = md;
+    out[1] = mq;
+}
 
 } // extern "C"

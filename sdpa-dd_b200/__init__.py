@@ -102,6 +102,16 @@ def lib() -> ctypes.CDLL:
         "sddd_work": (ci, [vp, ctypes.POINTER(cd), ctypes.POINTER(cd)]),
         "sddd_fp64_peak": (ci, [vp, ctypes.POINTER(cd)]),
         "sddd_adjoint": (ci, [vp, vp, vp, vp, SdddDD, vp, vp]),
+        "sddd_batch_create": (ci, [ci, ci, ctypes.POINTER(vp)]),
+        "sddd_batch_destroy": (ci, [vp]),
+        "sddd_batch_last_error": (ctypes.c_char_p, [vp]),
+        "sddd_batch_add_file": (ci, [vp, ctypes.c_char_p, ci, cd]),
+        "sddd_batch_add_problem": (ci, [vp, ci, ci, vp, vp, cl, vp, vp, vp, vp, vp, cd]),
+        "sddd_batch_count": (ci, [vp]),
+        "sddd_batch_solve": (ci, [vp, ctypes.POINTER(SdddParam), ci, vp]),
+        "sddd_batch_status": (ci, [vp, ci]),
+        "sddd_batch_get_point": (ci, [vp, ci, vp, vp, vp]),
+        "sddd_batch_grad_c": (ci, [vp, ci, vp]),
         "sddd_adjoint_grad_F": (ci, [vp, ci, vp]),
     }
     for name, (res, args) in sig.items():
@@ -226,6 +236,73 @@ class Context:
         self._check(self.L.sddd_solve(self.h, ctypes.byref(param), None if result_path is None else str(result_path).encode(), int(print_),
                                       ctypes.byref(r)), "solve")
         return r
+
+
+class Batch:
+    """Independent problems solved together on one GPU (sddd_batch_*)."""
+
+    def __init__(self, device: int = 0, workers: int = 0):
+        self.L = lib()
+        h = ctypes.c_void_p()
+        rc = self.L.sddd_batch_create(device, workers, ctypes.byref(h))
+        if rc != 0:
+            raise SdddError(f"sddd_batch_create failed ({rc}): {self.L.sddd_last_error(None).decode()}")
+        self.h = h
+        self.dims = []  # (m, space length) per problem
+
+    def close(self):
+        if self.h:
+            self.L.sddd_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _added(self, rc, m, space_len):
+        if rc < 0:
+            raise SdddError(f"batch add failed ({rc}): {self.L.sddd_batch_last_error(self.h).decode()}")
+        self.dims.append((m, space_len))
+        return rc
+
+    def add_file(self, path, m, space_len, sparse=True, kappa=1.2):
+        return self._added(self.L.sddd_batch_add_file(self.h, str(path).encode(), int(sparse), kappa), m, space_len)
+
+    def add(self, m, block_struct, b, k, blk, i, j, val, kappa=1.2):
+        bs = np.ascontiguousarray(block_struct, np.int32)
+        b = np.ascontiguousarray(b, DD)
+        k, blk, i, j = (np.ascontiguousarray(a, np.int32) for a in (k, blk, i, j))
+        val = np.ascontiguousarray(val, DD)
+        rc = self.L.sddd_batch_add_problem(self.h, int(m), len(bs), _ptr(bs), _ptr(b), len(val), _ptr(k), _ptr(blk), _ptr(i), _ptr(j), _ptr(val),
+                                           kappa)
+        return self._added(rc, int(m), int(sum(abs(int(x)) ** 2 for x in bs if x > 0)))
+
+    def solve(self, param: SdddParam, with_grad=False):
+        res = (SdddResult * len(self.dims))()
+        rc = self.L.sddd_batch_solve(self.h, ctypes.byref(param), int(with_grad), ctypes.cast(res, ctypes.c_void_p))
+        if rc < 0:
+            raise SdddError(f"sddd_batch_solve failed ({rc}): {self.L.sddd_batch_last_error(self.h).decode()}")
+        return list(res)
+
+    def status(self, index):
+        return self.L.sddd_batch_status(self.h, index)
+
+    def point(self, index):
+        m, L = self.dims[index]
+        X, y, Z = np.zeros(L, DD), np.zeros(m, DD), np.zeros(L, DD)
+        rc = self.L.sddd_batch_get_point(self.h, index, _ptr(X), _ptr(y), _ptr(Z))
+        if rc != 0:
+            raise SdddError(f"sddd_batch_get_point failed ({rc})")
+        return X, y, Z
+
+    def grad_c(self, index):
+        out = np.zeros(self.dims[index][0], DD)
+        rc = self.L.sddd_batch_grad_c(self.h, index, _ptr(out))
+        if rc != 0:
+            raise SdddError(f"sddd_batch_grad_c failed ({rc})")
+        return out
 
 
 def param(path=None, type_=0) -> SdddParam:

@@ -30,7 +30,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-ccbin", HOSTCXX,
                 "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-I", str(PKG.parent / "include")]
 LIB_SOURCES = ["prof.cu", "blas.cu", "schur.cu", "newton.cu", "eig.cu", "context.cu", "ddkern.cu", "noalloc.cu", "ozaki.cu", "adjoint.cu",
-               "problem.cpp", "solver.cpp", "capi.cpp", "cli.cpp"]
+               "problem.cpp", "solver.cpp", "capi.cpp", "cli.cpp", "batch.cpp"]
 
 
 def _compile(src: pathlib.Path, obj: pathlib.Path, force: bool) -> str:

@@ -101,8 +101,8 @@ int adjoint(Context &c, const dd_t *g_x, const dd_t *g_Y, const dd_t *g_X, dd_t 
     if (info != 0) return info;
     CK(cudaMemcpyAsync(c.adj_u.p, c.adj_v.p, sizeof(dd_t) * c.m, cudaMemcpyDeviceToDevice, st));
     TrsvSync &sync = trsv_sync(c, c.m);
-    trsv_lower(st, 'N', c.B.p, c.m, c.m, c.adj_u.p, sync);
-    trsv_lower(st, 'T', c.B.p, c.m, c.m, c.adj_u.p, sync);
+    trsv_lower(st, 'N', c.B.p, c.m, c.m, c.adj_u.p, sync, c.shared_gpu);
+    trsv_lower(st, 'T', c.B.p, c.m, c.m, c.adj_u.p, sync, c.shared_gpu);
     trsv_check(st, sync);
     // R_g = g_Z' + sym(X A^T(u) Z^-1) = g_Z' - sym(X (-A^T(u)) Z^-1)
     sum_yA(c, c.adj_u.p, c.Dz, 0, nullptr, nullptr);
@@ -110,7 +110,7 @@ int adjoint(Context &c, const dd_t *g_x, const dd_t *g_Y, const dd_t *g_X, dd_t 
     sym_blocks(c, c.adj_T);
     adj_sub_kernel<<<ceil_div(L, 256), 256, 0, st>>>(L, c.adj_R.buf.p, c.adj_T.buf.p, c.adj_R.buf.p);
     CK_LAUNCH();
-    CK(cudaStreamSynchronize(st));
+    stream_sync(c);
     c.adj_valid = true;
     return 0;
 }
@@ -127,9 +127,8 @@ void adjoint_grad_F0(Context &c, dd_t *out_dev) {
 
 void adjoint_grad_F(Context &c, int k, dd_t *out_dev) {
     dd_t uy[2];
-    CK(cudaMemcpyAsync(&uy[0], c.adj_u.p + k, sizeof(dd_t), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaMemcpyAsync(&uy[1], c.y.p + k, sizeof(dd_t), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaStreamSynchronize(c.stream));
+    d2h(c, &uy[0], c.adj_u.p + k, sizeof(dd_t));
+    d2h(c, &uy[1], c.y.p + k, sizeof(dd_t));
     adj_grad_F_kernel<<<ceil_div(c.space_len, 256), 256, 0, c.stream>>>(c.space_len, uy[0], uy[1], c.X.buf.p, c.adj_R.buf.p, out_dev);
     CK_LAUNCH();
 }

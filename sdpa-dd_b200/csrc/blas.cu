@@ -286,14 +286,16 @@ __global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, lon
 // k-order).  info is a device int; 0 on success, else the failing column.
 void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag_dev, OzakiWork *tc) {
     if (n <= 0) return;
-    static bool attr = false;
+    static thread_local bool attr[64] = {};
     const int nbmax = POTRF_NB;
     const size_t smem_diag = sizeof(double2) * nbmax * nbmax;
     const size_t smem_panel = sizeof(double2) * (nbmax * nbmax + PANEL_ROWS * nbmax + nbmax);
-    if (!attr) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (!attr[dev & 63]) {
         CK(cudaFuncSetAttribute(potrf_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag));
         CK(cudaFuncSetAttribute(potrf_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_panel));
-        attr = true;
+        attr[dev & 63] = true;
     }
     for (int c0 = 0; c0 < n; c0 += nbmax) {
         const int nb = std::min(nbmax, n - c0);
@@ -352,6 +354,7 @@ void zero_upper(cudaStream_t st, dd_t *A, long lda, int n) {
 constexpr int TRSV_B = 64;
 constexpr int TRSV_LD = 65;
 constexpr int TRSV_THREADS = 256;
+constexpr int TRSV_ONE_CTA = 8; // solves of at most 8 blocks (512 entries) run in one CTA
 constexpr size_t TRSV_SMEM = 2 * sizeof(double2) * TRSV_B * TRSV_LD + sizeof(double2) * TRSV_B;
 
 struct TrsvArgs {
@@ -566,7 +569,7 @@ static int trsv_grid_cap(const void *kernel) {
     return per * sms;
 }
 
-void trsv_lower(cudaStream_t st, char trans, const dd_t *L, long lda, int n, dd_t *x, TrsvSync &sync) {
+void trsv_lower(cudaStream_t st, char trans, const dd_t *L, long lda, int n, dd_t *x, TrsvSync &sync, bool shared_gpu) {
     if (n <= 0) return;
     if (trans != 'N' && trans != 'T') throw Error(ERR_ARG, "trsv: trans must be 'N' or 'T'");
     const int nblk = ceil_div(n, TRSV_B);
@@ -581,16 +584,34 @@ void trsv_lower(cudaStream_t st, char trans, const dd_t *L, long lda, int n, dd_
     int &cp = cap[trans == 'N' ? 0 : 1][dev & 63];
     if (cp == 0) cp = trsv_grid_cap(k);
     const int grid = std::min(nblk, cp);
-    void *args[] = {&a};
-    CK(cudaLaunchCooperativeKernel(k, grid, TRSV_THREADS, args, TRSV_SMEM, st));
+    if (shared_gpu && nblk <= TRSV_ONE_CTA) {
+        // a short solve in one CTA, which walks the blocks in order and
+        // never waits on another CTA: an ordinary launch, so it runs beside
+        // other streams' work (a cooperative launch waits for room for its
+        // whole grid); alone on the GPU the cooperative grid is faster
+        if (trans == 'N')
+            trsv_fwd_wave_kernel<<<1, TRSV_THREADS, TRSV_SMEM, st>>>(a);
+        else
+            trsv_bwd_wave_kernel<<<1, TRSV_THREADS, TRSV_SMEM, st>>>(a);
+    } else {
+        void *args[] = {&a};
+        CK(cudaLaunchCooperativeKernel(k, grid, TRSV_THREADS, args, TRSV_SMEM, st));
+    }
     CK_LAUNCH();
 }
 
 void trsv_check(cudaStream_t st, const TrsvSync &sync) {
     if (!sync.flags) return;
     int err = 0;
-    CK(cudaMemcpyAsync(&err, sync.flags + sync.capacity, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    int *h = sync.h_err ? sync.h_err : &err;
+    CK(cudaMemcpyAsync(h, sync.flags + sync.capacity, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (sync.wait_ev) {
+        CK(cudaEventRecord(sync.wait_ev, st));
+        CK(cudaEventSynchronize(sync.wait_ev));
+    } else {
+        CK(cudaStreamSynchronize(st));
+    }
+    err = *h;
     if (err != 0)
         throw Error(ERR_CUDA, "trsv: a block waited more than 2 s for block " + std::to_string(err - 1) + " (solve abandoned)");
 }

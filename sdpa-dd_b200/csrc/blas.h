@@ -27,9 +27,13 @@ struct TrsvSync {
     int *flags = nullptr; // capacity flags + 1 error word
     int capacity = 0;
     int epoch = 0;
+    int *h_err = nullptr; // pinned host word for reading the error word (or null)
+    cudaEvent_t wait_ev = nullptr; // blocking-sync event to wait on (or null: stream sync)
 };
 // x = L^-1 x ('N') or L^-T x ('T'), L lower, as Rtrsv("Lower", trans, "NonUnit").
-void trsv_lower(cudaStream_t st, char trans, const dd_t *L, long lda, int n, dd_t *x, TrsvSync &sync);
+// shared_gpu: other streams keep the GPU busy (a batch worker); short
+// solves then run in one CTA with an ordinary launch.
+void trsv_lower(cudaStream_t st, char trans, const dd_t *L, long lda, int n, dd_t *x, TrsvSync &sync, bool shared_gpu = false);
 // Throws when a solve since the flags were zeroed gave up waiting
 // (synchronises st).
 void trsv_check(cudaStream_t st, const TrsvSync &sync);

@@ -84,12 +84,14 @@ void from_param(const sddd::Param &q, sddd_param *p) {
 inline dd_t D(sddd_dd v) { return dd_make(v.hi, v.lo); }
 inline sddd_dd S(dd_t v) { return sddd_dd{v.hi, v.lo}; }
 
-void fill_result(sddd_ctx *ctx, sddd_result *out) {
-    sddd::Solver &s = *ctx->solver;
+void fill_result(sddd_ctx *ctx, sddd_result *out) { sddd_fill_result(*ctx->solver, ctx->stop_reason, out); }
+} // namespace
+
+void sddd_fill_result(const sddd::Solver &s, int stop_reason, sddd_result *out) {
     std::memset(out, 0, sizeof(*out));
     out->phase = (int)s.phase;
     out->iterations = s.pIteration;
-    out->stop_reason = ctx->stop_reason;
+    out->stop_reason = stop_reason;
     dd_t mean = dd_div_d(dd_add(dd_abs(s.objValPrimal), dd_abs(s.objValDual)), 2.0);
     dd_t gap = dd_abs(dd_sub(s.objValPrimal, s.objValDual));
     out->mu = S(s.mu_current);
@@ -103,7 +105,6 @@ void fill_result(sddd_ctx *ctx, sddd_result *out) {
     out->schur_seconds = s.tm.makebMat;
     out->cholesky_seconds = s.tm.choleskybMat;
 }
-} // namespace
 
 extern "C" {
 
@@ -469,7 +470,7 @@ int sddd_solve(sddd_ctx *ctx, const sddd_param *param, const char *result_path, 
     });
 }
 
-unsigned long long sddd_launch_count(void) { return sddd::g_launches; }
+unsigned long long sddd_launch_count(void) { return sddd::g_launches.load(); }
 
 void *sddd_stream(sddd_ctx *ctx) { return (ctx && ctx->c) ? (void *)ctx->c->stream : nullptr; }
 

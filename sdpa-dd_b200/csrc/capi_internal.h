@@ -10,3 +10,8 @@ int sddd_solve_stream(sddd_ctx *ctx, const sddd_param *param, FILE *disp, FILE *
 // Records the message that sddd_last_error(NULL) returns on this thread
 // (for entry points that take no context).
 void sddd_set_thread_error(const char *msg);
+namespace sddd {
+class Solver;
+}
+// The numbers sddd_solve reports, from a finished solver.
+void sddd_fill_result(const sddd::Solver &s, int stop_reason, sddd_result *out);

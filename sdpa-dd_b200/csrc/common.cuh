@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -39,7 +40,7 @@ inline void cuda_check(cudaError_t e, const char *what, const char *file, int li
 }
 // Kernels launched by this library in this process (every launch site
 // goes through CK_LAUNCH).
-extern unsigned long long g_launches;
+extern std::atomic<unsigned long long> g_launches;
 #define CK(call) ::sddd::cuda_check((call), #call, __FILE__, __LINE__)
 #define CK_LAUNCH()                                                                                                                                  \
     do {                                                                                                                                             \

@@ -3,6 +3,7 @@
 #include "context.h"
 
 #include <algorithm>
+#include <cstring>
 #include <numeric>
 
 namespace sddd {
@@ -39,7 +40,39 @@ BlockView BlockDev::view() const {
 }
 
 Context::~Context() {
+    if (sync_ev) cudaEventDestroy(sync_ev);
     if (stream) cudaStreamDestroy(stream);
+    if (h_pin) cudaFreeHost(h_pin);
+}
+
+void set_shared_gpu(Context &c, bool blocking_waits) {
+    c.shared_gpu = true;
+    if (blocking_waits && !c.sync_ev) CK(cudaEventCreateWithFlags(&c.sync_ev, cudaEventBlockingSync | cudaEventDisableTiming));
+    c.trsv.wait_ev = c.sync_ev;
+    c.tc.wait_ev = c.sync_ev;
+}
+
+void stream_sync(Context &c) {
+    if (c.sync_ev) {
+        CK(cudaEventRecord(c.sync_ev, c.stream));
+        CK(cudaEventSynchronize(c.sync_ev));
+    } else {
+        CK(cudaStreamSynchronize(c.stream));
+    }
+}
+
+void d2h(Context &c, void *dst, const void *src, size_t bytes) {
+    char *d = static_cast<char *>(dst);
+    const char *s = static_cast<const char *>(src);
+    while (bytes > 0) {
+        const size_t chunk = bytes < Context::H_PIN_BYTES ? bytes : Context::H_PIN_BYTES;
+        CK(cudaMemcpyAsync(c.h_pin, s, chunk, cudaMemcpyDeviceToHost, c.stream));
+        stream_sync(c);
+        std::memcpy(d, c.h_pin, chunk);
+        d += chunk;
+        s += chunk;
+        bytes -= chunk;
+    }
 }
 
 OzakiWork &tc_work(Context &c, int n, int slices) {
@@ -55,6 +88,8 @@ OzakiWork &tc_work(Context &c, int n, int slices) {
         c.tc.slices = c.tc_slice_buf.p;
         c.tc.exps = c.tc_exps.p;
         c.tc.err = c.tc_err.p;
+        c.tc.h_err = static_cast<int *>(c.h_pin);
+        c.tc.wait_ev = c.sync_ev;
         c.tc.row_cap = rows;
     }
     c.tc.slices_used = slices;
@@ -67,7 +102,7 @@ TrsvSync &trsv_sync(Context &c, int n) {
         CK(cudaStreamSynchronize(c.stream));
         c.trsv_flags.alloc((size_t)nblk + 1);
         CK(cudaMemsetAsync(c.trsv_flags.p, 0, sizeof(int) * ((size_t)nblk + 1), c.stream));
-        c.trsv = TrsvSync{c.trsv_flags.p, nblk, 0};
+        c.trsv = TrsvSync{c.trsv_flags.p, nblk, 0, static_cast<int *>(c.h_pin), c.sync_ev};
     }
     return c.trsv;
 }
@@ -80,6 +115,7 @@ Context *create_context(int device) {
     auto *c = new Context();
     c->device = device;
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaMallocHost(&c->h_pin, Context::H_PIN_BYTES));
     return c;
 }
 
@@ -305,13 +341,12 @@ void upload_problem(Context &c, Problem &&p) {
     c.off.assign(c.nSDP + 1, 0);
     for (int l = 0; l < c.nSDP; ++l) c.off[l + 1] = c.off[l] + (long)c.sizes[l] * c.sizes[l];
     c.space_len = c.off[c.nSDP];
-    c.blocks.clear();
+    // block objects (and their device buffers) are reused across uploads
+    if ((int)c.blocks.size() > c.nSDP) c.blocks.resize(c.nSDP);
+    while ((int)c.blocks.size() < c.nSDP) c.blocks.emplace_back(new BlockDev());
     c.schur_flops = 0;
     c.chol_flops = (double)c.m * c.m * c.m / 3.0;
-    for (int l = 0; l < c.nSDP; ++l) {
-        c.blocks.emplace_back(new BlockDev());
-        build_block(c, P, l, *c.blocks.back());
-    }
+    for (int l = 0; l < c.nSDP; ++l) build_block(c, P, l, *c.blocks[l]);
     std::vector<BlockView> views;
     for (auto &bd : c.blocks) views.push_back(bd->view());
     c.views.upload(views, c.stream);

@@ -15,11 +15,14 @@
 
 namespace sddd {
 
-// Device buffer owning cudaMalloc'd memory.
+// Device buffer owning cudaMalloc'd memory.  The capacity only grows: a
+// context that takes a smaller problem next keeps its memory, so uploads
+// in a long-lived context (a batch worker) neither allocate nor free
+// (cudaFree would synchronise the whole device).  n is the logical length.
 template <class T>
 struct DBuf {
     T *p = nullptr;
-    size_t n = 0;
+    size_t n = 0, cap = 0;
     DBuf() = default;
     DBuf(const DBuf &) = delete;
     DBuf &operator=(const DBuf &) = delete;
@@ -27,14 +30,17 @@ struct DBuf {
     void release() {
         if (p) cudaFree(p);
         p = nullptr;
-        n = 0;
+        n = cap = 0;
     }
     void alloc(size_t count) {
-        if (count == n && p) return;
+        if (p && count <= cap) {
+            n = count;
+            return;
+        }
         release();
         if (count == 0) return;
         CK(cudaMalloc(&p, sizeof(T) * count));
-        n = count;
+        n = cap = count;
     }
     void upload(const std::vector<T> &v, cudaStream_t st) {
         alloc(v.size());
@@ -115,6 +121,16 @@ struct Space {
 struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
+    bool shared_gpu = false; // a batch worker: other contexts' streams share the GPU
+    // pinned host staging for the small device-to-host reads of the solver
+    // (scalars, status words): a copy into pageable memory goes through the
+    // driver's shared staging path, which ties the streams of concurrent
+    // contexts together
+    static constexpr size_t H_PIN_BYTES = 1 << 16;
+    void *h_pin = nullptr;
+    // with shared_gpu: a blocking-sync event the host waits on instead of
+    // spinning in cudaStreamSynchronize (many workers share the host cores)
+    cudaEvent_t sync_ev = nullptr;
     std::string last_error;
     bool have_problem = false;
     Problem prob;
@@ -150,6 +166,10 @@ struct Context {
     DBuf<int> info;
     DBuf<dd_t> rdiag;
     DBuf<int> trsv_flags; // progress words of the one-launch triangular solve
+    // step-length eigenvalue work: block lists and Lanczos vectors (kept, so
+    // that no call allocates or frees)
+    DBuf<int> eig_ids_big, eig_ids_small;
+    DBuf<dd_t> eig_work;
     TrsvSync trsv;
     // tensor-core split of the Cholesky trailing updates of B: slices per
     // value (8..16), 0 = plain dd GEMMs (the reference's operation order)
@@ -177,6 +197,16 @@ TrsvSync &trsv_sync(Context &c, int n);
 // The split workspace for an order-n factorisation with `slices` slices
 // (grown as needed).
 OzakiWork &tc_work(Context &c, int n, int slices);
+
+// Marks the context as one of many sharing the GPU (a batch worker): short
+// triangular solves in one CTA; with blocking_waits, host waits block on an
+// event instead of spinning (for more workers than host cores).
+void set_shared_gpu(Context &c, bool blocking_waits);
+// Waits for the context's stream (blocking on an event when shared).
+void stream_sync(Context &c);
+// dst <- bytes at device address src, staged through the context's pinned
+// buffer; synchronises the context's stream.
+void d2h(Context &c, void *dst, const void *src, size_t bytes);
 
 // Host<->device for spaces laid out as the C-ABI defines: SDP blocks
 // concatenated, each n_l x n_l column-major.

@@ -339,17 +339,16 @@ dd_t min_eig(Context &c, const Space &L, const Space &D) {
     static_assert(LZ_KMAX >= 64, "Lanczos step bound");
     std::vector<dd_t> vals;
     if (!big.empty()) {
-        DBuf<int> ids;
+        DBuf<int> &ids = c.eig_ids_big;
         ids.upload(big, st);
         long maxn = 0;
         for (int l : big) maxn = std::max<long>(maxn, c.sizes[l]);
-        DBuf<dd_t> work;
+        DBuf<dd_t> &work = c.eig_work;
         work.alloc(5 * maxn * big.size());
         lanczos_kernel<<<(unsigned)big.size(), LZ_THREADS, 0, st>>>(ids.p, c.d_sizes.p, c.d_off.p, L.buf.p, D.buf.p, work.p, 5 * maxn, c.scal.p);
         CK_LAUNCH();
         std::vector<dd_t> h(big.size());
-        CK(cudaMemcpyAsync(h.data(), c.scal.p, sizeof(dd_t) * big.size(), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
+        d2h(c, h.data(), c.scal.p, sizeof(dd_t) * big.size());
         vals.insert(vals.end(), h.begin(), h.end());
     }
     if (!small.empty()) {
@@ -359,13 +358,12 @@ dd_t min_eig(Context &c, const Space &L, const Space &D) {
             gemm(st, 'N', 'T', GEMM_STORE, n, n, n, D.blk(c.off, l), n, 0, L.blk(c.off, l), n, 0, c.W2.blk(c.off, l), n, 0, 1, false);
             gemm(st, 'N', 'N', GEMM_STORE, n, n, n, L.blk(c.off, l), n, 0, c.W2.blk(c.off, l), n, 0, c.W1.blk(c.off, l), n, 0, 1, false);
         }
-        DBuf<int> ids;
+        DBuf<int> &ids = c.eig_ids_small;
         ids.upload(small, st);
         small_min_eig_kernel<<<(unsigned)small.size(), 32, 0, st>>>(ids.p, c.d_sizes.p, c.d_off.p, c.W1.buf.p, c.scal.p + 32);
         CK_LAUNCH();
         std::vector<dd_t> h(small.size());
-        CK(cudaMemcpyAsync(h.data(), c.scal.p + 32, sizeof(dd_t) * small.size(), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
+        d2h(c, h.data(), c.scal.p + 32, sizeof(dd_t) * small.size());
         vals.insert(vals.end(), h.begin(), h.end());
     }
     // blocks in order: re-sort the values by block index

@@ -127,8 +127,7 @@ bool compute_inverse(Context &c) {
         trmm_lt(st, c.invCholZ.blk(c.off, l), n, n, c.invZ.blk(c.off, l), n);
     }
     int info[2];
-    CK(cudaMemcpyAsync(info, c.info.p, sizeof(info), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    d2h(c, info, c.info.p, sizeof(info));
     return info[0] == 0 && info[1] == 0;
 }
 
@@ -167,8 +166,7 @@ int schur_factor(Context &c) {
     OzakiWork *tc = c.tc_slices > 0 ? &tc_work(c, c.m, c.tc_slices) : nullptr;
     potrf(c.stream, c.B.p, c.m, c.m, c.info.p, c.rdiag.p, tc);
     int info = 0;
-    CK(cudaMemcpyAsync(&info, c.info.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaStreamSynchronize(c.stream));
+    d2h(c, &info, c.info.p, sizeof(int));
     if (tc) ozaki_check(c.stream, *tc);
     return info;
 }
@@ -176,8 +174,8 @@ int schur_factor(Context &c) {
 void solve_dy(Context &c) {
     CK(cudaMemcpyAsync(c.Dy.p, c.g.p, sizeof(dd_t) * c.m, cudaMemcpyDeviceToDevice, c.stream));
     TrsvSync &sync = trsv_sync(c, c.m);
-    trsv_lower(c.stream, 'N', c.B.p, c.m, c.m, c.Dy.p, sync);
-    trsv_lower(c.stream, 'T', c.B.p, c.m, c.m, c.Dy.p, sync);
+    trsv_lower(c.stream, 'N', c.B.p, c.m, c.m, c.Dy.p, sync, c.shared_gpu);
+    trsv_lower(c.stream, 'T', c.B.p, c.m, c.m, c.Dy.p, sync, c.shared_gpu);
     trsv_check(c.stream, sync);
 }
 
@@ -191,8 +189,7 @@ void make_dz_dx(Context &c, bool dual_infeasible) {
 // ------------------------------------------------------------ inner products
 static dd_t fetch_sum(Context &c, int nslots) {
     std::vector<dd_t> h(nslots);
-    CK(cudaMemcpyAsync(h.data(), c.scal.p, sizeof(dd_t) * nslots, cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaStreamSynchronize(c.stream));
+    d2h(c, h.data(), c.scal.p, sizeof(dd_t) * nslots);
     dd_t r = dd_zero();
     for (int s = 0; s < nslots; ++s) r = dd_acc(r, h[s]);
     return r;
@@ -252,8 +249,7 @@ void residuals(Context &c, dd_t &normPrimal, dd_t &normDual) {
     maxabs(c.stream, c.primalVec.p, c.m, c.scal.p, c.red.p);
     maxabs(c.stream, c.dualMat.buf.p, c.space_len, c.scal.p + 1, c.red.p + 512);
     dd_t h[2];
-    CK(cudaMemcpyAsync(h, c.scal.p, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaStreamSynchronize(c.stream));
+    d2h(c, h, c.scal.p, sizeof(h));
     normPrimal = h[0];
     normDual = h[1];
 }

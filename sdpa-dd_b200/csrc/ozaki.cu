@@ -543,8 +543,15 @@ void ozaki_syrk_sub_lower(cudaStream_t st, const dd_t *P, long ldp, int n, int k
 void ozaki_check(cudaStream_t st, const OzakiWork &w) {
     if (!w.err) return;
     int err = 0;
-    CK(cudaMemcpyAsync(&err, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    int *h = w.h_err ? w.h_err : &err;
+    CK(cudaMemcpyAsync(h, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (w.wait_ev) {
+        CK(cudaEventRecord(w.wait_ev, st));
+        CK(cudaEventSynchronize(w.wait_ev));
+    } else {
+        CK(cudaStreamSynchronize(st));
+    }
+    err = *h;
     if (err != 0) throw Error(ERR_CUDA, "ozaki: a tensor-core split update gave up waiting (code " + std::to_string(err) + ")");
 }
 

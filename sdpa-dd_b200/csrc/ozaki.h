@@ -18,6 +18,8 @@ struct OzakiWork {
     int8_t *slices = nullptr; // OZ_MAX_SLICES x row_cap x 64 bytes, tiled
     int *exps = nullptr;      // row_cap
     int *err = nullptr;       // 0, or the code of a wait that gave up
+    int *h_err = nullptr;     // pinned host word for reading err (or null)
+    cudaEvent_t wait_ev = nullptr; // blocking-sync event to wait on (or null: stream sync)
     int row_cap = 0;
     int slices_used = 16;     // 7-bit slices per value (8..16)
 };

@@ -4,7 +4,7 @@
 namespace sddd {
 
 thread_local Profiler *g_prof = nullptr;
-unsigned long long g_launches = 0;
+std::atomic<unsigned long long> g_launches{0};
 
 cudaEvent_t Profiler::get() {
     if (!pool.empty()) {

@@ -266,9 +266,21 @@ void schur_build(Context &c) {
             // dense partners
             const int ndense = bd.nc - bd.nsparse;
             if (ndense > 0) {
-                constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4;
-                dim3 grid(ceil_div(ndense, BN), ceil_div(nfg, BM));
-                schur_dense_pairs_kernel<BM, BN, BK, TM, TN><<<grid, (BM / TM) * (BN / TN), 0, st>>>(bv, bd.ownFG.p, nfg, ndense, c.Gbuf.p, bd.dense.p, c.B.p, m);
+                // Every pair is one sequential dot over the n^2 entries.  With
+                // few pairs (small m) 64 x 64 tiles of 16 pairs per thread
+                // leave the GPU nearly idle on long chains; one pair per
+                // thread in 16 x 16 tiles spreads them over many more CTAs.
+                if ((long)ceil_div(ndense, 64) * ceil_div(nfg, 64) >= 2L * 148) {
+                    constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4;
+                    dim3 grid(ceil_div(ndense, BN), ceil_div(nfg, BM));
+                    schur_dense_pairs_kernel<BM, BN, BK, TM, TN>
+                        <<<grid, (BM / TM) * (BN / TN), 0, st>>>(bv, bd.ownFG.p, nfg, ndense, c.Gbuf.p, bd.dense.p, c.B.p, m);
+                } else {
+                    constexpr int BM = 16, BN = 16, BK = 32, TM = 1, TN = 1;
+                    dim3 grid(ceil_div(ndense, BN), ceil_div(nfg, BM));
+                    schur_dense_pairs_kernel<BM, BN, BK, TM, TN>
+                        <<<grid, (BM / TM) * (BN / TN), 0, st>>>(bv, bd.ownFG.p, nfg, ndense, c.Gbuf.p, bd.dense.p, c.B.p, m);
+                }
                 CK_LAUNCH();
             }
             // sparse partners

@@ -27,10 +27,11 @@ struct EvSpan {
     double *acc = nullptr;
 };
 struct EvClock {
+    Context &c;
     cudaStream_t st;
     std::vector<EvSpan> pending;
     std::vector<cudaEvent_t> owned;
-    explicit EvClock(cudaStream_t s) : st(s) {}
+    explicit EvClock(Context &ctx) : c(ctx), st(ctx.stream) {}
     ~EvClock() {
         for (auto e : owned) cudaEventDestroy(e);
     }
@@ -43,7 +44,7 @@ struct EvClock {
     }
     void span(cudaEvent_t a, cudaEvent_t b, double *acc) { pending.push_back({a, b, acc}); }
     void collect() {
-        CK(cudaStreamSynchronize(st));
+        stream_sync(c);
         for (auto &p : pending) {
             float ms = 0;
             CK(cudaEventElapsedTime(&ms, p.a, p.b));
@@ -183,7 +184,7 @@ static dd_t mu_after(const dd_t &mu, const dd_t &aP, const dd_t &aD, const dd_t 
 
 int Solver::step(FILE *display, FILE *out) {
     if (!(phase_update_check() && pIteration < param.maxIteration)) return 1;
-    EvClock clk(c.stream);
+    EvClock clk(c);
     const auto t_iter0 = std::chrono::steady_clock::now();
     // Switch::MehrotraPredictor, DirectionParameter::MehrotraPredictor
     // (sdpa_parts.cpp:487-496, 542-556)
