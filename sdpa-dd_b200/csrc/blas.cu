@@ -397,14 +397,21 @@ __device__ bool trsv_wait(const TrsvArgs &a, int blk) {
 }
 
 // T(i, j) = L(r0 + i, c0 + j) for i, j < 64 (zero outside the matrix).
+// Every thread of [t0, t0 + nt) puts all its 16-byte copies in flight at
+// once (cp.async; a source size of 0 writes zeros) and waits for them, so a
+// tile costs one memory latency rather than one per element; the caller's
+// __syncthreads then publishes the tile.
 __device__ __forceinline__ void trsv_load_tile(double2 *T, const TrsvArgs &a, int r0, int c0, int t0, int nt) {
     for (int e = t0; e < TRSV_B * TRSV_B; e += nt) {
         const int i = e % TRSV_B, j = e / TRSV_B;
         const int gi = r0 + i, gj = c0 + j;
-        double2 v = make_double2(0.0, 0.0);
-        if (gi < a.n && gj < a.n) v = __ldg(reinterpret_cast<const double2 *>(a.L + gi + a.lda * (long)gj));
-        T[i + TRSV_LD * j] = v;
+        const bool in = gi < a.n && gj < a.n;
+        const dd_t *src = in ? a.L + gi + a.lda * (long)gj : a.L;
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(T + i + TRSV_LD * j)), "l"(src),
+                     "r"(in ? 16 : 0)
+                     : "memory");
     }
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
 __device__ __forceinline__ dd_t tile_dd(const double2 *T, int i, int j) {
