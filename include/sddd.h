@@ -159,13 +159,15 @@ int sddd_cli_main(int argc, char **argv);
  * its derivative is 2 G_ij).  Outputs: grad_c (m) and grad_F0 (block space),
  * each may be NULL.  Returns > 0 (failing column) when B is not positive
  * definite at the iterate.  Overwrites the Newton direction and B.
- * Accuracy: for g_obj the result agrees with sixth-order finite
- * differences of whole solves to ~1e-20 and with the envelope gradient to
- * ~1e-19 at gap 1e-25.  The weights on x, Y and X give the linearisation at
- * the iterate itself: the solver stops off the central path, and there the
- * HKM form couples the range and null spaces of X differently from the
- * optimum, so these solution gradients can differ from the optimal
- * solution's derivative by 1e-6 (Y) to 1e-1 (x) relative.
+ * The optimal value's part is the linearisation at the iterate; the part
+ * for weights on x, Y, X is taken at the optimum: the iterate's
+ * eigendecomposition (dd Jacobi) gives exactly central points X_c Z_c =
+ * mu I with its range and null space, the adjoint is evaluated there at
+ * mu = h, 2h, 4h and extrapolated to mu -> 0 (the iterate itself is off the
+ * central path, where the HKM coupling of the two spaces is not the
+ * optimum's).  Accuracy at gap 1e-25, against sixth-order finite
+ * differences of whole solves: ~1e-20 for the optimal value, 1e-18 to 1e-14
+ * for the solution.  SDP blocks up to order 1024.
  * sddd_adjoint_grad_F then gives the gradient for F_k, k = 1..m, from the
  * same adjoint.  sddd_get 13 and 14 return its vector u = B^-1 (...) and
  * the matrix R (grad_F0 = -R, grad_F_k = -u_k Y + x_k R). */

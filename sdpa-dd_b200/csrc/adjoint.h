@@ -12,6 +12,13 @@ namespace sddd {
 // context; returns 0, or the failing column of the Cholesky of B.
 // Overwrites B, Dx, Dz and the work spaces.
 int adjoint(Context &c, const dd_t *g_x, const dd_t *g_Y, const dd_t *g_X, dd_t g_obj);
+// The same at the optimum: the adjoint at exactly central points built
+// from the iterate's eigendecomposition, extrapolated to mu -> 0
+// (adjoint.cu); the solution gradients are those of the optimal solution.
+int adjoint_limit(Context &c, const dd_t *g_x, const dd_t *g_Y, const dd_t *g_X, dd_t g_obj);
+// The adjoint for mixed weights (linear in them): the optimal value's part at
+// the iterate (adjoint), the solution's part at the limit (adjoint_limit).
+int adjoint_combined(Context &c, const dd_t *g_x, const dd_t *g_Y, const dd_t *g_X, dd_t g_obj);
 // Gradients from the stored adjoint (device outputs).
 void adjoint_grad_c(Context &c, dd_t g_obj, dd_t *out_dev);   // m
 void adjoint_grad_F0(Context &c, dd_t *out_dev);              // block space

@@ -111,7 +111,7 @@ void batch_worker(sddd_batch &B, const std::vector<int> &order, std::atomic<int>
             int st = 0;
             if (with_grad) {
                 const dd_t one = dd_make(1.0, 0.0);
-                st = sddd::adjoint(c, nullptr, nullptr, nullptr, one);
+                st = sddd::adjoint_combined(c, nullptr, nullptr, nullptr, one);
                 if (st == 0) {
                     sddd::adjoint_grad_c(c, one, c.adj_v.p);
                     B.grad_c[idx].resize(c.m);

@@ -383,8 +383,8 @@ int sddd_set(sddd_ctx *ctx, int what, const sddd_dd *in) {
 int sddd_adjoint(sddd_ctx *ctx, const sddd_dd *g_x, const sddd_dd *g_Y, const sddd_dd *g_X, sddd_dd g_obj, sddd_dd *grad_c, sddd_dd *grad_F0) {
     return guarded(ctx, [&] {
         sddd::Context &c = need_problem(ctx);
-        const int info = sddd::adjoint(c, reinterpret_cast<const dd_t *>(g_x), reinterpret_cast<const dd_t *>(g_Y),
-                                       reinterpret_cast<const dd_t *>(g_X), D(g_obj));
+        const int info = sddd::adjoint_combined(c, reinterpret_cast<const dd_t *>(g_x), reinterpret_cast<const dd_t *>(g_Y),
+                                                reinterpret_cast<const dd_t *>(g_X), D(g_obj));
         if (info != 0) return info;
         if (grad_c) {
             sddd::adjoint_grad_c(c, D(g_obj), c.adj_v.p);

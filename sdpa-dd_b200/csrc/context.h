@@ -184,6 +184,13 @@ struct Context {
     DBuf<dd_t> adj_u, adj_v, adj_x;
     Space adj_R, adj_T;
     bool adj_valid = false;
+    // the limit at the optimum (adjoint_limit): eigenvectors of X (Q, and
+    // Q with the range first), work, the saved X and Z^-1, the three
+    // central-point adjoints and the null-space inverse K per block
+    Space lim_Q, lim_Qp, lim_T, lim_M, lim_Xs, lim_Zs, lim_R[3];
+    DBuf<dd_t> lim_u[3], lim_lam, lim_K, lim_Kw;
+    DBuf<int> lim_perm, lim_sweeps;
+    DBuf<double> lim_offr;
     // algorithmic dd-flop counts of one Make_bMat and one Cholesky of B
     double schur_flops = 0, chol_flops = 0;
     ~Context();

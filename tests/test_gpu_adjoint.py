@@ -1,5 +1,6 @@
-"""Adjoint of a finished solve (sddd_adjoint) on the GPU: the gradient of
-the optimal value c.x with respect to the data c, F_0, F_k.
+"""Adjoint of a finished solve (sddd_adjoint) on the GPU: gradients of the
+optimal value c.x and of weighted sums of the solution (x, Y) with respect
+to the data c, F_0, F_k.
 
 The reference has no derivative code, so the adjoint is checked against the
 solver itself and against duality theory:
@@ -42,6 +43,9 @@ FD_TOL = 1e-19
 # The sixth-order stencil at h = 6e-5 keeps both that noise (~3e-21) and its
 # truncation error (h^6 ~ 5e-26) near 1e-20.
 FD2_TOL = 1e-11
+# solution gradients (weights on x and Y) vs sixth-order differences:
+# measured 2e-18 to 4e-14
+SOL_TOL = 1e-12
 # central stencils: sum_j coef_j (f(theta + j h) - f(theta - j h)) / (den h)
 CENTRAL2 = ([(1, 1)], 2)                      # truncation h^2 f(3) / 6
 CENTRAL6 = ([(1, 45), (2, -9), (3, 1)], 60)   # truncation h^6 f(7) / 140
@@ -208,6 +212,67 @@ def test_optimal_value_gradient_vs_differences(small, order):
             print(f"FD{order} {kind}[{idx}] iters {iters}: adjoint {float(g):+.16e} fd {float(fd):+.16e} rel {e:.2e}")
             worst = max(worst, e)
         assert worst < tol
+
+
+def _weighted(gx, gY, y, X):
+    """g_x . x + g_Y . Y with x = -y and Y the internal X, in decimals."""
+    s = Decimal(0)
+    for a, v in zip(gx, y):
+        if a:
+            s -= Decimal(float(a)) * _dec(v)
+    for a, v in zip(gY, X):
+        if a:
+            s += Decimal(float(a)) * _dec(v)
+    return s
+
+
+def _fd_f(ctx, w, par, which, f, h, stencil):
+    """Finite-difference derivative of f(r, X, y) of the solution."""
+    coefs, den = stencil
+    acc = Decimal(0)
+    for j, coef in coefs:
+        outs = []
+        for sgn in (1.0, -1.0):
+            b, val = w.b.copy(), w.val.copy()
+            arr, idx = (b, which[1]) if which[0] == "c" else (val, which[1])
+            hi, lo = _two_sum(float(arr["hi"][idx]), sgn * j * h)
+            arr["hi"][idx], arr["lo"][idx] = hi, lo + float(arr["lo"][idx])
+            r, X, y, Z = _solve(ctx, w, par, b, val)
+            outs.append(f(r, X, y))
+        acc += coef * (outs[0] - outs[1])
+    return acc / (Decimal(den) * Decimal(h))
+
+
+@pytest.mark.parametrize("sizes,m", [((12, 6), 60), ((20, 10), 150)])
+def test_solution_gradient_vs_sixth_order_differences(sizes, m):
+    """Weights on the solution: f = g_x . x + g_Y . Y (random dyadic g_x,
+    symmetric g_Y), gradients with respect to entries of c, F_0 and F_k."""
+    sddd = load_pkg()
+    w = Workload(sizes, m, seed=14)
+    rng = np.random.default_rng(5)
+    with tempfile.TemporaryDirectory() as td, sddd.Context(0) as ctx:
+        par = _param(td)
+        r, X, y, Z = _solve(ctx, w, par)
+        gx = np.round(rng.standard_normal(w.m) * 8) / 8
+        gY = np.zeros(len(X))
+        for b_, n in enumerate(w.sizes):
+            S = np.round(rng.standard_normal((n, n)) * 8) / 8
+            gY[int(w.off[b_]):int(w.off[b_ + 1])] = ((S + S.T) / 2).reshape(-1, order="F")
+        gxd, gYd = np.zeros(w.m, DD), np.zeros(len(gY), DD)
+        gxd["hi"], gYd["hi"] = gx, gY
+        gc, gF0 = ctx.adjoint(g_x=gxd, g_Y=gYd)
+        cases = [("c", 3, _dec(gc[3])), ("c", w.m - 1, _dec(gc[w.m - 1])),
+                 ("F", w.entry(0, 0, 4, 4), _dec(gF0[w.space_index(0, 4, 4)])),
+                 ("F", w.entry(0, 1, 1, 3), 2 * _dec(gF0[w.space_index(1, 1, 3)]))]
+        gk = ctx.adjoint_grad_F(7)
+        cases.append(("F", w.entry(7, 0, 2, 5), 2 * _dec(gk[w.space_index(0, 2, 5)])))
+        worst = 0.0
+        for kind, idx, g in cases:
+            fd = _fd_f(ctx, w, par, (kind, idx), lambda r_, X_, y_: _weighted(gx, gY, y_, X_), H6, CENTRAL6)
+            e = _rel(fd, g)
+            print(f"solution FD6 m={w.m} {kind}[{idx}]: adjoint {float(g):+.16e} fd {float(fd):+.16e} rel {e:.2e}")
+            worst = max(worst, e)
+        assert worst < SOL_TOL
 
 
 def test_torch_autograd_function(small):
