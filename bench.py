@@ -157,6 +157,8 @@ def batch_measure(sddd, device, rank, world, args):
     one GPU through sddd_batch_*; beside it the reference build on a seeded
     sample of the same problems, one single-thread process per core."""
     P = problems()
+    import importlib
+    shard = importlib.import_module("sdpa_dd_b200.shard")
     probs = P.batch(BATCH["count"], seed=BATCH["seed"])
     workdir = pathlib.Path(tempfile.gettempdir()) / f"sddd_batch_{os.getuid()}_{device}"
     workdir.mkdir(exist_ok=True)
@@ -168,17 +170,21 @@ def batch_measure(sddd, device, rank, world, args):
         paths.append((path, n, m))
     param_path = P.write_param(str(workdir / "param.sdpa"), eps=EPS, max_iter=200)
     par = sddd.param(param_path)
+    # independent problems shard over ranks by work, no data-path exchange
+    mine = shard.partition_by_work([shard.work_estimate(m, [n]) for _, n, m in paths], world)[rank]
     with sddd.Batch(device) as bt:
-        for path, n, m in paths:
+        for q in mine:
+            path, n, m = paths[q]
             bt.add_file(path, m, n * n)
         barrier(world)
         t = time.perf_counter()
-        res = bt.solve(par, with_grad=True)
+        res = bt.solve(par, with_grad=True) if mine else []
         dt = allmax(world, time.perf_counter() - t)
     phases = [sddd.PHASES[r.phase] for r in res]
     out = {"workload": f"{BATCH['count']} dense random SDPs, n ~ U[10,80], m ~ U[20,200], seed {BATCH['seed']}, gap {EPS:g}, with d(c.x)/dc",
-           "solves_per_s": world * len(res) / dt, "seconds": dt, "pdOPT": phases.count("pdOPT"),
-           "mean_iterations": sum(r.iterations for r in res) / len(res)}
+           "solves_per_s": len(paths) / dt, "seconds": dt, "ranks": world, "pdOPT_rank0": phases.count("pdOPT"),
+           "problems_rank0": len(mine),
+           "mean_iterations_rank0": (sum(r.iterations for r in res) / len(res)) if res else None}
     exe = ROOT / "oracle" / "_ref" / "sdpa_dd"
     if rank == 0 and world == 1 and not args.no_cpu_baseline and exe.exists():
         import concurrent.futures as cf
