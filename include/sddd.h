@@ -132,6 +132,19 @@ int sddd_inner(sddd_ctx *ctx, int which, sddd_dd *out);
 long sddd_get(sddd_ctx *ctx, int what, sddd_dd *out);
 int sddd_set(sddd_ctx *ctx, int what, const sddd_dd *in);
 
+/* -- initial point (the reference's -id / -is files, sdpa_main.cpp:237-251,
+ *    sdpa_io.cpp:152-283) --
+ * The next solves start from it instead of lambda I, with the reference's
+ * initial mu (X.Z / nDim) and its eta bookkeeping (SolveInfo::update with
+ * the initial point).  sddd_read_initial_point reads an init file (sparse
+ * != 0: "target block i j value" lines, target 1 = X, 2 = Y; else dense),
+ * whose unset entries keep lambda I (pass param.lambdaStar, as the
+ * reference starts from it); sddd_set_initial_point takes the file's x (m),
+ * X and Y (block spaces) directly.  A new problem clears it. */
+int sddd_read_initial_point(sddd_ctx *ctx, const char *path, int sparse, double lambda);
+int sddd_set_initial_point(sddd_ctx *ctx, const sddd_dd *x, const sddd_dd *X, const sddd_dd *Y);
+int sddd_clear_initial_point(sddd_ctx *ctx);
+
 /* -- the whole solve (pinpal) -- */
 /* display/result may be NULL.  The result file gets the reference's
  * layout; `display` is the console stream. */

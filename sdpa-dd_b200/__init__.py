@@ -102,6 +102,9 @@ def lib() -> ctypes.CDLL:
         "sddd_work": (ci, [vp, ctypes.POINTER(cd), ctypes.POINTER(cd)]),
         "sddd_fp64_peak": (ci, [vp, ctypes.POINTER(cd)]),
         "sddd_adjoint": (ci, [vp, vp, vp, vp, SdddDD, vp, vp]),
+        "sddd_read_initial_point": (ci, [vp, ctypes.c_char_p, ci, cd]),
+        "sddd_set_initial_point": (ci, [vp, vp, vp, vp]),
+        "sddd_clear_initial_point": (ci, [vp]),
         "sddd_batch_create": (ci, [ci, ci, ctypes.POINTER(vp)]),
         "sddd_batch_destroy": (ci, [vp]),
         "sddd_batch_last_error": (ctypes.c_char_p, [vp]),

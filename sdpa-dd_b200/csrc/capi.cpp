@@ -380,6 +380,47 @@ int sddd_set(sddd_ctx *ctx, int what, const sddd_dd *in) {
     });
 }
 
+static void store_init(sddd::Context &c, const dd_t *X, const dd_t *y, const dd_t *Z) {
+    c.init_X.buf.alloc(c.space_len);
+    c.init_Z.buf.alloc(c.space_len);
+    c.init_y.alloc(c.m);
+    sddd::space_from_host(c, c.init_X, X);
+    sddd::space_from_host(c, c.init_Z, Z);
+    CK(cudaMemcpyAsync(c.init_y.p, y, sizeof(dd_t) * c.m, cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    c.has_init = true;
+}
+
+int sddd_read_initial_point(sddd_ctx *ctx, const char *path, int sparse, double lambda) {
+    if (!path) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        std::vector<dd_t> X, y, Z;
+        sddd::read_init_point(path, sparse != 0, c.prob, lambda, X, y, Z);
+        store_init(c, X.data(), y.data(), Z.data());
+        return SDDD_OK;
+    });
+}
+
+int sddd_set_initial_point(sddd_ctx *ctx, const sddd_dd *x, const sddd_dd *X, const sddd_dd *Y) {
+    if (!x || !X || !Y) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        std::vector<dd_t> y(c.m);
+        for (int k = 0; k < c.m; ++k) y[k] = dd_neg(D(x[k])); // the internal y is -x
+        // the internal X is the file's Y, the internal Z its X
+        store_init(c, reinterpret_cast<const dd_t *>(Y), y.data(), reinterpret_cast<const dd_t *>(X));
+        return SDDD_OK;
+    });
+}
+
+int sddd_clear_initial_point(sddd_ctx *ctx) {
+    return guarded(ctx, [&] {
+        need_problem(ctx).has_init = false;
+        return SDDD_OK;
+    });
+}
+
 int sddd_adjoint(sddd_ctx *ctx, const sddd_dd *g_x, const sddd_dd *g_Y, const sddd_dd *g_X, sddd_dd g_obj, sddd_dd *grad_c, sddd_dd *grad_F0) {
     return guarded(ctx, [&] {
         sddd::Context &c = need_problem(ctx);

@@ -54,7 +54,7 @@ extern "C" int sddd_cli_main(int argc, char **argv) {
     time_t ltime;
     std::time(&ltime);
     std::printf("SDPA-DD start at    %s", std::ctime(&ltime));
-    bool isInitFile = false, isDataSparse = false;
+    bool isInitFile = false, isInitSparse = false, isDataSparse = false;
     const char *dataFile = nullptr, *initFile = nullptr, *outFile = nullptr, *paraFile = nullptr;
     int ptype = 0;
     double kappa = 1.2;
@@ -75,6 +75,7 @@ extern "C" int sddd_cli_main(int argc, char **argv) {
                 dataFile = argv[++i];
                 isDataSparse = true;
             } else if ((!std::strcmp(t, "-id") || !std::strcmp(t, "-is")) && i + 1 < argc) {
+                isInitSparse = !std::strcmp(t, "-is");
                 initFile = argv[++i];
                 isInitFile = true;
             } else if (!std::strcmp(t, "-o") && i + 1 < argc) {
@@ -103,6 +104,7 @@ extern "C" int sddd_cli_main(int argc, char **argv) {
             } else {
                 initFile = argv[i];
                 isInitFile = true;
+                isInitSparse = ends_with_s(initFile);
             }
         }
     }
@@ -116,10 +118,6 @@ extern "C" int sddd_cli_main(int argc, char **argv) {
     if (initFile) std::printf("initial   is %s\n", initFile);
     else std::printf("\n");
     if (!paraFile) std::printf("set       is %s\n", ptype == 0 ? "DEFAULT" : ptype == 1 ? "UNSTABLE_BUT_FAST" : "STABLE_BUT_SLOW");
-    if (isInitFile) {
-        std::fprintf(stderr, "initial point files are not supported by this build\n");
-        return 1;
-    }
     // pinpal
     const auto t0 = std::chrono::steady_clock::now();
     FILE *fo = std::fopen(outFile, "w");
@@ -160,12 +158,18 @@ extern "C" int sddd_cli_main(int argc, char **argv) {
     for (auto &cm : prob.comments) std::fprintf(fo, "%s\n", cm.c_str());
     std::fprintf(fo, "data      is %s\n", dataFile);
     if (paraFile) std::fprintf(fo, "parameter is %s\n", paraFile);
+    if (initFile) std::fprintf(fo, "initial   is %s\n", initFile);
     std::fprintf(fo, "out       is %s\n", outFile);
     try {
         sddd::finalize_problem(prob, kappa);
         sddd_attach_problem(ctx, std::move(prob));
     } catch (const sddd::Error &e) {
         std::printf("%s\n", e.what());
+        std::fclose(fo);
+        return 1;
+    }
+    if (isInitFile && sddd_read_initial_point(ctx, initFile, isInitSparse ? 1 : 0, param.lambdaStar) != SDDD_OK) {
+        std::printf("%s\n", sddd_last_error(ctx));
         std::fclose(fo);
         return 1;
     }

@@ -370,6 +370,7 @@ void upload_problem(Context &c, Problem &&p) {
     alloc_state(c);
     CK(cudaStreamSynchronize(c.stream));
     c.adj_valid = false;
+    c.has_init = false;
     c.have_problem = true;
 }
 

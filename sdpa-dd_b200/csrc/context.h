@@ -178,6 +178,11 @@ struct Context {
     DBuf<int> tc_exps, tc_err;
     OzakiWork tc;
     std::vector<dd_t> h_scal;
+    // a user-given initial point (the reference's -id / -is), used by the
+    // solver's start in place of lambda I
+    bool has_init = false;
+    Space init_X, init_Z;
+    DBuf<dd_t> init_y;
     // adjoint of the final iterate (adjoint.cu): u = B^-1 (g_y - A(g_Z')),
     // the symmetric gradient R of the dual constraint's right-hand side,
     // and work; allocated on first use

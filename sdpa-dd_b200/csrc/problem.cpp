@@ -268,6 +268,65 @@ Problem read_problem(const std::string &path, bool sparse) {
     return read_problem_text(ss.str(), sparse);
 }
 
+void read_init_point_text(const std::string &text, bool sparse, const Problem &P, double lambda, std::vector<dd_t> &X, std::vector<dd_t> &y,
+                          std::vector<dd_t> &Z) {
+    if (P.nLP > 0) throw Error(ERR_UNSUPPORTED, "initial point: LP blocks are not supported by the device path yet");
+    std::vector<long> off(P.nSDP + 1, 0);
+    for (int l = 0; l < P.nSDP; ++l) off[l + 1] = off[l] + (long)P.sdpSize[l] * P.sdpSize[l];
+    X.assign(off[P.nSDP], dd_zero());
+    Z.assign(off[P.nSDP], dd_zero());
+    for (int l = 0; l < P.nSDP; ++l) {
+        const int n = P.sdpSize[l];
+        for (int i = 0; i < n; ++i) X[off[l] + i + (long)n * i] = Z[off[l] + i + (long)n * i] = dd_from(lambda);
+    }
+    y.assign(P.m, dd_zero());
+    Scanner sc(text);
+    std::string tok;
+    for (int k = 0; k < P.m; ++k) {
+        if (!sc.skip_token(tok)) throw Error(ERR_IO, "initial point: the vector ended early");
+        y[k] = dd_neg(dd_parse(tok)); // yVec is opposite sign
+    }
+    // DenseLinearSpace::setElement_SDP (sdpa_struct.cpp:1564-1577)
+    auto set = [&](std::vector<dd_t> &M, int l, int i, int j, dd_t v) {
+        if (l < 0 || l >= P.nSDP || i < 0 || j < 0 || i >= P.sdpSize[l] || j >= P.sdpSize[l]) throw Error(ERR_IO, "out of range in input data");
+        const int n = P.sdpSize[l];
+        M[off[l] + i + (long)n * j] = v;
+        M[off[l] + j + (long)n * i] = v;
+    };
+    if (sparse) {
+        int target, l, i, j;
+        while (sc.skip_int(target) && sc.skip_int(l) && sc.skip_int(i) && sc.skip_int(j) && sc.skip_token(tok)) {
+            double probe;
+            if (std::sscanf(tok.c_str(), "%lf", &probe) <= 0) break;
+            const dd_t v = dd_parse(tok);
+            if (l > P.nSDP) throw Error(ERR_UNSUPPORTED, "initial point: an entry outside the SDP blocks");
+            set(target == 1 ? Z : X, l - 1, i - 1, j - 1, v);
+        }
+    } else {
+        for (int pass = 0; pass < 2; ++pass) { // Z (the file's X), then X (its Y)
+            std::vector<dd_t> &M = pass == 0 ? Z : X;
+            for (int l = 0; l < P.nSDP; ++l) {
+                const int n = P.sdpSize[l];
+                for (int i = 0; i < n; ++i)
+                    for (int j = 0; j < n; ++j) {
+                        if (!sc.skip_token(tok)) throw Error(ERR_IO, "initial point: the matrices ended early");
+                        const dd_t v = dd_parse(tok);
+                        if (i <= j && !dd_is_zero(v)) set(M, l, i, j, v);
+                    }
+            }
+        }
+    }
+}
+
+void read_init_point(const std::string &path, bool sparse, const Problem &P, double lambda, std::vector<dd_t> &X, std::vector<dd_t> &y,
+                     std::vector<dd_t> &Z) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) throw Error(ERR_IO, "Cannot open init file " + path);
+    std::stringstream ss;
+    ss << f.rdbuf();
+    read_init_point_text(ss.str(), sparse, P, lambda, X, y, Z);
+}
+
 Problem make_problem(int m, int nblock, const int *blockStruct, const dd_t *b, long nnz, const int *k, const int *blk, const int *i, const int *j,
                      const dd_t *val) {
     if (m <= 0 || nblock <= 0) throw Error(ERR_ARG, "m and nblock must be positive");

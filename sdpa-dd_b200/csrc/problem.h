@@ -68,6 +68,18 @@ Problem make_problem(int m, int nblock, const int *blockStruct, const dd_t *b, l
 // changeToDense for every matrix, per-block constraint lists, formulas.
 void finalize_problem(Problem &p, double kappa);
 
+// An initial point file as IO::read(fpInit, xMat, yVec, zMat, sparse) reads
+// it (sdpa_io.cpp:152-283): first the file's x (y = -x), then its X and Y
+// matrices (target 1 and 2 in sparse files; the SDP blocks of X, then of Y,
+// row by row in dense files) into the internal Z and X, each starting as
+// lambda I (Solutions::initialize): a sparse entry sets (i, j) and (j, i); a
+// dense file sets only the nonzero entries with i <= j (and their mirror).
+// X and Z are block spaces (SDP blocks concatenated, column-major).
+void read_init_point_text(const std::string &text, bool sparse, const Problem &P, double lambda, std::vector<dd_t> &X, std::vector<dd_t> &y,
+                          std::vector<dd_t> &Z);
+void read_init_point(const std::string &path, bool sparse, const Problem &P, double lambda, std::vector<dd_t> &X, std::vector<dd_t> &y,
+                     std::vector<dd_t> &Z);
+
 struct Param {
     int maxIteration = 200;
     double epsilonStar = 1.0e-30, lambdaStar = 1.0e+4, omegaStar = 2.0, lowerBound = -1.0e+5, upperBound = 1.0e+5, betaStar = 0.1, betaBar = 0.3,

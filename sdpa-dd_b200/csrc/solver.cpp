@@ -129,14 +129,25 @@ const char *phase_name(PhaseType p) {
 // (sdpa_main.cpp:229-282)
 void Solver::start() {
     const dd_t lambda = dd_from(param.lambdaStar);
-    init_point(c, lambda);
+    if (c.has_init) {
+        // an initial point file (sdpa_main.cpp:237-251, 276-278):
+        // computeInverse, then AverageComplementarity::initialize(Solutions)
+        const size_t bytes = sizeof(dd_t) * c.space_len;
+        CK(cudaMemcpyAsync(c.X.buf.p, c.init_X.buf.p, bytes, cudaMemcpyDeviceToDevice, c.stream));
+        CK(cudaMemcpyAsync(c.Z.buf.p, c.init_Z.buf.p, bytes, cudaMemcpyDeviceToDevice, c.stream));
+        CK(cudaMemcpyAsync(c.y.p, c.init_y.p, sizeof(dd_t) * c.m, cudaMemcpyDeviceToDevice, c.stream));
+        if (!compute_inverse(c)) throw Error(ERR_ARG, "the initial point is not positive definite (cholesky of X or Z failed)");
+        mu_initial = dd_div_d(inner_space(c, c.X, c.Z), (double)c.nDim);
+    } else {
+        init_point(c, lambda);
+        mu_initial = dd_mul(lambda, lambda);
+    }
     residuals(c, normPrimalVec, normDualMat);
     initNormPrimalVec = normPrimalVec;
     initNormDualMat = normDualMat;
     alpha_primal = alpha_dual = ZERO;
     beta_value = dd_from(param.betaStar);
     reduction_on = true;
-    mu_initial = dd_mul(lambda, lambda);
     mu_current = mu_initial;
     // RatioInitResCurrentRes::initialize (sdpa_parts.cpp:621-634)
     const dd_t accuracy = dd_from(param.epsilonDash);
@@ -335,7 +346,8 @@ int Solver::step(FILE *display, FILE *out) {
     // RatioInitResCurrentRes::update_exact (sdpa_parts.cpp:644-655)
     theta_primal = dd_gt_d(initNormPrimalVec, 1.0e-10) ? dd_div(normPrimalVec, initNormPrimalVec) : ZERO;
     theta_dual = dd_gt_d(initNormDualMat, 1.0e-10) ? dd_div(normDualMat, initNormDualMat) : ZERO;
-    // SolveInfo::update with the lambda*I initial point (sdpa_parts.cpp:708-770)
+    // SolveInfo::update (sdpa_parts.cpp:690-739 with an initial point file,
+    // :741-770 with lambda I)
     {
         objValPrimal = inner_C(c, c.X);
         objValDual = inner_b(c, c.y.p);
@@ -343,8 +355,8 @@ int Solver::step(FILE *display, FILE *out) {
         rho = ZERO;
         const dd_t x0z0 = dd_mul_d(mu_initial, (double)c.nDim);
         const dd_t xMatzMat = dd_mul_d(mu_current, (double)c.nDim);
-        const dd_t x0zMat = lambda_trace(c, c.Z, param.lambdaStar);
-        const dd_t xMatz0 = lambda_trace(c, c.X, param.lambdaStar);
+        const dd_t x0zMat = c.has_init ? inner_space(c, c.init_X, c.Z) : lambda_trace(c, c.Z, param.lambdaStar);
+        const dd_t xMatz0 = c.has_init ? inner_space(c, c.X, c.init_Z) : lambda_trace(c, c.X, param.lambdaStar);
         const dd_t accuracy = dd_from(param.epsilonDash);
         if (dd_le(normPrimalVec, accuracy))
             if (dd_lt(xMatz0, etaPrimal)) etaPrimal = xMatz0;
