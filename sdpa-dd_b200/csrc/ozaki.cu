@@ -12,24 +12,36 @@
 // Products (ozaki_syrk_kernel).  C(i,j) -= 2^(e_i+e_j) sum_d 2^-7d A_d(i,j),
 // A_d = sum_{s+t=d} D_s(i,:) . D_t(j,:), for d = 2..S+1 (the S(S+1)/2 slice
 // pairs that reach 7(S+1) bits).  Every A_d is an exact int32 (|A_d| <=
-// 16 * 64 * 64 * 64 = 2^22): it is accumulated by tcgen05.mma kind::i8 in
-// tensor memory.  Four consecutive diagonals combine exactly in int64
-// (2^21 A_d + 2^14 A_d+1 + 2^7 A_d+2 + A_d+3 < 2^44) and convert exactly to
-// double; the four group values become one dd (TwoSum, exact, then one dd
-// addition) that is scaled by 2^(e_i+e_j) and subtracted from C.
+// 16 * 64 * 64 * 64 = 2^22), accumulated by tcgen05.mma kind::i8 in tensor
+// memory.
 //
-// Kernel layout: one persistent CTA per SM over 128 x 32 output tiles of the
-// lower triangle (row-block major, so a CTA keeps its 128-row A slices while
-// it walks the columns).  Warp 0 lane 0 stages operands with bulk copies
-// (cp.async.bulk, no multicast) and issues the MMAs; warps 1-8 drain tensor
-// memory.  Tensor memory holds two rounds of eight diagonal accumulators
-// (8 x 32 columns each): round 0 (d = 10..17) of the next tile is issued
-// while round 1 (d = 2..9) of the current one is being drained.
+// One tcgen05.mma costs about the same time for any N up to 128 (on B200 a
+// kind::i8 M=128 K=32 instruction occupies the issuing thread ~97 cycles
+// for N = 32..128 and ~170 for N = 256), so the kernel issues few, wide
+// MMAs: a tile is 128 rows x 16 columns, its B operand the tile's S slices
+// stacked (row 16 (t-1) + j is slice t of column j), and its accumulators
+// are laid out by diagonal (diagonal d in columns 16 (d-2) .. 16 (d-2) + 15).
+// The MMA of A slice s against stacked B slices 1 .. S+1-s (N = 16 (S+1-s))
+// then writes diagonals s+1 .. S+1 in one instruction: S x 2 K steps = 32
+// MMAs per tile for 16 slices.
+//
+// Epilogue: four consecutive diagonals combine exactly in int64 (2^21 A_d +
+// 2^14 A_d+1 + 2^7 A_d+2 + A_d+3 < 2^44).  The two smallest groups fold into
+// an int64 carry in units of 2^-104, the third joins it as a dd, the
+// largest (an exact double) is added, and the dd is scaled by 2^(e_i+e_j)
+// and subtracted from C.
+//
+// Kernel layout: one persistent CTA per SM over the tiles of the lower
+// triangle (row-block major, so a CTA keeps its 128-row A slices in shared
+// memory while it walks the columns).  Warp 0 lane 0 stages operands with
+// bulk copies (cp.async.bulk, no multicast; B four tiles deep) and issues
+// the MMAs; warps 1-8 drain tensor memory, which holds two accumulator
+// buffers of 16 x 16 columns, so one tile multiplies while the last drains.
 // Operand layout in global and shared memory: per slice, 8-row groups of
 // 512 bytes, each four 128-byte core matrices (8 rows x 16 K-bytes): the
 // K-major, non-swizzled canonical layout of the MMA's shared-memory
 // descriptors (LBO 128 bytes between the two K chunks of one MMA, SBO 512
-// bytes between row groups).
+// bytes between row groups), so a tile's stacked B slices are contiguous.
 // Every mbarrier wait is bounded (2 s); on expiry the CTA records a code in
 // the error word, stops issuing, waits (bounded) for what it issued and
 // frees its tensor memory.
@@ -46,11 +58,20 @@ namespace {
 
 constexpr int OZ_THREADS = 288; // warp 0: copies + MMA; warps 1-8: epilogue
 constexpr int OZ_A_BYTES = OZ_ROWS_A * OZ_K; // one slice of a 128-row block
-constexpr int OZ_B_BYTES = OZ_COLS_B * OZ_K; // one slice of a 32-row block
-constexpr size_t OZ_SMEM = 1024 + (size_t)OZ_MAX_SLICES * OZ_A_BYTES + 2 * (size_t)OZ_MAX_SLICES * OZ_B_BYTES;
-// kind::i8 instruction descriptor: D s32, A and B s8, both K-major,
-// N = 32, M = 128.
-constexpr uint32_t OZ_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_COLS_B >> 3) << 17) | ((uint32_t)(OZ_ROWS_A >> 4) << 24);
+constexpr int OZ_B_BYTES = OZ_COLS_B * OZ_K; // one slice of a 16-row block
+constexpr int OZ_TILE_B = OZ_MAX_SLICES * OZ_B_BYTES; // the stacked B slices of a tile
+constexpr int OZ_STAGES = 4;                 // B tiles in shared memory
+constexpr int OZ_ACC_COLS = OZ_MAX_SLICES * OZ_COLS_B; // tensor-memory columns of one accumulator buffer
+static_assert(2 * OZ_ACC_COLS <= 512, "split kernel: two accumulator buffers must fit tensor memory");
+static_assert(OZ_ACC_COLS <= 256, "split kernel: the widest MMA has N = 16 S <= 256");
+// the 16 A slices of a row block and OZ_STAGES stacked B tiles
+constexpr size_t OZ_SMEM = 1024 + (size_t)OZ_MAX_SLICES * OZ_A_BYTES + (size_t)OZ_STAGES * OZ_TILE_B;
+static_assert(OZ_SMEM <= 232448 - 256, "split kernel: shared memory above the per-CTA limit");
+// kind::i8 instruction descriptor: D s32, A and B s8, both K-major, M = 128,
+// N = n (a multiple of 16, 16..256).
+__host__ __device__ constexpr uint32_t oz_idesc(int n) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(OZ_ROWS_A >> 4) << 24);
+}
 constexpr unsigned long long OZ_WAIT_NS = 2000000000ull;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -99,11 +120,6 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 __device__ __forceinline__ void tc_commit(uint64_t *b) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(b)) : "memory");
 }
-__device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t da, uint64_t db, uint32_t accumulate) {
-    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem), "l"(da),
-                 "l"(db), "r"(OZ_IDESC), "r"(accumulate)
-                 : "memory");
-}
 __device__ __forceinline__ void tc_ld8(uint32_t taddr, int32_t *r) {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
@@ -117,10 +133,9 @@ __device__ __forceinline__ uint64_t oz_desc(uint32_t saddr) {
     return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(512 >> 4) << 32) | (1ull << 46);
 }
 
-// First diagonal of round r.  Round 0 takes the small diagonals 10..17 (200
-// of the 272 MMAs of a 16-slice tile), round 1 the large ones 2..9: the
-// epilogue's C update then overlaps the long round 0 of the next tile.
-__host__ __device__ constexpr int oz_round_d0(int r) { return r == 0 ? 10 : 2; }
+// Diagonal groups of the epilogue: group g holds the diagonals d = 2+4g ..
+// 5+4g (those with d <= S+1).
+__host__ __device__ constexpr int oz_groups(int ns) { return (ns + 3) >> 2; }
 
 struct OzArgs {
     const int8_t *slices;
@@ -133,289 +148,291 @@ struct OzArgs {
     int *err;
 };
 
-// Tiles of the lower triangle, row-block major: row block I has
-// min(4 (I + 1), nJ) column blocks.
+// Tiles of the lower triangle, row-block major: row block I (128 rows) has
+// min(8 (I + 1), nJ) column blocks of 16.
+constexpr int OZ_JPI = OZ_ROWS_A / OZ_COLS_B;
 __device__ __forceinline__ void oz_tile_at(long t, int nI, int nJ, int &I, int &J) {
     I = 0;
     for (; I < nI; ++I) {
-        const long cnt = min(4L * (I + 1), (long)nJ);
+        const long cnt = min((long)OZ_JPI * (I + 1), (long)nJ);
         if (t < cnt) break;
         t -= cnt;
     }
     J = (int)t;
 }
 __device__ __forceinline__ void oz_tile_next(int nJ, int &I, int &J) {
-    if (++J >= min(4 * (I + 1), nJ)) {
+    if (++J >= min(OZ_JPI * (I + 1), nJ)) {
         ++I;
         J = 0;
     }
 }
 
 // Shared state of one CTA.
+//   barA          A slices of the current row block landed
+//   barB[st]      the B slices of the tile in stage st landed
+//   bfree[st]     every MMA of the tile in stage st completed (the stage,
+//                 and at a row-block change A, may be reloaded)
+//   tfull/tempty  accumulator buffer b holds a finished tile / is drained
+//   fin           every MMA the CTA issued completed (exit)
 struct OzShared {
-    uint64_t barA, barB[2], bfree[2], tfull[2], tempty[2];
+    uint64_t barA, barB[OZ_STAGES], bfree[OZ_STAGES], tfull[2], tempty[2], fin;
     uint32_t tmem;
     int abort_flag;
 };
 
-// MMAs of round R into its tensor-memory buffer: for each diagonal d of the
-// round, the slice pairs (s, d - s) over the two 32-byte K steps; the first
-// MMA of a diagonal overwrites, the others accumulate.  descA/descB address
-// slice 1 of the A and B operands; slices are OZ_A_BYTES / OZ_B_BYTES apart.
-template <int R, int NS>
-__device__ __forceinline__ void oz_issue_round(uint32_t tmem, uint64_t descA, uint64_t descB) {
+__device__ __forceinline__ void tc_mma_i8_n(uint32_t d_tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem), "l"(da),
+                 "l"(db), "r"(idesc), "r"(accumulate)
+                 : "memory");
+}
+
+// The MMAs of one tile into the accumulator buffer at dbuf: for A slice s
+// and K step kk, one MMA against the stacked B slices t = 1 .. S+1-s
+// (N = 16 (S+1-s)) writes the columns of diagonals s+1 .. S+1.  The first
+// (s = 1, N = 16 S) covers every column and overwrites; the rest accumulate.
+template <int NS>
+__device__ __forceinline__ void oz_issue_tile(uint32_t dbuf, uint64_t descA, uint64_t descB) {
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-        const int d = oz_round_d0(R) + u;
-        if (d <= NS + 1) {
-            const uint32_t dcol = tmem + (uint32_t)(R * 256 + u * 32);
+    for (int s = 1; s <= NS; ++s) {
 #pragma unroll
-            for (int s = 1; s <= NS; ++s) {
-                const int t = d - s;
-                if (t >= 1 && t <= NS) {
-#pragma unroll
-                    for (int kk = 0; kk < 2; ++kk) {
-                        const uint64_t da = descA + (uint64_t)(((s - 1) * OZ_A_BYTES + kk * 256) >> 4);
-                        const uint64_t db = descB + (uint64_t)(((t - 1) * OZ_B_BYTES + kk * 256) >> 4);
-                        const int s_first = d - NS > 1 ? d - NS : 1;
-                        tc_mma_i8(dcol, da, db, (s == s_first && kk == 0) ? 0u : 1u);
-                    }
-                }
-            }
+        for (int kk = 0; kk < 2; ++kk)
+            tc_mma_i8_n(dbuf + (uint32_t)((s - 1) * OZ_COLS_B), descA + (uint64_t)(((s - 1) * OZ_A_BYTES + kk * 256) >> 4),
+                        descB + (uint64_t)((kk * 256) >> 4), oz_idesc((NS + 1 - s) * OZ_COLS_B), (s == 1 && kk == 0) ? 0u : 1u);
+    }
+}
+__device__ __forceinline__ void oz_issue_tile_rt(int ns, uint32_t dbuf, uint64_t descA, uint64_t descB) {
+    for (int s = 1; s <= ns; ++s)
+        for (int kk = 0; kk < 2; ++kk)
+            tc_mma_i8_n(dbuf + (uint32_t)((s - 1) * OZ_COLS_B), descA + (uint64_t)(((s - 1) * OZ_A_BYTES + kk * 256) >> 4),
+                        descB + (uint64_t)((kk * 256) >> 4), oz_idesc((ns + 1 - s) * OZ_COLS_B), (s == 1 && kk == 0) ? 0u : 1u);
+}
+
+// A wait that ignores the abort flag (still bounded): used on the way out,
+// where copies and MMAs already issued must finish before the CTA releases
+// its shared and tensor memory.
+__device__ void oz_wait_out(uint64_t *b, uint32_t parity, int *err) {
+    const unsigned long long t0 = oz_ns();
+    while (!mbar_try_wait(b, parity)) {
+        if (oz_ns() - t0 > OZ_WAIT_NS) {
+            atomicCAS(err, 0, 5);
+            return;
         }
     }
 }
 
-// The same for a slice count known only at run time.
-__device__ __forceinline__ void oz_issue_round_rt(int r, int ns, uint32_t tmem, uint64_t descA, uint64_t descB) {
-    for (int u = 0; u < 8; ++u) {
-        const int d = oz_round_d0(r) + u;
-        if (d > ns + 1) break;
-        const uint32_t dcol = tmem + (uint32_t)(r * 256 + u * 32);
-        uint32_t acc = 0;
-        const int s_lo = max(1, d - ns), s_hi = min(ns, d - 1);
-        for (int s = s_lo; s <= s_hi; ++s) {
-            const int t = d - s;
-            for (int kk = 0; kk < 2; ++kk) {
-                tc_mma_i8(dcol, descA + (uint64_t)(((s - 1) * OZ_A_BYTES + kk * 256) >> 4), descB + (uint64_t)(((t - 1) * OZ_B_BYTES + kk * 256) >> 4),
-                          acc);
-                acc = 1;
-            }
-        }
-    }
-}
-
+// Warp 0, lane 0: bulk copies of the operands and the MMAs.  The A slices
+// of a row block stay in shared memory while the CTA walks its columns; the
+// B slices of the next OZ_STAGES - 1 tiles are in flight while a tile
+// multiplies (tile n in stage n mod OZ_STAGES, accumulators in buffer
+// n mod 2).
 __device__ void oz_producer(const OzArgs &a, OzShared &S, uint8_t *smA, uint8_t *smB, long t_begin, long t_end) {
     volatile int *abort_flag = &S.abort_flag;
-    int I, J;
-    oz_tile_at(t_begin, a.nI, a.nJ, I, J);
-    auto issue_B = [&](int jb, int buf) {
-        mbar_expect_tx(&S.barB[buf], (uint32_t)(a.ns * OZ_B_BYTES));
-        for (int s = 0; s < a.ns; ++s)
-            bulk_g2s(smB + (size_t)buf * OZ_MAX_SLICES * OZ_B_BYTES + (size_t)s * OZ_B_BYTES, a.slices + s * a.slice_stride + (long)jb * OZ_B_BYTES,
-                     OZ_B_BYTES, &S.barB[buf]);
+    const int ns = a.ns;
+    const long ntile = t_end - t_begin;
+    auto load_B = [&](int jb, int st) {
+        mbar_expect_tx(&S.barB[st], (uint32_t)(ns * OZ_B_BYTES));
+        for (int s = 0; s < ns; ++s)
+            bulk_g2s(smB + (size_t)st * OZ_TILE_B + (size_t)s * OZ_B_BYTES, a.slices + s * a.slice_stride + (long)jb * OZ_B_BYTES, OZ_B_BYTES,
+                     &S.barB[st]);
     };
     const uint64_t descA = oz_desc(smem_u32(smA));
-    const uint64_t descB0 = oz_desc(smem_u32(smB)), descB1 = oz_desc(smem_u32(smB + (size_t)OZ_MAX_SLICES * OZ_B_BYTES));
-    // phase parities, one bit per barrier of a pair; pending copies likewise
-    uint32_t phA = 0, phB = 0, phFree = 0, phEmpty = 0, pendB = 0;
+    const uint64_t descB0 = oz_desc(smem_u32(smB));
+    int Ip, Jp; // the next tile to prefetch (np)
+    oz_tile_at(t_begin, a.nI, a.nJ, Ip, Jp);
+    long np = 0;
+    for (; np < ntile && np < OZ_STAGES - 1; ++np) {
+        load_B(Jp, (int)(np % OZ_STAGES));
+        oz_tile_next(a.nJ, Ip, Jp);
+    }
+    int I, J;
+    oz_tile_at(t_begin, a.nI, a.nJ, I, J);
+    uint32_t phA = 0;
+    bool pendA = false, issued = false;
     int curA = -1;
-    bool pendA = false;
-    issue_B(J, 0);
-    pendB = 1u;
-    long n = 0;
+    long nb = 0; // tiles whose B copy has been waited for
     bool ok = true;
-    for (long t = t_begin; t < t_end && ok; ++t, ++n) {
-        const int b = (int)(n & 1);
-        bool prev_done = n == 0; // tile n-1 complete (its B buffer and A free)
+    for (long n = 0; n < ntile && ok; ++n) {
+        const int st = (int)(n % OZ_STAGES), b = (int)(n & 1);
         if (I != curA) {
-            if (!prev_done) {
-                ok = oz_wait(&S.bfree[b ^ 1], (phFree >> (b ^ 1)) & 1u, abort_flag, a.err, 1);
-                phFree ^= 1u << (b ^ 1);
+            // every MMA of the previous tile reads A
+            if (n > 0) {
+                ok = oz_wait(&S.bfree[(n - 1) % OZ_STAGES], (uint32_t)(((n - 1) / OZ_STAGES) & 1), abort_flag, a.err, 1);
                 if (!ok) break;
-                prev_done = true;
             }
-            mbar_expect_tx(&S.barA, (uint32_t)(a.ns * OZ_A_BYTES));
-            for (int s = 0; s < a.ns; ++s)
+            mbar_expect_tx(&S.barA, (uint32_t)(ns * OZ_A_BYTES));
+            for (int s = 0; s < ns; ++s)
                 bulk_g2s(smA + (size_t)s * OZ_A_BYTES, a.slices + s * a.slice_stride + (long)I * OZ_A_BYTES, OZ_A_BYTES, &S.barA);
             pendA = true;
             ok = oz_wait(&S.barA, phA, abort_flag, a.err, 2);
-            phA ^= 1u;
             if (!ok) break;
+            phA ^= 1u;
             pendA = false;
             curA = I;
         }
-        ok = oz_wait(&S.barB[b], (phB >> b) & 1u, abort_flag, a.err, 3);
-        phB ^= 1u << b;
+        ok = oz_wait(&S.barB[st], (uint32_t)((n / OZ_STAGES) & 1), abort_flag, a.err, 3);
         if (!ok) break;
-        pendB &= ~(1u << b);
-        const uint64_t descB = b ? descB1 : descB0;
-        for (int r = 0; r < 2 && ok; ++r) {
-            ok = oz_wait(&S.tempty[r], ((phEmpty >> r) & 1u) ^ 1u, abort_flag, a.err, 4);
-            phEmpty ^= 1u << r;
-            if (!ok) break;
-            tc_fence_after();
-            if (a.ns == OZ_MAX_SLICES) {
-                if (r == 0)
-                    oz_issue_round<0, OZ_MAX_SLICES>(S.tmem, descA, descB);
-                else
-                    oz_issue_round<1, OZ_MAX_SLICES>(S.tmem, descA, descB);
-            } else {
-                oz_issue_round_rt(r, a.ns, S.tmem, descA, descB);
-            }
-            tc_commit(&S.tfull[r]);
-        }
+        nb = n + 1;
+        ok = oz_wait(&S.tempty[b], (uint32_t)(((n >> 1) & 1) ^ 1), abort_flag, a.err, 4);
         if (!ok) break;
-        tc_commit(&S.bfree[b]);
-        // next tile's B into the other buffer, once tile n-1 has released it
-        int In = I, Jn = J;
-        oz_tile_next(a.nJ, In, Jn);
-        if (t + 1 < t_end) {
-            if (!prev_done) {
-                ok = oz_wait(&S.bfree[b ^ 1], (phFree >> (b ^ 1)) & 1u, abort_flag, a.err, 1);
-                phFree ^= 1u << (b ^ 1);
+        tc_fence_after();
+        const uint64_t descB = descB0 + (uint64_t)(((size_t)st * OZ_TILE_B) >> 4);
+        if (ns == OZ_MAX_SLICES)
+            oz_issue_tile<OZ_MAX_SLICES>(S.tmem + (uint32_t)(b * OZ_ACC_COLS), descA, descB);
+        else
+            oz_issue_tile_rt(ns, S.tmem + (uint32_t)(b * OZ_ACC_COLS), descA, descB);
+        issued = true;
+        tc_commit(&S.tfull[b]);
+        tc_commit(&S.bfree[st]);
+        // prefetch tile np (= n + OZ_STAGES - 1) once tile np - OZ_STAGES
+        // (= n - 1), the last user of its stage, has completed
+        if (np < ntile) {
+            const int sp = (int)(np % OZ_STAGES);
+            if (np >= OZ_STAGES) {
+                ok = oz_wait(&S.bfree[sp], (uint32_t)(((np - OZ_STAGES) / OZ_STAGES) & 1), abort_flag, a.err, 1);
                 if (!ok) break;
             }
-            issue_B(Jn, b ^ 1);
-            pendB |= 1u << (b ^ 1);
+            load_B(Jp, sp);
+            oz_tile_next(a.nJ, Ip, Jp);
+            ++np;
         }
-        I = In;
-        J = Jn;
+        oz_tile_next(a.nJ, I, J);
     }
-    // Before the CTA frees its tensor memory: every issued copy has landed
-    // (bounded waits; an aborted CTA gives up after 2 s each).
-    if (pendA) oz_wait(&S.barA, phA, abort_flag, a.err, 5);
-    for (int b2 = 0; b2 < 2; ++b2)
-        if ((pendB >> b2) & 1u) oz_wait(&S.barB[b2], (phB >> b2) & 1u, abort_flag, a.err, 5);
-}
-
-__device__ __forceinline__ double oz_combine(const int32_t *a0, const int32_t *a1, const int32_t *a2, const int32_t *a3, int c, double scale) {
-    const long long v = ((long long)a0[c] << 21) + ((long long)a1[c] << 14) + ((long long)a2[c] << 7) + (long long)a3[c];
-    return __ll2double_rn(v) * scale;
+    // On the way out every issued copy lands and every issued MMA completes
+    // (bounded waits) before the CTA frees its memory.
+    if (pendA) oz_wait_out(&S.barA, phA, a.err);
+    for (long k = nb; k < np; ++k) oz_wait_out(&S.barB[k % OZ_STAGES], (uint32_t)((k / OZ_STAGES) & 1), a.err);
+    if (issued) {
+        tc_commit(&S.fin);
+        oz_wait_out(&S.fin, 0, a.err);
+    }
 }
 
 // 2^e as a double for -1022 <= e <= 1023 (built from its bits)
 __device__ __forceinline__ double oz_pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
 
-// Drains round R (its 8 diagonals from oz_round_d0(R)) for this thread's 16 columns
-// into the dd accumulator (R = 0 sets it, R = 1 adds to it).
-template <int R>
-__device__ __forceinline__ void oz_drain(const OzArgs &a, uint32_t lane_base, double *acc_hi, double *acc_lo) {
-    constexpr int D0 = oz_round_d0(R);
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {
-        double g[2][8];
-#pragma unroll
-        for (int gi = 0; gi < 2; ++gi) {
-            int32_t v[4][8];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int slot = 4 * gi + u;
-                if (D0 + slot <= a.ns + 1) {
-                    tc_ld8(lane_base + (uint32_t)(R * 256 + slot * 32 + 8 * half), v[u]);
-                } else {
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) v[u][c] = 0;
-                }
-            }
-            tc_wait_ld();
-            // group value (2^21 A_d + 2^14 A_d+1 + 2^7 A_d+2 + A_d+3) 2^-7(d+3)
-            const double sc = oz_pow2(-7 * (D0 + 4 * gi + 3));
-#pragma unroll
-            for (int c = 0; c < 8; ++c) g[gi][c] = oz_combine(v[0], v[1], v[2], v[3], c, sc);
-        }
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int cc = 8 * half + c;
-            double e, s = ddm::two_sum(g[0][c], g[1][c], e); // exact: 72 bits at most
-            if (R == 0) {
-                acc_hi[cc] = s;
-                acc_lo[cc] = e;
-            } else { // accurate dd addition of (s, e)
-                double t1, t2, s2;
-                double s1 = ddm::two_sum(acc_hi[cc], s, s2);
-                t1 = ddm::two_sum(acc_lo[cc], e, t2);
-                s2 += t1;
-                s1 = ddm::fast_two_sum(s1, s2, s2);
-                s2 += t2;
-                acc_hi[cc] = ddm::fast_two_sum(s1, s2, acc_lo[cc]);
-            }
-        }
-    }
+__device__ __forceinline__ void tc_ld4(uint32_t taddr, int32_t *r) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];" : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(taddr));
 }
 
-// C(i, jb + c) -= 2^(e_i + e_j) acc[c] for c in [c0, c0 + 8) (cv: C prefetched)
-__device__ __forceinline__ void oz_update8(const OzArgs &a, int i, int jb, int c0, int ei, const double *acc_hi, const double *acc_lo,
-                                           const double2 *cv) {
-    const int4 e0 = *reinterpret_cast<const int4 *>(a.exps + jb + c0), e1 = *reinterpret_cast<const int4 *>(a.exps + jb + c0 + 4);
-    const int ej[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+// Group g of four of this thread's columns, at tb in the accumulator buffer
+// (diagonal d in columns 16 (d - 2) ..): V = 2^21 A_d + 2^14 A_d+1 +
+// 2^7 A_d+2 + A_d+3 (d = 2 + 4g; exact, |V| < 2^44; diagonals beyond S+1
+// count as zero).  Its value is V 2^-(35 + 28 g) in units of 2^(e_i + e_j).
+__device__ __forceinline__ void oz_group4(int ns, int g, uint32_t tb, long long *V) {
+    const int d0 = 2 + 4 * g;
+    int32_t v[4][4];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        const int j = jb + c0 + c;
-        if (i < a.n && j < a.n && j <= i) {
-            const int sc = ei + ej[c];
-            dd_t p;
-            if (sc >= -1022 && sc <= 1023) {
-                const double pw = oz_pow2(sc);
-                p = dd_make(acc_hi[c0 + c] * pw, acc_lo[c0 + c] * pw);
-            } else {
-                p = dd_make(ldexp(acc_hi[c0 + c], sc), ldexp(acc_lo[c0 + c], sc));
-            }
-            const dd_t r = dd_sub(dd_make(cv[c].x, cv[c].y), p);
-            __stcs(reinterpret_cast<double2 *>(a.C + i + a.ldc * (long)j), make_double2(r.hi, r.lo));
+    for (int u = 0; u < 4; ++u) {
+        if (d0 + u <= ns + 1) {
+            tc_ld4(tb + (uint32_t)((d0 + u - 2) * OZ_COLS_B), v[u]);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) v[u][c] = 0;
         }
     }
-}
-
-__device__ __forceinline__ void oz_load8(const OzArgs &a, int i, int jb, int c0, double2 *cv) {
+    tc_wait_ld();
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        const int j = jb + c0 + c;
-        cv[c] = (i < a.n && j < a.n && j <= i) ? __ldcs(reinterpret_cast<const double2 *>(a.C + i + a.ldc * (long)j)) : make_double2(0.0, 0.0);
-    }
+    for (int c = 0; c < 4; ++c) V[c] = ((long long)v[0][c] << 21) + ((long long)v[1][c] << 14) + ((long long)v[2][c] << 7) + (long long)v[3][c];
 }
 
+// Epilogue warps 1-8: warp w reads tensor-memory lanes 32 (w mod 4) .. +31
+// (its rows of the tile) and columns 8 h .. 8 h + 7 of every diagonal,
+// h = (w - 1) / 4.  The groups come smallest first.  Groups g >= 2
+// (diagonals 10..17) fold exactly into one int64 per entry in units of
+// 2^-104 (group 2 shifted up by 13 bits, group 3 down by 15 with rounding:
+// |carry| < 2^58, the rounding at most 2^-105).  Group 1 and the carry
+// become a dd (the group's exact double, the carry as two exact doubles,
+// two TwoSums); group 0, an exact double, is added to it; the sum is scaled
+// by 2^(e_i + e_j) and subtracted from C, whose entries were requested
+// before the wait for the accumulators.
 __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_end) {
     volatile int *abort_flag = &S.abort_flag;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int q = warp & 3, h = (warp - 1) >> 2;
     const int row = 32 * q + lane;
-    const uint32_t lane_base = S.tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(16 * h);
+    const uint32_t lane_base = S.tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(8 * h);
+    const int G = oz_groups(a.ns);
     int I, J;
     oz_tile_at(t_begin, a.nI, a.nJ, I, J);
-    uint32_t ph = 0; // parity of tfull[0] and tfull[1] (they complete in step)
     // lane 0 waits; the warp follows its outcome (the tensor-memory loads
     // are warp-collective)
-    auto wait_full = [&](int r) {
+    auto wait_full = [&](int b, uint32_t parity) {
         int okw = 1;
-        if (lane == 0) okw = oz_wait(&S.tfull[r], ph, abort_flag, a.err, 6) ? 1 : 0;
+        if (lane == 0) okw = oz_wait(&S.tfull[b], parity, abort_flag, a.err, 6) ? 1 : 0;
         return __shfl_sync(0xffffffffu, okw, 0) != 0;
     };
-    auto release = [&](int r) {
+    for (long n = 0; n < t_end - t_begin; ++n) {
+        const int i = I * OZ_ROWS_A + row;
+        const int jb = J * OZ_COLS_B + 8 * h;
+        const int b = (int)(n & 1);
+        double2 cv[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int j = jb + c;
+            cv[c] = (i < a.n && j < a.n && j <= i) ? __ldcs(reinterpret_cast<const double2 *>(a.C + i + a.ldc * (long)j)) : make_double2(0.0, 0.0);
+        }
+        if (!wait_full(b, (uint32_t)((n >> 1) & 1))) break;
+        tc_fence_after();
+        const uint32_t tb = lane_base + (uint32_t)(b * OZ_ACC_COLS);
+        long long acc[8];
+        double phi[8], plo[8];
+        for (int g = G - 1; g >= 0; --g) {
+            const bool first = g == G - 1;
+#pragma unroll
+            for (int ch = 0; ch < 2; ++ch) {
+                long long V[4];
+                oz_group4(a.ns, g, tb + (uint32_t)(4 * ch), V);
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) {
+                    const int c = 4 * ch + cc;
+                    const long long Vc = V[cc];
+                    if (g >= 2) {
+                        const int sh = 69 - 28 * g; // 2^(69 - 28 g): units of 2^-104
+                        const long long v = sh >= 0 ? (Vc << sh) : ((Vc + (1LL << (-sh - 1))) >> (-sh));
+                        acc[c] = first ? v : acc[c] + v;
+                    } else if (g == 1) {
+                        const long long A = first ? 0LL : acc[c];
+                        const long long alo = A & 0x3FFFFFFLL, ahi = A - alo; // both exact as doubles
+                        const double gv = __ll2double_rn(Vc) * oz_pow2(-63);
+                        const double ah = __ll2double_rn(ahi) * oz_pow2(-104), al = __ll2double_rn(alo) * oz_pow2(-104);
+                        double e1, s1 = ddm::two_sum(gv, ah, e1);
+                        double e2, s2 = ddm::two_sum(s1, al, e2);
+                        phi[c] = ddm::fast_two_sum(s2, e1 + e2, plo[c]);
+                    } else {
+                        const double gv = __ll2double_rn(Vc) * oz_pow2(-35);
+                        if (first) {
+                            phi[c] = gv;
+                            plo[c] = 0.0;
+                        } else {
+                            double e, s = ddm::two_sum(phi[c], gv, e);
+                            phi[c] = ddm::fast_two_sum(s, e + plo[c], plo[c]);
+                        }
+                    }
+                }
+            }
+        }
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&S.tempty[r]);
-    };
-    for (long t = t_begin; t < t_end; ++t) {
-        const int i = I * OZ_ROWS_A + row;
-        const int jb = J * OZ_COLS_B + 16 * h;
+        if (lane == 0) mbar_arrive(&S.tempty[b]);
         const int ei = a.exps[i]; // scale exponent of the row (padded rows hold 0)
-        double acc_hi[16], acc_lo[16];
-        double2 cv[8];
-        if (!wait_full(0)) break;
-        tc_fence_after();
-        oz_drain<0>(a, lane_base, acc_hi, acc_lo);
-        release(0);
-        if (!wait_full(1)) break;
-        tc_fence_after();
-        oz_drain<1>(a, lane_base, acc_hi, acc_lo);
-        release(1);
-        ph ^= 1u;
-        // the next tile's MMAs run while C is read and written
-        oz_load8(a, i, jb, 0, cv);
-        oz_update8(a, i, jb, 0, ei, acc_hi, acc_lo, cv);
-        oz_load8(a, i, jb, 8, cv);
-        oz_update8(a, i, jb, 8, ei, acc_hi, acc_lo, cv);
+        const int4 e0 = *reinterpret_cast<const int4 *>(a.exps + jb), e1 = *reinterpret_cast<const int4 *>(a.exps + jb + 4);
+        const int ej[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int j = jb + c;
+            if (i < a.n && j < a.n && j <= i) {
+                const int sc = ei + ej[c];
+                dd_t p;
+                if (sc >= -1022 && sc <= 1023) {
+                    const double pw = oz_pow2(sc);
+                    p = dd_make(phi[c] * pw, plo[c] * pw);
+                } else {
+                    p = dd_make(ldexp(phi[c], sc), ldexp(plo[c], sc));
+                }
+                const dd_t res = dd_sub(dd_make(cv[c].x, cv[c].y), p);
+                __stcs(reinterpret_cast<double2 *>(a.C + i + a.ldc * (long)j), make_double2(res.hi, res.lo));
+            }
+        }
         oz_tile_next(a.nJ, I, J);
     }
 }
@@ -431,9 +448,12 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_syrk_kernel(OzArgs a) {
     if (tid == 0) {
         S.abort_flag = *(volatile int *)a.err != 0;
         mbar_init(&S.barA, 1);
+        mbar_init(&S.fin, 1);
+        for (int st = 0; st < OZ_STAGES; ++st) {
+            mbar_init(&S.barB[st], 1);
+            mbar_init(&S.bfree[st], 1);
+        }
         for (int b = 0; b < 2; ++b) {
-            mbar_init(&S.barB[b], 1);
-            mbar_init(&S.bfree[b], 1);
             mbar_init(&S.tfull[b], 1);
             mbar_init(&S.tempty[b], 8);
         }
@@ -525,7 +545,7 @@ void ozaki_syrk_sub_lower(cudaStream_t st, const dd_t *P, long ldp, int n, int k
     a.nJ = (int)ceil_div(n, OZ_COLS_B);
     a.err = w.err;
     long tiles = 0;
-    for (int I = 0; I < a.nI; ++I) tiles += std::min(4L * (I + 1), (long)a.nJ);
+    for (int I = 0; I < a.nI; ++I) tiles += std::min((long)(OZ_ROWS_A / OZ_COLS_B) * (I + 1), (long)a.nJ);
     a.tiles = tiles;
     static thread_local int sms[64] = {};
     int dev = 0;

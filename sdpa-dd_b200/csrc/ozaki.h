@@ -10,7 +10,7 @@ namespace sddd {
 constexpr int OZ_MAX_SLICES = 16;
 constexpr int OZ_K = 64;        // panel width the split handles (K of the update)
 constexpr int OZ_ROWS_A = 128;  // output tile rows (MMA M)
-constexpr int OZ_COLS_B = 32;   // output tile columns (MMA N)
+constexpr int OZ_COLS_B = 16;   // output tile columns (per B slice)
 
 // Device workspace of the split: slices for `row_cap` rows (a multiple of
 // 128), row exponents and an error word.
