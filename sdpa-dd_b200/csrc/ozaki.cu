@@ -133,10 +133,6 @@ __device__ __forceinline__ uint64_t oz_desc(uint32_t saddr) {
     return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(512 >> 4) << 32) | (1ull << 46);
 }
 
-// Diagonal groups of the epilogue: group g holds the diagonals d = 2+4g ..
-// 5+4g (those with d <= S+1).
-__host__ __device__ constexpr int oz_groups(int ns) { return (ns + 3) >> 2; }
-
 struct OzArgs {
     const int8_t *slices;
     long slice_stride; // bytes between slices
@@ -314,44 +310,39 @@ __device__ __forceinline__ void tc_ld4(uint32_t taddr, int32_t *r) {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];" : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(taddr));
 }
 
-// Group g of four of this thread's columns, at tb in the accumulator buffer
-// (diagonal d in columns 16 (d - 2) ..): V = 2^21 A_d + 2^14 A_d+1 +
-// 2^7 A_d+2 + A_d+3 (d = 2 + 4g; exact, |V| < 2^44; diagonals beyond S+1
-// count as zero).  Its value is V 2^-(35 + 28 g) in units of 2^(e_i + e_j).
-__device__ __forceinline__ void oz_group4(int ns, int g, uint32_t tb, long long *V) {
-    const int d0 = 2 + 4 * g;
-    int32_t v[4][4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        if (d0 + u <= ns + 1) {
-            tc_ld4(tb + (uint32_t)((d0 + u - 2) * OZ_COLS_B), v[u]);
-        } else {
-#pragma unroll
-            for (int c = 0; c < 4; ++c) v[u][c] = 0;
-        }
-    }
-    tc_wait_ld();
-#pragma unroll
-    for (int c = 0; c < 4; ++c) V[c] = ((long long)v[0][c] << 21) + ((long long)v[1][c] << 14) + ((long long)v[2][c] << 7) + (long long)v[3][c];
+// Exact int64 -> double for |x| < 2^51: the bits of 1.5 * 2^52 plus x are
+// the double 1.5 * 2^52 + x (its significand holds 2^51 + x), from which
+// 1.5 * 2^52 is subtracted exactly (the classic magic-number conversion).
+__device__ __forceinline__ double oz_i2d(long long x) {
+    return __dsub_rn(__longlong_as_double(x + 0x4338000000000000LL), 6755399441055744.0);
+}
+
+// Group g of diagonals (d = 2+4g .. 5+4g) of one entry from its diagonal
+// values v[0..15] (diagonal d at v[d-2]; those beyond S+1 are zero):
+// V = 2^21 A_d + 2^14 A_d+1 + 2^7 A_d+2 + A_d+3, exact (|V| < 2^44; the
+// pairs 2^7 A + A' < 2^30 are exact in int32).  Its value is
+// V 2^-(35 + 28 g) in units of 2^(e_i + e_j).
+__device__ __forceinline__ long long oz_group(const int32_t (*v)[4], int g, int c) {
+    const int32_t p0 = v[4 * g][c] * 128 + v[4 * g + 1][c], p1 = v[4 * g + 2][c] * 128 + v[4 * g + 3][c];
+    return (long long)p0 * 16384 + p1;
 }
 
 // Epilogue warps 1-8: warp w reads tensor-memory lanes 32 (w mod 4) .. +31
 // (its rows of the tile) and columns 8 h .. 8 h + 7 of every diagonal,
-// h = (w - 1) / 4.  The groups come smallest first.  Groups g >= 2
-// (diagonals 10..17) fold exactly into one int64 per entry in units of
-// 2^-104 (group 2 shifted up by 13 bits, group 3 down by 15 with rounding:
-// |carry| < 2^58, the rounding at most 2^-105).  Group 1 and the carry
-// become a dd (the group's exact double, the carry as two exact doubles,
-// two TwoSums); group 0, an exact double, is added to it; the sum is scaled
-// by 2^(e_i + e_j) and subtracted from C, whose entries were requested
-// before the wait for the accumulators.
+// h = (w - 1) / 4, four columns at a time with all diagonals in one round
+// trip.  Per entry, groups 3 and 2 fold exactly into an int64 carry in
+// units of 2^-104 (group 2 shifted up by 13 bits, group 3 down by 15 with
+// rounding: |carry| < 2^58, the rounding at most 2^-105); group 1 and the
+// carry become a dd (three exact doubles, two TwoSums); group 0, an exact
+// double, is added; the sum is scaled by 2^(e_i + e_j) and subtracted from
+// C, whose entries were requested before the wait for the accumulators.
 __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_end) {
     volatile int *abort_flag = &S.abort_flag;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int q = warp & 3, h = (warp - 1) >> 2;
     const int row = 32 * q + lane;
     const uint32_t lane_base = S.tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(8 * h);
-    const int G = oz_groups(a.ns);
+    const int nd = a.ns; // diagonals 2 .. S+1
     int I, J;
     oz_tile_at(t_begin, a.nI, a.nJ, I, J);
     // lane 0 waits; the warp follows its outcome (the tensor-memory loads
@@ -374,63 +365,53 @@ __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_e
         if (!wait_full(b, (uint32_t)((n >> 1) & 1))) break;
         tc_fence_after();
         const uint32_t tb = lane_base + (uint32_t)(b * OZ_ACC_COLS);
-        long long acc[8];
-        double phi[8], plo[8];
-        for (int g = G - 1; g >= 0; --g) {
-            const bool first = g == G - 1;
-#pragma unroll
-            for (int ch = 0; ch < 2; ++ch) {
-                long long V[4];
-                oz_group4(a.ns, g, tb + (uint32_t)(4 * ch), V);
-#pragma unroll
-                for (int cc = 0; cc < 4; ++cc) {
-                    const int c = 4 * ch + cc;
-                    const long long Vc = V[cc];
-                    if (g >= 2) {
-                        const int sh = 69 - 28 * g; // 2^(69 - 28 g): units of 2^-104
-                        const long long v = sh >= 0 ? (Vc << sh) : ((Vc + (1LL << (-sh - 1))) >> (-sh));
-                        acc[c] = first ? v : acc[c] + v;
-                    } else if (g == 1) {
-                        const long long A = first ? 0LL : acc[c];
-                        const long long alo = A & 0x3FFFFFFLL, ahi = A - alo; // both exact as doubles
-                        const double gv = __ll2double_rn(Vc) * oz_pow2(-63);
-                        const double ah = __ll2double_rn(ahi) * oz_pow2(-104), al = __ll2double_rn(alo) * oz_pow2(-104);
-                        double e1, s1 = ddm::two_sum(gv, ah, e1);
-                        double e2, s2 = ddm::two_sum(s1, al, e2);
-                        phi[c] = ddm::fast_two_sum(s2, e1 + e2, plo[c]);
-                    } else {
-                        const double gv = __ll2double_rn(Vc) * oz_pow2(-35);
-                        if (first) {
-                            phi[c] = gv;
-                            plo[c] = 0.0;
-                        } else {
-                            double e, s = ddm::two_sum(phi[c], gv, e);
-                            phi[c] = ddm::fast_two_sum(s, e + plo[c], plo[c]);
-                        }
-                    }
-                }
-            }
-        }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&S.tempty[b]);
         const int ei = a.exps[i]; // scale exponent of the row (padded rows hold 0)
         const int4 e0 = *reinterpret_cast<const int4 *>(a.exps + jb), e1 = *reinterpret_cast<const int4 *>(a.exps + jb + 4);
         const int ej[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int j = jb + c;
-            if (i < a.n && j < a.n && j <= i) {
-                const int sc = ei + ej[c];
-                dd_t p;
-                if (sc >= -1022 && sc <= 1023) {
-                    const double pw = oz_pow2(sc);
-                    p = dd_make(phi[c] * pw, plo[c] * pw);
+        for (int ch = 0; ch < 2; ++ch) {
+            int32_t v[OZ_MAX_SLICES][4];
+#pragma unroll
+            for (int u = 0; u < OZ_MAX_SLICES; ++u) {
+                if (u < nd) {
+                    tc_ld4(tb + (uint32_t)(u * OZ_COLS_B + 4 * ch), v[u]);
                 } else {
-                    p = dd_make(ldexp(phi[c], sc), ldexp(plo[c], sc));
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) v[u][c] = 0;
                 }
-                const dd_t res = dd_sub(dd_make(cv[c].x, cv[c].y), p);
-                __stcs(reinterpret_cast<double2 *>(a.C + i + a.ldc * (long)j), make_double2(res.hi, res.lo));
+            }
+            tc_wait_ld();
+            if (ch == 1) { // the buffer is drained
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&S.tempty[b]);
+            }
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int cc = 4 * ch + c;
+                const long long carry = oz_group(v, 2, c) * 8192 + ((oz_group(v, 3, c) + 16384) >> 15);
+                const long long ahi = carry >> 26, alo = carry - ahi * 67108864; // |ahi| < 2^32, 0 <= alo < 2^26
+                const double g1 = oz_i2d(oz_group(v, 1, c)) * 0x1p-63;
+                const double ah = oz_i2d(ahi) * 0x1p-78, al = oz_i2d(alo) * 0x1p-104;
+                double e1, s1 = ddm::two_sum(g1, ah, e1);
+                double e2, s2 = ddm::two_sum(s1, al, e2);
+                double plo, phi = ddm::fast_two_sum(s2, e1 + e2, plo);
+                const double g0 = oz_i2d(oz_group(v, 0, c)) * 0x1p-35;
+                double e3, s3 = ddm::two_sum(phi, g0, e3);
+                phi = ddm::fast_two_sum(s3, e3 + plo, plo);
+                const int j = jb + cc;
+                if (i < a.n && j < a.n && j <= i) {
+                    const int sc = ei + ej[cc];
+                    dd_t p;
+                    if (sc >= -1022 && sc <= 1023) {
+                        const double pw = oz_pow2(sc);
+                        p = dd_make(phi * pw, plo * pw);
+                    } else {
+                        p = dd_make(ldexp(phi, sc), ldexp(plo, sc));
+                    }
+                    const dd_t res = dd_sub(dd_make(cv[cc].x, cv[cc].y), p);
+                    __stcs(reinterpret_cast<double2 *>(a.C + i + a.ldc * (long)j), make_double2(res.hi, res.lo));
+                }
             }
         }
         oz_tile_next(a.nJ, I, J);
