@@ -35,7 +35,7 @@
 // triangle (row-block major, so a CTA keeps its 128-row A slices in shared
 // memory while it walks the columns).  Warp 0 lane 0 stages operands with
 // bulk copies (cp.async.bulk, no multicast; B four tiles deep) and issues
-// the MMAs; warps 1-8 drain tensor memory, which holds two accumulator
+// the MMAs; warps 1-16 drain tensor memory, which holds two accumulator
 // buffers of 16 x 16 columns, so one tile multiplies while the last drains.
 // Operand layout in global and shared memory: per slice, 8-row groups of
 // 512 bytes, each four 128-byte core matrices (8 rows x 16 K-bytes): the
@@ -56,7 +56,11 @@ namespace sddd {
 
 namespace {
 
-constexpr int OZ_THREADS = 288; // warp 0: copies + MMA; warps 1-8: epilogue
+constexpr int OZ_EPI_WARPS = 16; // epilogue warps: four per tensor-memory lane quadrant
+constexpr int OZ_EPI_COLS = OZ_COLS_B / (OZ_EPI_WARPS / 4); // tile columns per epilogue thread
+constexpr int OZ_THREADS = 32 * (1 + OZ_EPI_WARPS); // warp 0: copies + MMA; the rest: epilogue
+// 17 warps put five on one SM sub-partition: 5 x 32 x 96 registers fit its 16384
+constexpr int OZ_MAX_REGS = 96;
 constexpr int OZ_A_BYTES = OZ_ROWS_A * OZ_K; // one slice of a 128-row block
 constexpr int OZ_B_BYTES = OZ_COLS_B * OZ_K; // one slice of a 16-row block
 constexpr int OZ_TILE_B = OZ_MAX_SLICES * OZ_B_BYTES; // the stacked B slices of a tile
@@ -119,11 +123,6 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_commit(uint64_t *b) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(b)) : "memory");
-}
-__device__ __forceinline__ void tc_ld8(uint32_t taddr, int32_t *r) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr));
 }
 __device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
@@ -306,8 +305,8 @@ __device__ void oz_producer(const OzArgs &a, OzShared &S, uint8_t *smA, uint8_t 
 // 2^e as a double for -1022 <= e <= 1023 (built from its bits)
 __device__ __forceinline__ double oz_pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
 
-__device__ __forceinline__ void tc_ld4(uint32_t taddr, int32_t *r) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];" : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(taddr));
+__device__ __forceinline__ void tc_ld2(uint32_t taddr, int32_t *r) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(taddr));
 }
 
 // Exact int64 -> double for |x| < 2^51: the bits of 1.5 * 2^52 plus x are
@@ -322,14 +321,14 @@ __device__ __forceinline__ double oz_i2d(long long x) {
 // V = 2^21 A_d + 2^14 A_d+1 + 2^7 A_d+2 + A_d+3, exact (|V| < 2^44; the
 // pairs 2^7 A + A' < 2^30 are exact in int32).  Its value is
 // V 2^-(35 + 28 g) in units of 2^(e_i + e_j).
-__device__ __forceinline__ long long oz_group(const int32_t (*v)[4], int g, int c) {
+__device__ __forceinline__ long long oz_group(const int32_t (*v)[2], int g, int c) {
     const int32_t p0 = v[4 * g][c] * 128 + v[4 * g + 1][c], p1 = v[4 * g + 2][c] * 128 + v[4 * g + 3][c];
     return (long long)p0 * 16384 + p1;
 }
 
-// Epilogue warps 1-8: warp w reads tensor-memory lanes 32 (w mod 4) .. +31
-// (its rows of the tile) and columns 8 h .. 8 h + 7 of every diagonal,
-// h = (w - 1) / 4, four columns at a time with all diagonals in one round
+// Epilogue warps 1-16: warp w reads tensor-memory lanes 32 (w mod 4) .. +31
+// (its rows of the tile) and columns 4 h .. 4 h + 3 of every diagonal,
+// h = (w - 1) / 4, two columns at a time with all diagonals in one round
 // trip.  Per entry, groups 3 and 2 fold exactly into an int64 carry in
 // units of 2^-104 (group 2 shifted up by 13 bits, group 3 down by 15 with
 // rounding: |carry| < 2^58, the rounding at most 2^-105); group 1 and the
@@ -341,7 +340,7 @@ __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_e
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int q = warp & 3, h = (warp - 1) >> 2;
     const int row = 32 * q + lane;
-    const uint32_t lane_base = S.tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(8 * h);
+    const uint32_t lane_base = S.tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(OZ_EPI_COLS * h);
     const int nd = a.ns; // diagonals 2 .. S+1
     int I, J;
     oz_tile_at(t_begin, a.nI, a.nJ, I, J);
@@ -354,11 +353,11 @@ __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_e
     };
     for (long n = 0; n < t_end - t_begin; ++n) {
         const int i = I * OZ_ROWS_A + row;
-        const int jb = J * OZ_COLS_B + 8 * h;
+        const int jb = J * OZ_COLS_B + OZ_EPI_COLS * h;
         const int b = (int)(n & 1);
-        double2 cv[8];
+        double2 cv[OZ_EPI_COLS];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
+        for (int c = 0; c < OZ_EPI_COLS; ++c) {
             const int j = jb + c;
             cv[c] = (i < a.n && j < a.n && j <= i) ? __ldcs(reinterpret_cast<const double2 *>(a.C + i + a.ldc * (long)j)) : make_double2(0.0, 0.0);
         }
@@ -366,29 +365,29 @@ __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_e
         tc_fence_after();
         const uint32_t tb = lane_base + (uint32_t)(b * OZ_ACC_COLS);
         const int ei = a.exps[i]; // scale exponent of the row (padded rows hold 0)
-        const int4 e0 = *reinterpret_cast<const int4 *>(a.exps + jb), e1 = *reinterpret_cast<const int4 *>(a.exps + jb + 4);
-        const int ej[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+        const int4 e4 = *reinterpret_cast<const int4 *>(a.exps + jb);
+        const int ej[4] = {e4.x, e4.y, e4.z, e4.w};
 #pragma unroll
-        for (int ch = 0; ch < 2; ++ch) {
-            int32_t v[OZ_MAX_SLICES][4];
+        for (int ch = 0; ch < OZ_EPI_COLS / 2; ++ch) {
+            int32_t v[OZ_MAX_SLICES][2];
 #pragma unroll
             for (int u = 0; u < OZ_MAX_SLICES; ++u) {
                 if (u < nd) {
-                    tc_ld4(tb + (uint32_t)(u * OZ_COLS_B + 4 * ch), v[u]);
+                    tc_ld2(tb + (uint32_t)(u * OZ_COLS_B + 2 * ch), v[u]);
                 } else {
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) v[u][c] = 0;
+                    v[u][0] = 0;
+                    v[u][1] = 0;
                 }
             }
             tc_wait_ld();
-            if (ch == 1) { // the buffer is drained
+            if (ch == OZ_EPI_COLS / 2 - 1) { // the buffer is drained
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&S.tempty[b]);
             }
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const int cc = 4 * ch + c;
+            for (int c = 0; c < 2; ++c) {
+                const int cc = 2 * ch + c;
                 const long long carry = oz_group(v, 2, c) * 8192 + ((oz_group(v, 3, c) + 16384) >> 15);
                 const long long ahi = carry >> 26, alo = carry - ahi * 67108864; // |ahi| < 2^32, 0 <= alo < 2^26
                 const double g1 = oz_i2d(oz_group(v, 1, c)) * 0x1p-63;
@@ -418,7 +417,7 @@ __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_e
     }
 }
 
-__global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_syrk_kernel(OzArgs a) {
+__global__ void __maxnreg__(OZ_MAX_REGS) ozaki_syrk_kernel(OzArgs a) {
     extern __shared__ uint8_t oz_raw[];
     __shared__ OzShared S;
     uint8_t *smA = reinterpret_cast<uint8_t *>(((uintptr_t)oz_raw + 1023) & ~(uintptr_t)1023);
@@ -436,7 +435,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_syrk_kernel(OzArgs a) {
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&S.tfull[b], 1);
-            mbar_init(&S.tempty[b], 8);
+            mbar_init(&S.tempty[b], OZ_EPI_WARPS);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
