@@ -309,11 +309,14 @@ __device__ __forceinline__ void tc_ld2(uint32_t taddr, int32_t *r) {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(taddr));
 }
 
-// Exact int64 -> double for |x| < 2^51: the bits of 1.5 * 2^52 plus x are
-// the double 1.5 * 2^52 + x (its significand holds 2^51 + x), from which
-// 1.5 * 2^52 is subtracted exactly (the classic magic-number conversion).
+// Exact x 2^-K as a double for integer |x| < 2^51 (the magic-number
+// conversion): the double M = 1.5 * 2^(52-K) has ulp 2^-K, so its bits plus
+// x are the double M + x 2^-K (the significand holds 2^51 + x), from which
+// M is subtracted exactly.
+template <int K>
 __device__ __forceinline__ double oz_i2d(long long x) {
-    return __dsub_rn(__longlong_as_double(x + 0x4338000000000000LL), 6755399441055744.0);
+    constexpr long long bits = ((long long)(1023 + 52 - K) << 52) | (1LL << 51);
+    return __dsub_rn(__longlong_as_double(x + bits), __longlong_as_double(bits));
 }
 
 // Group g of diagonals (d = 2+4g .. 5+4g) of one entry from its diagonal
@@ -326,22 +329,43 @@ __device__ __forceinline__ long long oz_group(const int32_t (*v)[2], int g, int 
     return (long long)p0 * 16384 + p1;
 }
 
+// Exact sum of the diagonals of one entry as a dd, from its diagonal
+// values v[0..15] (diagonal d at v[d-2]; those beyond S+1 are zero), in
+// units of 2^(e_i + e_j).  With the groups V_g (oz_group) the value is
+// V0 2^-35 + V1 2^-63 + V2 2^-91 + V3 2^-119.  Groups 2 and 3 fold into an
+// int64 carry in units of 2^-104 (V3 rounded: at most 2^-105, |carry| <
+// 2^58); T = V0 2^69 + V1 2^41 + carry (|T| < 2^109, |V0| < 2^40) is
+// formed exactly as a 128-bit integer H 2^64 + L and cut into
+// t2 2^84 + t1 2^42 + t0 (0 <= t0, t1 < 2^42, |t2| < 2^25), three exact
+// doubles; TwoSum of the top two, the third added to the error (exact but
+// for 2^-106 of the value) and a FastTwoSum give the dd.
+__device__ __forceinline__ void oz_entry_dd(const int32_t (*v)[2], int c, double &hi, double &lo) {
+    const long long V0 = oz_group(v, 0, c), V1 = oz_group(v, 1, c);
+    const long long carry = oz_group(v, 2, c) * 8192 + ((oz_group(v, 3, c) + 16384) >> 15);
+    const unsigned long long l1 = (unsigned long long)V1 << 41, L = l1 + (unsigned long long)carry;
+    const long long H = V0 * 32 + (V1 >> 23) + (carry >> 63) + (L < l1 ? 1 : 0);
+    const long long t0 = (long long)(L & 0x3FFFFFFFFFFULL);
+    const long long t1 = (long long)((L >> 42) | ((unsigned long long)(H & 0xFFFFF) << 22));
+    const long long t2 = H >> 20;
+    const double d2 = oz_i2d<20>(t2), d1 = oz_i2d<62>(t1), d0 = oz_i2d<104>(t0);
+    double e, s = ddm::two_sum(d2, d1, e);
+    hi = ddm::fast_two_sum(s, e + d0, lo);
+}
+
 // Epilogue warps 1-16: warp w reads tensor-memory lanes 32 (w mod 4) .. +31
 // (its rows of the tile) and columns 4 h .. 4 h + 3 of every diagonal,
 // h = (w - 1) / 4, two columns at a time with all diagonals in one round
-// trip.  Per entry, groups 3 and 2 fold exactly into an int64 carry in
-// units of 2^-104 (group 2 shifted up by 13 bits, group 3 down by 15 with
-// rounding: |carry| < 2^58, the rounding at most 2^-105); group 1 and the
-// carry become a dd (three exact doubles, two TwoSums); group 0, an exact
-// double, is added; the sum is scaled by 2^(e_i + e_j) and subtracted from
-// C, whose entries were requested before the wait for the accumulators.
+// trip; each entry's dd (oz_entry_dd) is scaled by 2^(e_i + e_j) and
+// subtracted from C, whose entries were requested before the wait for the
+// accumulators.  NSC: the slice count when known at compile time, else 0.
+template <int NSC>
 __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_end) {
     volatile int *abort_flag = &S.abort_flag;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int q = warp & 3, h = (warp - 1) >> 2;
     const int row = 32 * q + lane;
     const uint32_t lane_base = S.tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(OZ_EPI_COLS * h);
-    const int nd = a.ns; // diagonals 2 .. S+1
+    const int nd = NSC > 0 ? NSC : a.ns; // diagonals 2 .. S+1
     int I, J;
     oz_tile_at(t_begin, a.nI, a.nJ, I, J);
     // lane 0 waits; the warp follows its outcome (the tensor-memory loads
@@ -355,12 +379,13 @@ __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_e
         const int i = I * OZ_ROWS_A + row;
         const int jb = J * OZ_COLS_B + OZ_EPI_COLS * h;
         const int b = (int)(n & 1);
+        dd_t *cp = a.C + i + a.ldc * (long)jb;
+        // entries of the lower triangle of C: columns jb .. jb + ncol - 1
+        const int ncol = i < a.n ? max(0, min(OZ_EPI_COLS, min(a.n, i + 1) - jb)) : 0;
         double2 cv[OZ_EPI_COLS];
 #pragma unroll
-        for (int c = 0; c < OZ_EPI_COLS; ++c) {
-            const int j = jb + c;
-            cv[c] = (i < a.n && j < a.n && j <= i) ? __ldcs(reinterpret_cast<const double2 *>(a.C + i + a.ldc * (long)j)) : make_double2(0.0, 0.0);
-        }
+        for (int c = 0; c < OZ_EPI_COLS; ++c)
+            cv[c] = c < ncol ? __ldcs(reinterpret_cast<const double2 *>(cp + a.ldc * (long)c)) : make_double2(0.0, 0.0);
         if (!wait_full(b, (uint32_t)((n >> 1) & 1))) break;
         tc_fence_after();
         const uint32_t tb = lane_base + (uint32_t)(b * OZ_ACC_COLS);
@@ -388,18 +413,9 @@ __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_e
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
                 const int cc = 2 * ch + c;
-                const long long carry = oz_group(v, 2, c) * 8192 + ((oz_group(v, 3, c) + 16384) >> 15);
-                const long long ahi = carry >> 26, alo = carry - ahi * 67108864; // |ahi| < 2^32, 0 <= alo < 2^26
-                const double g1 = oz_i2d(oz_group(v, 1, c)) * 0x1p-63;
-                const double ah = oz_i2d(ahi) * 0x1p-78, al = oz_i2d(alo) * 0x1p-104;
-                double e1, s1 = ddm::two_sum(g1, ah, e1);
-                double e2, s2 = ddm::two_sum(s1, al, e2);
-                double plo, phi = ddm::fast_two_sum(s2, e1 + e2, plo);
-                const double g0 = oz_i2d(oz_group(v, 0, c)) * 0x1p-35;
-                double e3, s3 = ddm::two_sum(phi, g0, e3);
-                phi = ddm::fast_two_sum(s3, e3 + plo, plo);
-                const int j = jb + cc;
-                if (i < a.n && j < a.n && j <= i) {
+                double phi, plo;
+                oz_entry_dd(v, c, phi, plo);
+                if (cc < ncol) {
                     const int sc = ei + ej[cc];
                     dd_t p;
                     if (sc >= -1022 && sc <= 1023) {
@@ -409,7 +425,7 @@ __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_e
                         p = dd_make(ldexp(phi, sc), ldexp(plo, sc));
                     }
                     const dd_t res = dd_sub(dd_make(cv[cc].x, cv[cc].y), p);
-                    __stcs(reinterpret_cast<double2 *>(a.C + i + a.ldc * (long)j), make_double2(res.hi, res.lo));
+                    __stcs(reinterpret_cast<double2 *>(cp + a.ldc * (long)cc), make_double2(res.hi, res.lo));
                 }
             }
         }
@@ -453,7 +469,10 @@ __global__ void __maxnreg__(OZ_MAX_REGS) ozaki_syrk_kernel(OzArgs a) {
         if ((tid & 31) == 0) oz_producer(a, S, smA, smB, t_begin, t_end);
         __syncwarp();
     } else {
-        oz_epilogue(a, S, t_begin, t_end);
+        if (a.ns == OZ_MAX_SLICES)
+            oz_epilogue<OZ_MAX_SLICES>(a, S, t_begin, t_end);
+        else
+            oz_epilogue<0>(a, S, t_begin, t_end);
     }
     tc_fence_before();
     __syncthreads();
