@@ -155,7 +155,8 @@ void gemm(cudaStream_t st, char ta, char tb, int mode, int M, int N, int K, cons
 // test, mplapack/Rpotrf2.cpp).  1/L(j,j) for the panel goes to rdiag.
 // Step k: warp 0 takes column k+1 through its step-k update, its pivot
 // (sqrt, reciprocal) and its scaling, while the other warps apply the
-// step-k update to columns k+2 and beyond; one barrier per step.  Every
+// step-k update to columns k+2 and beyond (one column per warp at a time,
+// one row per lane); one barrier per step.  Every
 // entry sees the same operations in the same order as the column-by-column
 // form: x(i,j) -= L(j,k) L(i,k) for k ascending, then the scaling.
 constexpr int DIAG_THREADS = 1024;
@@ -210,11 +211,11 @@ __global__ void __launch_bounds__(DIAG_THREADS) potrf_diag_kernel(dd_t *A, long 
             __syncwarp();
             finish_column(k + 1);
         } else {
-            const int w = nb - k - 2;
-            for (int p = tid - 32; p < w * w; p += nt - 32) {
-                const int i = k + 2 + p % w, j = k + 2 + p / w;
-                if (i < j) continue;
-                put(i, j, dd_sub(at(i, j), dd_mul(at(j, k), at(i, k))));
+            // warps 1.. take the columns k+2.. round-robin, lanes the rows
+            // of the column's lower part
+            for (int j = k + 2 + warp - 1; j < nb; j += nt / 32 - 1) {
+                const dd_t ljk = at(j, k);
+                for (int i = j + lane; i < nb; i += 32) put(i, j, dd_sub(at(i, j), dd_mul(ljk, at(i, k))));
             }
         }
         __syncthreads();
@@ -233,6 +234,7 @@ __global__ void __launch_bounds__(DIAG_THREADS) potrf_diag_kernel(dd_t *A, long 
 // from its entries right of k and, for column k+1, applies the scaling at
 // once (the entry is final then): one barrier per step.
 constexpr int PANEL_ROWS = 32;
+static_assert(PANEL_ROWS == 32, "potrf_panel_kernel maps one row to each lane");
 constexpr int PANEL_THREADS = 512;
 __global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, long lda, int n, int nb, int c0, const int *info, const dd_t *rdiag) {
     extern __shared__ double2 sm[];
@@ -263,14 +265,19 @@ __global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, lon
             P[e] = make_double2(x.hi, x.lo);
         }
     __syncthreads();
+    // lane = row (PANEL_ROWS = 32), warps take the columns right of k
+    // round-robin
+    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     for (int k = 0; k + 1 < nb; ++k) {
-        for (int e = tid; e < PANEL_ROWS * nb; e += nt) {
-            const int i = e % PANEL_ROWS, j = e / PANEL_ROWS;
-            if (j <= k || i >= rows) continue;
-            const double2 ljk = L11[j + nb * k], xik = P[i + PANEL_ROWS * k], v = P[e];
-            dd_t y = dd_sub(dd_make(v.x, v.y), dd_mul(dd_make(ljk.x, ljk.y), dd_make(xik.x, xik.y)));
-            if (j == k + 1) y = dd_mul(rk(k + 1), y);
-            P[e] = make_double2(y.hi, y.lo);
+        if (lane < rows) {
+            const double2 xik = P[lane + PANEL_ROWS * k];
+            const dd_t x_ik = dd_make(xik.x, xik.y);
+            for (int j = k + 1 + warp; j < nb; j += nw) {
+                const double2 ljk = L11[j + nb * k], v = P[lane + PANEL_ROWS * j];
+                dd_t y = dd_sub(dd_make(v.x, v.y), dd_mul(dd_make(ljk.x, ljk.y), x_ik));
+                if (j == k + 1) y = dd_mul(rk(k + 1), y);
+                P[lane + PANEL_ROWS * j] = make_double2(y.hi, y.lo);
+            }
         }
         __syncthreads();
     }
