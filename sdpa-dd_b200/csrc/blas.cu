@@ -287,6 +287,21 @@ __global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, lon
     }
 }
 
+// The next diagonal block's update by the panel just solved, ahead of the
+// trailing update (the split form's lookahead): D(i, j) -= P(j, k) P(i, k)
+// for k ascending, i >= j; CTA j takes column j, thread i row i.  D is the
+// nb x nb block at c0, P its rows of the nbp panel columns before c0.
+__global__ void potrf_diag_pre_kernel(dd_t *A, long lda, int c0, int nb, int nbp, const int *info) {
+    if (*info != 0) return;
+    const int j = blockIdx.x, i = threadIdx.x;
+    if (i < j || i >= nb) return;
+    const dd_t *P = A + c0 + lda * (long)(c0 - nbp);
+    dd_t *d = A + (c0 + i) + lda * (long)(c0 + j);
+    dd_t x = ld_dd(d);
+    for (int k = 0; k < nbp; ++k) x = dd_sub(x, dd_mul(ld_dd(P + j + lda * (long)k), ld_dd(P + i + lda * (long)k)));
+    st_dd(d, x);
+}
+
 // Right-looking blocked Cholesky: per panel of POTRF_NB columns, factor the
 // diagonal block, solve the rows below, then subtract the panel's outer
 // product from the trailing lower triangle (GEMM_SUB keeps each entry's
@@ -303,6 +318,49 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
         CK(cudaFuncSetAttribute(potrf_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag));
         CK(cudaFuncSetAttribute(potrf_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_panel));
         attr[dev & 63] = true;
+    }
+    if (tc && tc->side && n > 2 * nbmax) {
+        // Split form with one block of lookahead: after panel k, the next
+        // diagonal block takes panel k's update in dd (a small kernel) and
+        // is factored on the side stream, on an SM the trailing update
+        // leaves free, while the trailing update of panel k (all but that
+        // block) runs; panel k+1 waits for both.
+        {
+            PROF_SCOPE("potrf_diag", st);
+            potrf_diag_kernel<<<1, DIAG_THREADS, sizeof(double2) * nbmax * nbmax, st>>>(A, lda, nbmax, 0, info_dev, rdiag_dev);
+            CK_LAUNCH();
+        }
+        for (int c0 = 0;; c0 += nbmax) {
+            const int nb = std::min(nbmax, n - c0);
+            const int below = n - c0 - nb;
+            if (below <= 0) break;
+            {
+                PROF_SCOPE("potrf_panel", st);
+                potrf_panel_kernel<<<ceil_div(below, PANEL_ROWS), PANEL_THREADS, sizeof(double2) * (nb * nb + PANEL_ROWS * nb + nb), st>>>(
+                    A, lda, n, nb, c0, info_dev, rdiag_dev);
+                CK_LAUNCH();
+            }
+            const int c1 = c0 + nb, nb1 = std::min(nbmax, n - c1);
+            {
+                PROF_SCOPE("potrf_diag_pre", st);
+                potrf_diag_pre_kernel<<<nb1, nbmax, 0, st>>>(A, lda, c1, nb1, nb, info_dev);
+                CK_LAUNCH();
+            }
+            CK(cudaEventRecord(tc->ev_pre, st));
+            CK(cudaStreamWaitEvent(tc->side, tc->ev_pre, 0));
+            {
+                PROF_SCOPE("potrf_diag", tc->side);
+                potrf_diag_kernel<<<1, DIAG_THREADS, sizeof(double2) * nb1 * nb1, tc->side>>>(A, lda, nb1, c1, info_dev, rdiag_dev);
+                CK_LAUNCH();
+            }
+            CK(cudaEventRecord(tc->ev_diag, tc->side));
+            if (below > nb1) {
+                PROF_SCOPE("potrf_trailing_update_tc", st);
+                ozaki_syrk_sub_lower(st, A + c1 + lda * (long)c0, lda, below, nb, A + c1 + lda * (long)c1, lda, *tc, nb1, 1);
+            }
+            CK(cudaStreamWaitEvent(st, tc->ev_diag, 0));
+        }
+        return;
     }
     for (int c0 = 0; c0 < n; c0 += nbmax) {
         const int nb = std::min(nbmax, n - c0);

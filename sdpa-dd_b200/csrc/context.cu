@@ -40,6 +40,9 @@ BlockView BlockDev::view() const {
 }
 
 Context::~Context() {
+    if (tc.ev_pre) cudaEventDestroy(tc.ev_pre);
+    if (tc.ev_diag) cudaEventDestroy(tc.ev_diag);
+    if (tc.side) cudaStreamDestroy(tc.side);
     if (sync_ev) cudaEventDestroy(sync_ev);
     if (stream) cudaStreamDestroy(stream);
     if (h_pin) cudaFreeHost(h_pin);
@@ -91,6 +94,11 @@ OzakiWork &tc_work(Context &c, int n, int slices) {
         c.tc.h_err = static_cast<int *>(c.h_pin);
         c.tc.wait_ev = c.sync_ev;
         c.tc.row_cap = rows;
+    }
+    if (!c.tc.side) {
+        CK(cudaStreamCreateWithFlags(&c.tc.side, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c.tc.ev_pre, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c.tc.ev_diag, cudaEventDisableTiming));
     }
     c.tc.slices_used = slices;
     return c.tc;

@@ -139,6 +139,7 @@ struct OzArgs {
     dd_t *C;
     long ldc;
     int n, ns, nI, nJ;
+    int skip; // rows below skip are not written (their block is updated elsewhere)
     long tiles;
     int *err;
 };
@@ -381,7 +382,7 @@ __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_e
         const int b = (int)(n & 1);
         dd_t *cp = a.C + i + a.ldc * (long)jb;
         // entries of the lower triangle of C: columns jb .. jb + ncol - 1
-        const int ncol = i < a.n ? max(0, min(OZ_EPI_COLS, min(a.n, i + 1) - jb)) : 0;
+        const int ncol = (i < a.n && i >= a.skip) ? max(0, min(OZ_EPI_COLS, min(a.n, i + 1) - jb)) : 0;
         double2 cv[OZ_EPI_COLS];
 #pragma unroll
         for (int c = 0; c < OZ_EPI_COLS; ++c)
@@ -523,7 +524,7 @@ __global__ void __launch_bounds__(128) ozaki_split_kernel(const dd_t *P, long ld
 
 } // namespace
 
-void ozaki_syrk_sub_lower(cudaStream_t st, const dd_t *P, long ldp, int n, int k, dd_t *C, long ldc, OzakiWork &w) {
+void ozaki_syrk_sub_lower(cudaStream_t st, const dd_t *P, long ldp, int n, int k, dd_t *C, long ldc, OzakiWork &w, int skip, int reserve_sms) {
     if (n <= 0 || k <= 0) return;
     if (k > OZ_K) throw Error(ERR_ARG, "ozaki: panel wider than 64 columns");
     if (w.slices_used < 8 || w.slices_used > OZ_MAX_SLICES) throw Error(ERR_ARG, "ozaki: slice count must be 8..16");
@@ -542,6 +543,7 @@ void ozaki_syrk_sub_lower(cudaStream_t st, const dd_t *P, long ldp, int n, int k
     a.ns = w.slices_used;
     a.nI = rows / OZ_ROWS_A;
     a.nJ = (int)ceil_div(n, OZ_COLS_B);
+    a.skip = skip;
     a.err = w.err;
     long tiles = 0;
     for (int I = 0; I < a.nI; ++I) tiles += std::min((long)(OZ_ROWS_A / OZ_COLS_B) * (I + 1), (long)a.nJ);
@@ -554,7 +556,7 @@ void ozaki_syrk_sub_lower(cudaStream_t st, const dd_t *P, long ldp, int n, int k
         CK(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev));
         CK(cudaFuncSetAttribute(ozaki_syrk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)OZ_SMEM));
     }
-    const int grid = (int)std::min<long>(sm, tiles);
+    const int grid = (int)std::min<long>(std::max(1, sm - reserve_sms), tiles);
     ozaki_syrk_kernel<<<grid, OZ_THREADS, OZ_SMEM, st>>>(a);
     CK_LAUNCH();
 }

@@ -22,11 +22,19 @@ struct OzakiWork {
     cudaEvent_t wait_ev = nullptr; // blocking-sync event to wait on (or null: stream sync)
     int row_cap = 0;
     int slices_used = 16;     // 7-bit slices per value (8..16)
+    // the Cholesky's lookahead: the next diagonal block is factored on
+    // `side` while the trailing update runs (ev_pre: its block is ready;
+    // ev_diag: it is factored)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_pre = nullptr, ev_diag = nullptr;
 };
 
 // C(i, j) -= sum_k P(i, k) P(j, k) for rows/cols < n with i >= j; P is
 // n x k (k <= 64) column-major with leading dimension ldp, C n x n with ldc.
-void ozaki_syrk_sub_lower(cudaStream_t st, const dd_t *P, long ldp, int n, int k, dd_t *C, long ldc, OzakiWork &w);
+// Rows below `skip` (the leading skip x skip block, updated elsewhere) are
+// left alone; `reserve_sms` SMs are left free for concurrent kernels.
+void ozaki_syrk_sub_lower(cudaStream_t st, const dd_t *P, long ldp, int n, int k, dd_t *C, long ldc, OzakiWork &w, int skip = 0,
+                          int reserve_sms = 0);
 // Throws when a launch since the last check gave up waiting (synchronises st).
 void ozaki_check(cudaStream_t st, const OzakiWork &w);
 
