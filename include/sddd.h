@@ -144,6 +144,19 @@ int sddd_set(sddd_ctx *ctx, int what, const sddd_dd *in);
 int sddd_read_initial_point(sddd_ctx *ctx, const char *path, int sparse, double lambda);
 int sddd_set_initial_point(sddd_ctx *ctx, const sddd_dd *x, const sddd_dd *X, const sddd_dd *Y);
 int sddd_clear_initial_point(sddd_ctx *ctx);
+/* The current point (after a solve: the final one) as an initial-point file
+ * that sddd_read_initial_point, the -id / -is options and the reference's
+ * own reader (sdpa_io.cpp:152-283) take, every number with 34 significant
+ * digits, so a later solve can start from it (warm start, checkpoint).  The
+ * reference writes only the high doubles of its result (sdpa_io.cpp:1205-
+ * 1234, SURVEY's full-precision result I/O); read back, this file gives the
+ * dd point to a few units in its last place.  sparse != 0: "target block i
+ * j value" lines (diagonal always, other zeros left out); else dense. */
+int sddd_write_point(sddd_ctx *ctx, const char *path, int sparse);
+/* v as a correctly rounded decimal string of `digits` (1..60) significant
+ * digits ("d.ddd...e+XX"), exact from hi + lo; writes at most len bytes with
+ * the terminating zero and returns the string length (needs no device). */
+int sddd_dd_to_decimal(sddd_dd v, int digits, char *buf, int len);
 
 /* -- the whole solve (pinpal) -- */
 /* display/result may be NULL.  The result file gets the reference's

@@ -105,6 +105,8 @@ def lib() -> ctypes.CDLL:
         "sddd_read_initial_point": (ci, [vp, ctypes.c_char_p, ci, cd]),
         "sddd_set_initial_point": (ci, [vp, vp, vp, vp]),
         "sddd_clear_initial_point": (ci, [vp]),
+        "sddd_write_point": (ci, [vp, ctypes.c_char_p, ci]),
+        "sddd_dd_to_decimal": (ci, [SdddDD, ci, ctypes.c_char_p, ci]),
         "sddd_batch_create": (ci, [ci, ci, ctypes.POINTER(vp)]),
         "sddd_batch_destroy": (ci, [vp]),
         "sddd_batch_last_error": (ctypes.c_char_p, [vp]),

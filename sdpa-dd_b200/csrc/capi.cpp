@@ -414,6 +414,36 @@ int sddd_set_initial_point(sddd_ctx *ctx, const sddd_dd *x, const sddd_dd *X, co
     });
 }
 
+int sddd_write_point(sddd_ctx *ctx, const char *path, int sparse) {
+    if (!path) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        std::vector<dd_t> X(c.space_len), Z(c.space_len), y(c.m);
+        sddd::space_to_host(c, c.X, X.data());
+        sddd::space_to_host(c, c.Z, Z.data());
+        CK(cudaMemcpyAsync(y.data(), c.y.p, sizeof(dd_t) * c.m, cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+        const std::string text = sddd::write_init_point_text(c.prob, X, y, Z, sparse != 0);
+        FILE *f = std::fopen(path, "wb");
+        if (!f) throw sddd::Error(SDDD_ERR_IO, std::string("cannot open ") + path);
+        const size_t w = std::fwrite(text.data(), 1, text.size(), f);
+        const int rc = std::fclose(f);
+        if (w != text.size() || rc != 0) throw sddd::Error(SDDD_ERR_IO, std::string("cannot write ") + path);
+        return SDDD_OK;
+    });
+}
+
+int sddd_dd_to_decimal(sddd_dd v, int digits, char *buf, int len) {
+    if (!buf || len <= 0 || digits < 1 || digits > 60) return SDDD_ERR_ARG;
+    return guarded(nullptr, [&] {
+        const std::string s = sddd::dd_to_decimal(D(v), digits);
+        const int n = (int)std::min<size_t>(s.size(), (size_t)len - 1);
+        std::memcpy(buf, s.data(), n);
+        buf[n] = 0;
+        return (int)s.size();
+    });
+}
+
 int sddd_clear_initial_point(sddd_ctx *ctx) {
     return guarded(ctx, [&] {
         need_problem(ctx).has_init = false;

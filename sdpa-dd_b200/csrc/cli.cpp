@@ -32,6 +32,8 @@ void usage(const char *argv0) {
     std::printf("  -pt : parameters , 0 default, 1 fast (unstable)\n");
     std::printf("                     2 slow (stable)         \n");
     std::printf("  -tc : slices (8-16) of the tensor-core split Cholesky of the Schur matrix\n");
+    std::printf("  -wd : write the final point, dense  (an init file with 34 digits)\n");
+    std::printf("  -ws : write the final point, sparse (an init file with 34 digits)\n");
     std::printf("example2-1: %s -o example1.result -dd example1.dat\n", argv0);
     std::printf("example2-2: %s -ds example1.dat-s -o example2.result -p param.sdpa\n", argv0);
     std::printf("example2-3: %s -ds example1.dat-s -o example3.result -pt 2\n", argv0);
@@ -56,6 +58,8 @@ extern "C" int sddd_cli_main(int argc, char **argv) {
     std::printf("SDPA-DD start at    %s", std::ctime(&ltime));
     bool isInitFile = false, isInitSparse = false, isDataSparse = false;
     const char *dataFile = nullptr, *initFile = nullptr, *outFile = nullptr, *paraFile = nullptr;
+    const char *pointFile = nullptr; // -wd / -ws: the final point as an init file (this build's extension)
+    bool isPointSparse = false;
     int ptype = 0;
     double kappa = 1.2;
     int device = 0;
@@ -90,6 +94,9 @@ extern "C" int sddd_cli_main(int argc, char **argv) {
                 paraFile = nullptr;
             } else if (!std::strcmp(t, "-tc") && i + 1 < argc) {
                 tc_slices = std::atoi(argv[++i]);
+            } else if ((!std::strcmp(t, "-wd") || !std::strcmp(t, "-ws")) && i + 1 < argc) {
+                isPointSparse = !std::strcmp(t, "-ws");
+                pointFile = argv[++i];
             }
         }
     } else {
@@ -191,6 +198,10 @@ extern "C" int sddd_cli_main(int argc, char **argv) {
     rc = sddd_solve_stream(ctx, &p, stdout, fo, fileRead, &mainLoop);
     const double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (rc != SDDD_OK) std::fprintf(stderr, "%s\n", sddd_last_error(ctx));
+    if (rc == SDDD_OK && pointFile && sddd_write_point(ctx, pointFile, isPointSparse ? 1 : 0) != SDDD_OK) {
+        std::fprintf(stderr, "%s\n", sddd_last_error(ctx));
+        rc = 1;
+    }
     std::printf("  main loop time = %.6f\n", mainLoop);
     std::fprintf(fo, "    main loop time = %.6f\n", mainLoop);
     std::printf("      total time = %.6f\n", total);

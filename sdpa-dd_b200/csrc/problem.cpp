@@ -2,6 +2,7 @@
 #include "problem.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cctype>
 #include <cstdlib>
 #include <cstring>
@@ -325,6 +326,201 @@ void read_init_point(const std::string &path, bool sparse, const Problem &P, dou
     std::stringstream ss;
     ss << f.rdbuf();
     read_init_point_text(ss.str(), sparse, P, lambda, X, y, Z);
+}
+
+// ------------------------------------------------------ exact dd printing
+namespace {
+// Non-negative integer in base 2^32, least significant limb first.
+struct BigNat {
+    std::vector<uint32_t> d;
+    bool zero() const { return d.empty(); }
+    void trim() {
+        while (!d.empty() && d.back() == 0) d.pop_back();
+    }
+    void mul_small(uint32_t f) {
+        uint64_t carry = 0;
+        for (uint32_t &w : d) {
+            const uint64_t t = (uint64_t)w * f + carry;
+            w = (uint32_t)t;
+            carry = t >> 32;
+        }
+        if (carry) d.push_back((uint32_t)carry);
+    }
+    void shl(int k) { // *= 2^k
+        while (k >= 31) {
+            mul_small(1u << 31);
+            k -= 31;
+        }
+        if (k > 0) mul_small(1u << k);
+    }
+    uint32_t div_small(uint32_t q) { // /= q, returns the remainder
+        uint64_t r = 0;
+        for (size_t i = d.size(); i-- > 0;) {
+            const uint64_t t = (r << 32) | d[i];
+            d[i] = (uint32_t)(t / q);
+            r = t % q;
+        }
+        trim();
+        return (uint32_t)r;
+    }
+    static BigNat from(uint64_t v) {
+        BigNat b;
+        while (v) {
+            b.d.push_back((uint32_t)v);
+            v >>= 32;
+        }
+        return b;
+    }
+    // a - b for a >= b
+    static BigNat sub(const BigNat &a, const BigNat &b) {
+        BigNat r = a;
+        int64_t borrow = 0;
+        for (size_t i = 0; i < r.d.size(); ++i) {
+            int64_t t = (int64_t)r.d[i] - borrow - (i < b.d.size() ? (int64_t)b.d[i] : 0);
+            borrow = t < 0;
+            r.d[i] = (uint32_t)(t + (borrow ? (int64_t)1 << 32 : 0));
+        }
+        r.trim();
+        return r;
+    }
+    static BigNat add(const BigNat &a, const BigNat &b) {
+        BigNat r;
+        uint64_t carry = 0;
+        for (size_t i = 0; i < std::max(a.d.size(), b.d.size()); ++i) {
+            const uint64_t t = (uint64_t)(i < a.d.size() ? a.d[i] : 0) + (i < b.d.size() ? b.d[i] : 0) + carry;
+            r.d.push_back((uint32_t)t);
+            carry = t >> 32;
+        }
+        if (carry) r.d.push_back((uint32_t)carry);
+        return r;
+    }
+    std::string decimal() const {
+        if (d.empty()) return "0";
+        BigNat t = *this;
+        std::string out;
+        while (!t.zero()) {
+            uint32_t r = t.div_small(1000000000u);
+            for (int k = 0; k < 9; ++k) {
+                out.push_back((char)('0' + r % 10));
+                r /= 10;
+            }
+        }
+        while (out.size() > 1 && out.back() == '0') out.pop_back();
+        std::reverse(out.begin(), out.end());
+        return out;
+    }
+};
+} // namespace
+
+std::string dd_to_decimal(dd_t x, int digits) {
+    digits = std::max(1, std::min(60, digits));
+    if (std::isnan(x.hi) || std::isnan(x.lo)) return "nan";
+    if (std::isinf(x.hi)) return x.hi > 0 ? "inf" : "-inf";
+    if (x.hi == 0.0 && x.lo == 0.0) return "0";
+    // |x| = |hi| + s |lo| exactly, s = +-1 (|lo| < |hi|); each part an
+    // integer significand times a power of two
+    const bool neg = x.hi < 0.0 || (x.hi == 0.0 && x.lo < 0.0);
+    const double h = std::fabs(x.hi), l = std::fabs(x.lo);
+    const bool same = x.hi == 0.0 || x.lo == 0.0 || ((x.hi < 0.0) == (x.lo < 0.0));
+    int eh = 0, el = 0;
+    const uint64_t mh = h > 0.0 ? (uint64_t)std::ldexp(std::frexp(h, &eh), 53) : 0;
+    const uint64_t ml = l > 0.0 ? (uint64_t)std::ldexp(std::frexp(l, &el), 53) : 0;
+    eh -= 53;
+    el -= 53;
+    const int e = h > 0.0 && l > 0.0 ? std::min(eh, el) : (h > 0.0 ? eh : el);
+    BigNat A = BigNat::from(mh), B = BigNat::from(ml);
+    if (h > 0.0) A.shl(eh - e);
+    if (l > 0.0) B.shl(el - e);
+    BigNat N = same ? BigNat::add(A, B) : BigNat::sub(A, B);
+    // |x| = N 2^e: for e < 0 it is N 5^-e 10^e, an integer times a power of ten
+    int dexp = 0;
+    if (e >= 0) {
+        N.shl(e);
+    } else {
+        for (int k = 0; k < -e; ++k) N.mul_small(5);
+        dexp = e;
+    }
+    std::string s = N.decimal();
+    // round half to even at `digits` significant digits
+    if ((int)s.size() > digits) {
+        const char next = s[digits];
+        bool rest = false;
+        for (size_t k = digits + 1; k < s.size(); ++k) rest |= s[k] != '0';
+        const bool up = next > '5' || (next == '5' && (rest || ((s[digits - 1] - '0') & 1)));
+        dexp += (int)s.size() - digits;
+        s.resize(digits);
+        if (up) {
+            int k = digits - 1;
+            while (k >= 0 && s[k] == '9') s[k--] = '0';
+            if (k >= 0) {
+                s[k]++;
+            } else {
+                s.insert(s.begin(), '1');
+                s.pop_back();
+                dexp += 1;
+            }
+        }
+    }
+    const int exp10 = dexp + (int)s.size() - 1; // of the first digit
+    std::string out = neg ? "-" : "";
+    out += s[0];
+    if (s.size() > 1) {
+        out += '.';
+        out.append(s, 1, std::string::npos);
+    }
+    char eb[16];
+    std::snprintf(eb, sizeof eb, "e%+03d", exp10);
+    return out + eb;
+}
+
+std::string write_init_point_text(const Problem &P, const std::vector<dd_t> &X, const std::vector<dd_t> &y, const std::vector<dd_t> &Z,
+                                  bool sparse) {
+    if (P.nLP > 0) throw Error(ERR_UNSUPPORTED, "initial point: LP blocks are not supported by the device path yet");
+    std::vector<long> off(P.nSDP + 1, 0);
+    for (int l = 0; l < P.nSDP; ++l) off[l + 1] = off[l] + (long)P.sdpSize[l] * P.sdpSize[l];
+    if ((long)X.size() < off[P.nSDP] || (long)Z.size() < off[P.nSDP] || (int)y.size() < P.m) throw Error(ERR_ARG, "initial point: arrays too short");
+    constexpr int D = 34;
+    std::string out = "{";
+    for (int k = 0; k < P.m; ++k) {
+        if (k) out += ',';
+        out += dd_to_decimal(dd_neg(y[k]), D); // the file's x is -y
+    }
+    out += "}\n";
+    if (sparse) {
+        for (int pass = 0; pass < 2; ++pass) { // target 1: internal Z (the file's X); 2: internal X (its Y)
+            const std::vector<dd_t> &M = pass == 0 ? Z : X;
+            for (int l = 0; l < P.nSDP; ++l) {
+                const int n = P.sdpSize[l];
+                for (int i = 0; i < n; ++i)
+                    for (int j = i; j < n; ++j) {
+                        const dd_t v = M[off[l] + i + (long)n * j];
+                        if (i != j && dd_is_zero(v)) continue;
+                        out += std::to_string(pass + 1) + ' ' + std::to_string(l + 1) + ' ' + std::to_string(i + 1) + ' ' + std::to_string(j + 1) + ' ' +
+                               dd_to_decimal(v, D) + '\n';
+                    }
+            }
+        }
+    } else {
+        for (int pass = 0; pass < 2; ++pass) {
+            const std::vector<dd_t> &M = pass == 0 ? Z : X;
+            for (int l = 0; l < P.nSDP; ++l) {
+                const int n = P.sdpSize[l];
+                out += "{ ";
+                for (int i = 0; i < n; ++i) {
+                    out += '{';
+                    for (int j = 0; j < n; ++j) {
+                        if (j) out += ',';
+                        // the reader takes entries with i <= j: write the upper triangle's
+                        // values in both places, so the file is symmetric
+                        out += dd_to_decimal(M[off[l] + std::min(i, j) + (long)n * std::max(i, j)], D);
+                    }
+                    out += i + 1 < n ? "}," : "}";
+                }
+                out += " }\n";
+            }
+        }
+    }
+    return out;
 }
 
 Problem make_problem(int m, int nblock, const int *blockStruct, const dd_t *b, long nnz, const int *k, const int *blk, const int *i, const int *j,

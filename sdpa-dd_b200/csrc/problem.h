@@ -80,6 +80,22 @@ void read_init_point_text(const std::string &text, bool sparse, const Problem &P
 void read_init_point(const std::string &path, bool sparse, const Problem &P, double lambda, std::vector<dd_t> &X, std::vector<dd_t> &y,
                      std::vector<dd_t> &Z);
 
+// hi + lo as a decimal string of `digits` significant digits (1..60),
+// correctly rounded (half to even) from the exact value: "d.ddd...e+XX",
+// "0", "nan", "inf" or "-inf".  The reference prints dd values through QD's
+// to_string; this conversion is exact instead, so a point written with 34
+// digits reads back (QD's parser, as the initial-point reader) to within a
+// few units in the last place of the dd.
+std::string dd_to_decimal(dd_t x, int digits);
+// The inverse of read_init_point_text: a point (internal X, y, Z, block
+// spaces as there) as an initial-point file in the layout that reader takes,
+// every number with 34 significant digits.  Dense: the file's x (= -y) on
+// the first line, then its X (the internal Z) and its Y (the internal X),
+// block by block, row by row.  Sparse: the same x line, then "1 l i j v"
+// (internal Z) and "2 l i j v" (internal X) for i <= j, diagonal always.
+std::string write_init_point_text(const Problem &P, const std::vector<dd_t> &X, const std::vector<dd_t> &y, const std::vector<dd_t> &Z,
+                                  bool sparse);
+
 struct Param {
     int maxIteration = 200;
     double epsilonStar = 1.0e-30, lambdaStar = 1.0e+4, omegaStar = 2.0, lowerBound = -1.0e+5, upperBound = 1.0e+5, betaStar = 0.1, betaBar = 0.3,
