@@ -81,7 +81,12 @@ int sddd_read_problem(sddd_ctx *ctx, const char *path, int sparse, double kappa)
  * block_struct as in the file (negative = LP).  Data is copied. */
 int sddd_upload_problem(sddd_ctx *ctx, int m, int nblock, const int *block_struct, const sddd_dd *b, long nnz, const int *k, const int *blk,
                         const int *i, const int *j, const sddd_dd *val, double kappa);
-/* m, number of SDP blocks, nDim; sizes[] gets the SDP block sizes. */
+/* m, number of SDP blocks, nDim; sizes[] gets the SDP block sizes.  LP
+ * entries (negative block sizes) are carried as SDP blocks of order 1 after
+ * the data's SDP blocks, one per entry in the file's LP order: they count
+ * in nsdp and sizes[], and every block space (points, gradients) holds them
+ * there.  The result file and initial-point files keep the reference's LP
+ * layout. */
 int sddd_dims(const sddd_ctx *ctx, int *m, int *nsdp, long *ndim, int *sizes, int cap);
 /* Length in dd of a block space. */
 long sddd_space_len(const sddd_ctx *ctx);

@@ -337,7 +337,6 @@ static void build_block(Context &c, const Problem &P, int l, BlockDev &bd) {
 }
 
 void upload_problem(Context &c, Problem &&p) {
-    if (p.nLP > 0) throw Error(ERR_UNSUPPORTED, "LP blocks are not supported by the device path yet");
     if (p.nSDP == 0) throw Error(ERR_ARG, "no SDP block");
     CK(cudaSetDevice(c.device));
     c.prob = std::move(p);

@@ -16,7 +16,7 @@ namespace sddd {
 long Problem::nDim() const {
     long s = 0;
     for (int n : sdpSize) s += n;
-    return s + nLP;
+    return s; // the LP entries are among the blocks
 }
 
 // ------------------------------------------------------------ decimal reader
@@ -158,6 +158,9 @@ static void set_blocks(Problem &P, const std::vector<int> &bs) {
             throw Error(ERR_IO, "block struct");
         }
     }
+    P.nSDPdata = P.nSDP;
+    P.sdpSize.insert(P.sdpSize.end(), P.nLP, 1);
+    P.nSDP += P.nLP;
 }
 
 // SparseLinearSpace::setElement_SDP (sdpa_struct.cpp:1217-1249)
@@ -174,12 +177,17 @@ static void add_entry(Problem &P, int k, int l2, int i, int j, dd_t v) {
         M.val.push_back(k == 0 ? dd_neg(v) : v);
         M.effect += (i == j) ? 1 : 2;
     } else {
+        // LP entry i of this block: its order-1 block (a later entry for the
+        // same place overwrites, as change_to_dense keeps the last value)
         if (i != j) throw Error(ERR_IO, "LP part 3rd element != 4th element");
-        int idx = P.blockNumber[l2] + i;
-        if (k == 0)
-            P.lpC[idx] = dd_neg(v);
-        else
-            P.lpA[k - 1].push_back({idx, v});
+        if (i < 0 || i >= P.blockStruct[l2]) throw Error(ERR_IO, "out of range in input data");
+        const int l = P.nSDPdata + P.blockNumber[l2] + i;
+        BlockMat &M = (k == 0) ? P.C[l] : P.A[k - 1][l];
+        M.n = 1;
+        M.row.push_back(0);
+        M.col.push_back(0);
+        M.val.push_back(k == 0 ? dd_neg(v) : v);
+        M.effect += 1;
     }
 }
 
@@ -212,8 +220,6 @@ Problem read_problem_text(const std::string &text, bool sparse) {
         if (!sc.skip_int(bs[l])) throw Error(ERR_IO, "cannot read bLOCKsTRUCT");
     set_blocks(P, bs);
     P.A.resize(P.m);
-    P.lpA.resize(P.m);
-    P.lpC.assign(P.nLP, dd_zero());
     P.b.resize(P.m);
     for (int k = 0; k < P.m; ++k) {
         std::string tok;
@@ -271,7 +277,6 @@ Problem read_problem(const std::string &path, bool sparse) {
 
 void read_init_point_text(const std::string &text, bool sparse, const Problem &P, double lambda, std::vector<dd_t> &X, std::vector<dd_t> &y,
                           std::vector<dd_t> &Z) {
-    if (P.nLP > 0) throw Error(ERR_UNSUPPORTED, "initial point: LP blocks are not supported by the device path yet");
     std::vector<long> off(P.nSDP + 1, 0);
     for (int l = 0; l < P.nSDP; ++l) off[l + 1] = off[l] + (long)P.sdpSize[l] * P.sdpSize[l];
     X.assign(off[P.nSDP], dd_zero());
@@ -300,13 +305,18 @@ void read_init_point_text(const std::string &text, bool sparse, const Problem &P
             double probe;
             if (std::sscanf(tok.c_str(), "%lf", &probe) <= 0) break;
             const dd_t v = dd_parse(tok);
-            if (l > P.nSDP) throw Error(ERR_UNSUPPORTED, "initial point: an entry outside the SDP blocks");
-            set(target == 1 ? Z : X, l - 1, i - 1, j - 1, v);
+            if (l <= P.nSDPdata) {
+                set(target == 1 ? Z : X, l - 1, i - 1, j - 1, v);
+            } else { // the LP part: entry i (setElement_LP)
+                if (i != j) throw Error(ERR_IO, "initial point: LP part 3rd element != 4th element");
+                if (i < 1 || i > P.nLP) throw Error(ERR_IO, "out of range in input data");
+                set(target == 1 ? Z : X, P.nSDPdata + i - 1, 0, 0, v);
+            }
         }
     } else {
         for (int pass = 0; pass < 2; ++pass) { // Z (the file's X), then X (its Y)
             std::vector<dd_t> &M = pass == 0 ? Z : X;
-            for (int l = 0; l < P.nSDP; ++l) {
+            for (int l = 0; l < P.nSDPdata; ++l) {
                 const int n = P.sdpSize[l];
                 for (int i = 0; i < n; ++i)
                     for (int j = 0; j < n; ++j) {
@@ -314,6 +324,11 @@ void read_init_point_text(const std::string &text, bool sparse, const Problem &P
                         const dd_t v = dd_parse(tok);
                         if (i <= j && !dd_is_zero(v)) set(M, l, i, j, v);
                     }
+            }
+            for (int t = 0; t < P.nLP; ++t) { // then the LP part, nonzero entries
+                if (!sc.skip_token(tok)) throw Error(ERR_IO, "initial point: the LP part ended early");
+                const dd_t v = dd_parse(tok);
+                if (!dd_is_zero(v)) set(M, P.nSDPdata + t, 0, 0, v);
             }
         }
     }
@@ -475,7 +490,6 @@ std::string dd_to_decimal(dd_t x, int digits) {
 
 std::string write_init_point_text(const Problem &P, const std::vector<dd_t> &X, const std::vector<dd_t> &y, const std::vector<dd_t> &Z,
                                   bool sparse) {
-    if (P.nLP > 0) throw Error(ERR_UNSUPPORTED, "initial point: LP blocks are not supported by the device path yet");
     std::vector<long> off(P.nSDP + 1, 0);
     for (int l = 0; l < P.nSDP; ++l) off[l + 1] = off[l] + (long)P.sdpSize[l] * P.sdpSize[l];
     if ((long)X.size() < off[P.nSDP] || (long)Z.size() < off[P.nSDP] || (int)y.size() < P.m) throw Error(ERR_ARG, "initial point: arrays too short");
@@ -489,7 +503,10 @@ std::string write_init_point_text(const Problem &P, const std::vector<dd_t> &X, 
     if (sparse) {
         for (int pass = 0; pass < 2; ++pass) { // target 1: internal Z (the file's X); 2: internal X (its Y)
             const std::vector<dd_t> &M = pass == 0 ? Z : X;
-            for (int l = 0; l < P.nSDP; ++l) {
+            for (int t = 0; t < P.nLP; ++t) // the LP part: "target block i i v", block past the SDP ones
+                out += std::to_string(pass + 1) + ' ' + std::to_string(P.nSDPdata + 1) + ' ' + std::to_string(t + 1) + ' ' + std::to_string(t + 1) + ' ' +
+                       dd_to_decimal(M[off[P.nSDPdata + t]], D) + '\n';
+            for (int l = 0; l < P.nSDPdata; ++l) {
                 const int n = P.sdpSize[l];
                 for (int i = 0; i < n; ++i)
                     for (int j = i; j < n; ++j) {
@@ -503,7 +520,7 @@ std::string write_init_point_text(const Problem &P, const std::vector<dd_t> &X, 
     } else {
         for (int pass = 0; pass < 2; ++pass) {
             const std::vector<dd_t> &M = pass == 0 ? Z : X;
-            for (int l = 0; l < P.nSDP; ++l) {
+            for (int l = 0; l < P.nSDPdata; ++l) {
                 const int n = P.sdpSize[l];
                 out += "{ ";
                 for (int i = 0; i < n; ++i) {
@@ -518,6 +535,14 @@ std::string write_init_point_text(const Problem &P, const std::vector<dd_t> &X, 
                 }
                 out += " }\n";
             }
+            if (P.nLP > 0) { // the LP part, one list
+                out += '{';
+                for (int t = 0; t < P.nLP; ++t) {
+                    if (t) out += ',';
+                    out += dd_to_decimal(M[off[P.nSDPdata + t]], D);
+                }
+                out += "}\n";
+            }
         }
     }
     return out;
@@ -530,8 +555,6 @@ Problem make_problem(int m, int nblock, const int *blockStruct, const dd_t *b, l
     P.m = m;
     set_blocks(P, std::vector<int>(blockStruct, blockStruct + nblock));
     P.A.resize(m);
-    P.lpA.resize(m);
-    P.lpC.assign(P.nLP, dd_zero());
     P.b.assign(b, b + m);
     for (long e = 0; e < nnz; ++e) {
         if (k[e] < 0 || k[e] > m) throw Error(ERR_ARG, "constraint index out of range");

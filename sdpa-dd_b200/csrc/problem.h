@@ -36,14 +36,19 @@ struct Problem {
     std::vector<int> blockStruct;  // |size|, after sign handling
     std::vector<int> blockType;    // 1 SDP, 3 LP (sdpa_main.cpp:114-131)
     std::vector<int> blockNumber;  // index within its kind
-    int nSDP = 0, nLP = 0;
-    std::vector<int> sdpSize;      // SDP block sizes
+    // LP entries (negative block sizes) are carried as SDP blocks of order 1,
+    // appended after the data's SDP blocks: the same problem (a 1 x 1
+    // positive semidefinite block is a non-negative scalar, its HKM direction
+    // and step length are the LP ones, and every quantity the loop tests is a
+    // max-abs norm or a sum over all entries), solved by the ordinary path.
+    // Blocks 0 .. nSDPdata-1 are the data's SDP blocks; LP entry t (in
+    // blockNumber order) is block nSDPdata + t.
+    int nSDP = 0, nLP = 0, nSDPdata = 0;
+    std::vector<int> sdpSize;      // SDP block sizes (the LP entries' 1s at the end)
     std::vector<dd_t> b;           // objective of the file (b in SDPA's internal names)
     // C and A[k] by SDP block (C holds -F0 as the reference stores it)
     std::map<int, BlockMat> C;
     std::vector<std::map<int, BlockMat>> A;
-    std::vector<dd_t> lpC;                      // C on LP entries (size nLP)
-    std::vector<std::vector<std::pair<int, dd_t>>> lpA; // per k: (LP index, value)
     std::string title;
     std::vector<std::string> comments;
     // per SDP block l: constraints k touching it, ascending

@@ -564,11 +564,25 @@ static void com_display(FILE *fp, const Timers &t) {
 }
 
 static void display_space_last(FILE *fp, Context &c, const Space &s) {
-    // IO::displayDenseLinarSpaceLast (sdpa_io.cpp:1205-1234), hi parts "%+18.12e"
+    // IO::displayDenseLinarSpaceLast (sdpa_io.cpp:1205-1234), hi parts "%+18.12e",
+    // the data's blocks in their order: an SDP block as a matrix, an LP block
+    // as one list (its entries are the order-1 blocks from nSDPdata on)
     std::vector<dd_t> h(c.space_len);
     space_to_host(c, s, h.data());
+    const Problem &P = c.prob;
     std::fprintf(fp, "{\n");
-    for (int l = 0; l < c.nSDP; ++l) {
+    for (int b = 0; b < P.nBlock; ++b) {
+        if (P.blockType[b] != 1) {
+            const int n = P.blockStruct[b], base = P.nSDPdata + P.blockNumber[b];
+            std::fprintf(fp, "{");
+            for (int t = 0; t < n - 1; ++t) std::fprintf(fp, "%+18.12e,", h[c.off[base + t]].hi);
+            if (n > 0)
+                std::fprintf(fp, "%+18.12e}\n", h[c.off[base + n - 1]].hi);
+            else
+                std::fprintf(fp, "  }\n");
+            continue;
+        }
+        const int l = P.blockNumber[b];
         const int n = c.sizes[l];
         const dd_t *M = h.data() + c.off[l];
         // DenseMatrix::display (sdpa_struct.cpp:684-713)

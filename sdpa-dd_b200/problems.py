@@ -33,6 +33,7 @@ __all__ = [
     "dense_random",
     "maxcut",
     "theta",
+    "with_lp",
     "control_like",
     "batch",
     "workload",
@@ -108,6 +109,32 @@ def control_like(sizes=(100, 50), m: int = 1326, seed: int = 3) -> str:
     for k in range(m):
         for b in range(len(sizes)):
             w.dense_upper(k + 1, b + 1, Fs[b][k])
+    return w.text()
+
+
+def with_lp(n: int = 30, q: int = 24, m: int = 40, seed: int = 7) -> str:
+    """An SDP block of order n and an LP block of q entries (block structure
+    "n -q"), strictly feasible on both sides: F_k ~ N(0,1)/sqrt(n) on the
+    SDP block, LP coefficients ~ N(0,1) on about half the entries; one x0 ~
+    N(0,1) with slacks X0 = I + G G^T / n and s0 ~ 1 + U(0,1) sets F_0; c_k =
+    tr F_k + the sum of its LP coefficients, so Y = I, y_lp = 1 is dual
+    feasible."""
+    rng = np.random.default_rng(seed)
+    x0 = rng.standard_normal(m)
+    A = rng.standard_normal((m, n, n)) / np.sqrt(n)
+    A = 0.5 * (A + A.transpose(0, 2, 1))
+    G = rng.standard_normal((n, n))
+    F0 = np.tensordot(x0, A, axes=1) - (np.eye(n) + G @ G.T / n)
+    a = rng.standard_normal((m, q)) * (rng.random((m, q)) < 0.5)
+    f0 = x0 @ a - (1.0 + rng.random(q))
+    c = np.trace(A, axis1=1, axis2=2) + a.sum(axis=1)
+    w = _Writer(m, [n, -q], c, f"SDP block {n} + LP block {q}, m={m} seed={seed}")
+    w.dense_upper(0, 1, F0)
+    w.entries(0, 2, range(q), range(q), f0)
+    for k in range(m):
+        w.dense_upper(k + 1, 1, A[k])
+        nz = np.nonzero(a[k])[0]
+        w.entries(k + 1, 2, nz, nz, a[k, nz])
     return w.text()
 
 
