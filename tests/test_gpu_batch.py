@@ -6,8 +6,10 @@ test requires identical phases, iteration counts and dd bits of the
 objectives, of X, y, Z and of the gradient of the optimal value with
 respect to c (sddd_adjoint), problem by problem.  The workload is the
 batched construction at small sizes (dense random SDPs of uneven order and
-constraint count), plus one problem the device path rejects (an LP block),
-which must fail alone.
+constraint count) and one problem with an LP block, plus one problem whose
+gradient cannot be formed (a constraint with a zero matrix: the Schur
+matrix is singular, the solve stops at its first factorisation and the
+adjoint refuses), which must fail alone.
 """
 import ctypes
 import importlib
@@ -35,6 +37,10 @@ def _same(a, b):
 LP_PROBLEM = '"one LP block"\n1 = mDIM\n1 = nBLOCK\n-2 = bLOCKsTRUCT\n{1}\n0 1 1 1 1.0\n1 1 1 1 1.0\n1 1 2 2 1.0\n'
 
 
+# min x1 + x2 s.t. x1 I - I >= 0 with F_2 = 0: B has a zero row and column
+ZERO_CONSTRAINT = '"a zero constraint"\n2 = mDIM\n1 = nBLOCK\n2 = bLOCKsTRUCT\n{1, 1}\n0 1 1 1 1.0\n0 1 2 2 1.0\n1 1 1 1 1.0\n1 1 2 2 1.0\n'
+
+
 def test_batch_matches_single_solves(tmp_path):
     sddd = load_pkg()
     P = _problems()
@@ -47,17 +53,23 @@ def test_batch_matches_single_solves(tmp_path):
         cases.append((path, n, m))
     lp = tmp_path / "lp.dat-s"
     lp.write_text(LP_PROBLEM)
+    cases.append((lp, None, 1))  # block space: two order-1 blocks
+    zero = tmp_path / "zero.dat-s"
+    zero.write_text(ZERO_CONSTRAINT)
     par = sddd.param(P.write_param(str(tmp_path / "p.sdpa"), eps=1e-25, max_iter=100))
     with sddd.Batch(0, workers=5) as bt:
         for path, n, m in cases[:6]:
             bt.add_file(path, m, n * n)
-        bad = bt.add_file(lp, 1, 0)
+        bad = bt.add_file(zero, 2, 4)
         for path, n, m in cases[6:]:
-            bt.add_file(path, m, n * n)
+            bt.add_file(path, m, 2 if n is None else n * n)
         res = (sddd.SdddResult * len(bt.dims))()
         rc = bt.L.sddd_batch_solve(bt.h, ctypes.byref(par), 1, ctypes.cast(res, ctypes.c_void_p))
-        assert rc == -7 and b"LP blocks" in bt.L.sddd_batch_last_error(bt.h)  # SDDD_ERR_UNSUPPORTED
-        assert bt.status(bad) == -7
+        assert rc == 0
+        # the solve ended at its first Schur factorisation (stop reason 2);
+        # the gradient was refused (a positive status: the factor's failing
+        # column), for this problem alone
+        assert bt.status(bad) > 0 and res[bad].stop_reason == 2
         idx = [q for q in range(len(bt.dims)) if q != bad]
         for q, (path, n, m) in zip(idx, cases):
             assert bt.status(q) == 0, q
