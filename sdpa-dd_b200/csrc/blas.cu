@@ -290,15 +290,23 @@ __global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, lon
 // The next diagonal block's update by the panel just solved, ahead of the
 // trailing update (the split form's lookahead): D(i, j) -= P(j, k) P(i, k)
 // for k ascending, i >= j; CTA j takes column j, thread i row i.  D is the
-// nb x nb block at c0, P its rows of the nbp panel columns before c0.
+// nb x nb block at c0, P its rows of the nbp panel columns before c0, staged
+// in shared memory first (column by column, coalesced) so that the chain of
+// each entry reads no global memory.
 __global__ void potrf_diag_pre_kernel(dd_t *A, long lda, int c0, int nb, int nbp, const int *info) {
+    extern __shared__ double2 pre_sp[]; // pre_sp[k * blockDim.x + r] = P(r, k)
     if (*info != 0) return;
-    const int j = blockIdx.x, i = threadIdx.x;
-    if (i < j || i >= nb) return;
+    const int j = blockIdx.x, i = threadIdx.x, w = blockDim.x;
     const dd_t *P = A + c0 + lda * (long)(c0 - nbp);
+    for (int k = 0; k < nbp; ++k) pre_sp[k * w + i] = i < nb ? *reinterpret_cast<const double2 *>(P + i + lda * (long)k) : make_double2(0.0, 0.0);
+    __syncthreads();
+    if (i < j || i >= nb) return;
     dd_t *d = A + (c0 + i) + lda * (long)(c0 + j);
     dd_t x = ld_dd(d);
-    for (int k = 0; k < nbp; ++k) x = dd_sub(x, dd_mul(ld_dd(P + j + lda * (long)k), ld_dd(P + i + lda * (long)k)));
+    for (int k = 0; k < nbp; ++k) {
+        const double2 pj = pre_sp[k * w + j], pi = pre_sp[k * w + i];
+        x = dd_sub(x, dd_mul(dd_make(pj.x, pj.y), dd_make(pi.x, pi.y)));
+    }
     st_dd(d, x);
 }
 
@@ -317,6 +325,7 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
     if (!attr[dev & 63]) {
         CK(cudaFuncSetAttribute(potrf_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag));
         CK(cudaFuncSetAttribute(potrf_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_panel));
+        CK(cudaFuncSetAttribute(potrf_diag_pre_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(double2) * nbmax * nbmax)));
         attr[dev & 63] = true;
     }
     if (tc && tc->side && n > 2 * nbmax) {
@@ -343,7 +352,7 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
             const int c1 = c0 + nb, nb1 = std::min(nbmax, n - c1);
             {
                 PROF_SCOPE("potrf_diag_pre", st);
-                potrf_diag_pre_kernel<<<nb1, nbmax, 0, st>>>(A, lda, c1, nb1, nb, info_dev);
+                potrf_diag_pre_kernel<<<nb1, nbmax, sizeof(double2) * nbmax * nb, st>>>(A, lda, c1, nb1, nb, info_dev);
                 CK_LAUNCH();
             }
             CK(cudaEventRecord(tc->ev_pre, st));
