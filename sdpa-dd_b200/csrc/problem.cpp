@@ -8,6 +8,7 @@
 #include <cstring>
 #include <fstream>
 #include <sstream>
+#include <thread>
 
 #include "common.cuh"
 
@@ -81,14 +82,15 @@ int dd_read(const char *s, dd_t *out) {
 }
 
 // QD's operator=(const char*) turns an unreadable string into NaN.
-static dd_t dd_parse(const std::string &tok) {
+static dd_t dd_parse(const char *tok) {
     dd_t v;
-    if (dd_read(tok.c_str(), &v) != 0) {
+    if (dd_read(tok, &v) != 0) {
         double nan = std::nan("");
         return dd_make(nan, nan);
     }
     return v;
 }
+static dd_t dd_parse(const std::string &tok) { return dd_parse(tok.c_str()); }
 
 // --------------------------------------------------------------- tokenizer
 // The fscanf patterns of sdpa_io.cpp over an in-memory copy of the file.
@@ -116,20 +118,33 @@ struct Scanner {
         size_t q = p;
         if (q < t.size() && (t[q] == '+' || t[q] == '-')) ++q;
         size_t d = q;
-        while (q < t.size() && std::isdigit((unsigned char)t[q])) ++q;
+        long acc = 0; // the digits atoi reads
+        while (q < t.size() && t[q] >= '0' && t[q] <= '9') {
+            if (acc < (1L << 40)) acc = acc * 10 + (t[q] - '0');
+            ++q;
+        }
         if (q == d) return false;
-        v = std::atoi(t.substr(p, q - p).c_str());
+        if (acc > 2147483647L) acc = 2147483647L; // out of any index range, as strtol saturates
+        v = (int)(t[p] == '-' ? -acc : acc);
         p = q;
         return true;
     }
     bool skip_int(int &v) { return skip_nonnum() && int_(v); }
     // "%*[^0-9+-]%[^,} \t\n]"
     bool skip_token(std::string &tok) {
+        size_t b, e;
+        if (!skip_token_span(b, e)) return false;
+        tok = t.substr(b, e - b);
+        return true;
+    }
+    // the same, giving the token's place in the text
+    bool skip_token_span(size_t &b, size_t &e) {
         if (!skip_nonnum()) return false;
         size_t q = p;
         while (q < t.size() && !tokdelim(t[q])) ++q;
         if (q == p) return false;
-        tok = t.substr(p, q - p);
+        b = p;
+        e = q;
         p = q;
         return true;
     }
@@ -211,8 +226,9 @@ Problem read_problem_text(const std::string &text, bool sparse) {
         break;
     }
     if (!have_m || P.m <= 0) throw Error(ERR_IO, "cannot read mDIM");
-    std::string rest = text.substr(pos);
+    const std::string &rest = text; // scanned from pos on, without a copy
     Scanner sc(rest);
+    sc.p = pos;
     int nb = 0;
     if (!sc.int_(nb) || nb <= 0) throw Error(ERR_IO, "cannot read nBLOCK");
     std::vector<int> bs(nb);
@@ -227,19 +243,58 @@ Problem read_problem_text(const std::string &text, bool sparse) {
         P.b[k] = dd_parse(tok);
     }
     if (sparse) {
-        // IO::setElement, sdpa_io.cpp:653-700
-        while (true) {
+        // IO::setElement, sdpa_io.cpp:653-700: the reference stops at the
+        // first entry whose indices or value do not read (sscanf "%lf").
+        // Here the entries are located first, their values converted on all
+        // host cores (each conversion is the same QD read, independent of
+        // the others), then taken in file order with the reference's stop
+        // and range checks: the problem is the one the serial loop builds.
+        struct Ent {
             int k, l, i, j;
-            std::string tok;
-            if (!sc.skip_int(k)) break;
-            if (!sc.skip_int(l)) break;
-            if (!sc.skip_int(i)) break;
-            if (!sc.skip_int(j)) break;
-            if (!sc.skip_token(tok)) break;
-            double probe;
-            if (std::sscanf(tok.c_str(), "%lf", &probe) <= 0) break;
-            if (k < 0 || k > P.m) throw Error(ERR_IO, "constraint index out of range in input data");
-            add_entry(P, k, l - 1, i - 1, j - 1, dd_parse(tok));
+            size_t b, e;
+        };
+        std::vector<Ent> ents;
+        ents.reserve((text.size() - pos) / 24 + 16); // a short entry line is ~ 24 bytes
+        while (true) {
+            Ent en;
+            if (!sc.skip_int(en.k) || !sc.skip_int(en.l) || !sc.skip_int(en.i) || !sc.skip_int(en.j) || !sc.skip_token_span(en.b, en.e)) break;
+            ents.push_back(en);
+        }
+        std::vector<dd_t> vals(ents.size());
+        std::vector<char> readable(ents.size());
+        auto convert = [&](size_t lo, size_t hi) {
+            char buf[64];
+            std::string big;
+            for (size_t q = lo; q < hi; ++q) {
+                const size_t len = ents[q].e - ents[q].b;
+                const char *tok;
+                if (len < sizeof buf) {
+                    std::memcpy(buf, rest.data() + ents[q].b, len);
+                    buf[len] = 0;
+                    tok = buf;
+                } else {
+                    big.assign(rest, ents[q].b, len);
+                    tok = big.c_str();
+                }
+                double probe;
+                readable[q] = std::sscanf(tok, "%lf", &probe) > 0;
+                if (readable[q]) vals[q] = dd_parse(tok);
+            }
+        };
+        const size_t ne = ents.size();
+        const unsigned nth = ne < 200000 ? 1u : std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        if (nth == 1) {
+            convert(0, ne);
+        } else {
+            std::vector<std::thread> pool;
+            for (unsigned t = 0; t < nth; ++t) pool.emplace_back(convert, ne * t / nth, ne * (t + 1) / nth);
+            for (auto &th : pool) th.join();
+        }
+        for (size_t q = 0; q < ne; ++q) {
+            if (!readable[q]) break;
+            const Ent &en = ents[q];
+            if (en.k < 0 || en.k > P.m) throw Error(ERR_IO, "constraint index out of range in input data");
+            add_entry(P, en.k, en.l - 1, en.i - 1, en.j - 1, vals[q]);
         }
     } else {
         // dense: every entry of every block, k = 0..m (sdpa_io.cpp:701-786)
@@ -267,12 +322,27 @@ Problem read_problem_text(const std::string &text, bool sparse) {
     return P;
 }
 
+// The whole file in one string, read in one go.
+static bool slurp(const std::string &path, std::string &out) {
+    std::FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) return false;
+    out.clear();
+    char buf[1 << 16];
+    size_t n;
+    if (std::fseek(f, 0, SEEK_END) == 0) {
+        const long len = std::ftell(f);
+        if (len > 0) out.reserve((size_t)len);
+        std::rewind(f);
+    }
+    while ((n = std::fread(buf, 1, sizeof buf, f)) > 0) out.append(buf, n);
+    std::fclose(f);
+    return true;
+}
+
 Problem read_problem(const std::string &path, bool sparse) {
-    std::ifstream f(path, std::ios::binary);
-    if (!f) throw Error(ERR_IO, "Cannot open data file " + path);
-    std::stringstream ss;
-    ss << f.rdbuf();
-    return read_problem_text(ss.str(), sparse);
+    std::string text;
+    if (!slurp(path, text)) throw Error(ERR_IO, "Cannot open data file " + path);
+    return read_problem_text(text, sparse);
 }
 
 void read_init_point_text(const std::string &text, bool sparse, const Problem &P, double lambda, std::vector<dd_t> &X, std::vector<dd_t> &y,
@@ -336,11 +406,9 @@ void read_init_point_text(const std::string &text, bool sparse, const Problem &P
 
 void read_init_point(const std::string &path, bool sparse, const Problem &P, double lambda, std::vector<dd_t> &X, std::vector<dd_t> &y,
                      std::vector<dd_t> &Z) {
-    std::ifstream f(path, std::ios::binary);
-    if (!f) throw Error(ERR_IO, "Cannot open init file " + path);
-    std::stringstream ss;
-    ss << f.rdbuf();
-    read_init_point_text(ss.str(), sparse, P, lambda, X, y, Z);
+    std::string text;
+    if (!slurp(path, text)) throw Error(ERR_IO, "Cannot open init file " + path);
+    read_init_point_text(text, sparse, P, lambda, X, y, Z);
 }
 
 // ------------------------------------------------------ exact dd printing
