@@ -6,8 +6,6 @@
 #include <cctype>
 #include <cstdlib>
 #include <cstring>
-#include <fstream>
-#include <sstream>
 #include <thread>
 
 #include "common.cuh"
