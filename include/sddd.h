@@ -88,6 +88,10 @@ int sddd_upload_problem(sddd_ctx *ctx, int m, int nblock, const int *block_struc
  * there.  The result file and initial-point files keep the reference's LP
  * layout. */
 int sddd_dims(const sddd_ctx *ctx, int *m, int *nsdp, long *ndim, int *sizes, int cap);
+/* The same dimensions for a problem file, read on the host only (no device,
+ * no context): for sizing buffers or planning a batch before any GPU work.
+ * space_len is the length in dd of a block space of that problem. */
+int sddd_problem_info(const char *path, int sparse, int *m, int *nsdp, long *space_len, int *sizes, int cap);
 /* Length in dd of a block space. */
 long sddd_space_len(const sddd_ctx *ctx);
 /* Formula table useFormula[k * nsdp + l] (0 F1, 1 F2, 2 F3, -1 absent). */

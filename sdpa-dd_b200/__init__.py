@@ -106,6 +106,7 @@ def lib() -> ctypes.CDLL:
         "sddd_set_initial_point": (ci, [vp, vp, vp, vp]),
         "sddd_clear_initial_point": (ci, [vp]),
         "sddd_write_point": (ci, [vp, ctypes.c_char_p, ci]),
+        "sddd_problem_info": (ci, [ctypes.c_char_p, ci, ctypes.POINTER(ci), ctypes.POINTER(ci), ctypes.POINTER(cl), vp, ci]),
         "sddd_dd_to_decimal": (ci, [SdddDD, ci, ctypes.c_char_p, ci]),
         "sddd_batch_create": (ci, [ci, ci, ctypes.POINTER(vp)]),
         "sddd_batch_destroy": (ci, [vp]),
@@ -272,7 +273,11 @@ class Batch:
         self.dims.append((m, space_len))
         return rc
 
-    def add_file(self, path, m, space_len, sparse=True, kappa=1.2):
+    def add_file(self, path, m=None, space_len=None, sparse=True, kappa=1.2):
+        """Adds a problem file; m and the block-space length default to
+        the file's own (problem_info, read on the host)."""
+        if m is None or space_len is None:
+            m, _, space_len = problem_info(path, sparse)
         return self._added(self.L.sddd_batch_add_file(self.h, str(path).encode(), int(sparse), kappa), m, space_len)
 
     def add(self, m, block_struct, b, k, blk, i, j, val, kappa=1.2):
@@ -308,6 +313,19 @@ class Batch:
         if rc != 0:
             raise SdddError(f"sddd_batch_grad_c failed ({rc})")
         return out
+
+
+def problem_info(path, sparse=True):
+    """(m, SDP block sizes, block-space length) of a problem file, read on
+    the host only (sddd_problem_info: no device needed).  LP entries count
+    as trailing blocks of order 1."""
+    L = lib()
+    m, ns, ln = ctypes.c_int(), ctypes.c_int(), ctypes.c_long()
+    sizes = np.zeros(65536, np.int32)
+    rc = L.sddd_problem_info(str(path).encode(), int(sparse), ctypes.byref(m), ctypes.byref(ns), ctypes.byref(ln), _ptr(sizes), len(sizes))
+    if rc != 0:
+        raise SdddError(f"sddd_problem_info failed ({rc}): {L.sddd_last_error(None).decode()}")
+    return m.value, sizes[: min(ns.value, len(sizes))].tolist(), ln.value
 
 
 def param(path=None, type_=0) -> SdddParam:

@@ -186,6 +186,21 @@ int sddd_dims(const sddd_ctx *cctx, int *m, int *nsdp, long *ndim, int *sizes, i
 
 long sddd_space_len(const sddd_ctx *ctx) { return (ctx && ctx->c && ctx->c->have_problem) ? ctx->c->space_len : -1; }
 
+int sddd_problem_info(const char *path, int sparse, int *m, int *nsdp, long *space_len, int *sizes, int cap) {
+    if (!path) return SDDD_ERR_ARG;
+    return guarded(nullptr, [&] {
+        const sddd::Problem p = sddd::read_problem(path, sparse != 0);
+        if (m) *m = p.m;
+        if (nsdp) *nsdp = p.nSDP;
+        long len = 0;
+        for (int n : p.sdpSize) len += (long)n * n;
+        if (space_len) *space_len = len;
+        if (sizes)
+            for (int l = 0; l < p.nSDP && l < cap; ++l) sizes[l] = p.sdpSize[l];
+        return SDDD_OK;
+    });
+}
+
 int sddd_formula(const sddd_ctx *cctx, int *out) {
     sddd_ctx *ctx = const_cast<sddd_ctx *>(cctx);
     if (!out) return SDDD_ERR_ARG;
