@@ -6,6 +6,7 @@
 #include <cctype>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <thread>
 
 #include "common.cuh"
@@ -260,23 +261,28 @@ Problem read_problem_text(const std::string &text, bool sparse) {
         }
         std::vector<dd_t> vals(ents.size());
         std::vector<char> readable(ents.size());
-        auto convert = [&](size_t lo, size_t hi) {
-            char buf[64];
-            std::string big;
-            for (size_t q = lo; q < hi; ++q) {
-                const size_t len = ents[q].e - ents[q].b;
-                const char *tok;
-                if (len < sizeof buf) {
-                    std::memcpy(buf, rest.data() + ents[q].b, len);
-                    buf[len] = 0;
-                    tok = buf;
-                } else {
-                    big.assign(rest, ents[q].b, len);
-                    tok = big.c_str();
+        std::atomic<bool> failed{false};
+        auto convert = [&](size_t lo, size_t hi) noexcept {
+            try {
+                char buf[64];
+                std::string big;
+                for (size_t q = lo; q < hi; ++q) {
+                    const size_t len = ents[q].e - ents[q].b;
+                    const char *tok;
+                    if (len < sizeof buf) {
+                        std::memcpy(buf, rest.data() + ents[q].b, len);
+                        buf[len] = 0;
+                        tok = buf;
+                    } else {
+                        big.assign(rest, ents[q].b, len);
+                        tok = big.c_str();
+                    }
+                    double probe;
+                    readable[q] = std::sscanf(tok, "%lf", &probe) > 0;
+                    if (readable[q]) vals[q] = dd_parse(tok);
                 }
-                double probe;
-                readable[q] = std::sscanf(tok, "%lf", &probe) > 0;
-                if (readable[q]) vals[q] = dd_parse(tok);
+            } catch (...) { // a token too large to copy: report it in the caller's thread
+                failed = true;
             }
         };
         const size_t ne = ents.size();
@@ -288,6 +294,7 @@ Problem read_problem_text(const std::string &text, bool sparse) {
             for (unsigned t = 0; t < nth; ++t) pool.emplace_back(convert, ne * t / nth, ne * (t + 1) / nth);
             for (auto &th : pool) th.join();
         }
+        if (failed) throw Error(ERR_IO, "input data: out of memory while reading the values");
         for (size_t q = 0; q < ne; ++q) {
             if (!readable[q]) break;
             const Ent &en = ents[q];
