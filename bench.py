@@ -16,12 +16,18 @@ The headline runs the tensor-core split form (--tc, default 16 slices: the
 Cholesky trailing updates as INT8 slice products on tcgen05); the same
 passes in the plain dd form (the reference's operation order, bit for bit)
 are timed beside it ("plain_dd"), and both forms solve the problem from the
-standard initial point to relative gap 1e-25 ("solve_to_gap", wall clock).
+standard initial point to relative gap 1e-25 ("solve_to_gap", wall clock),
+as do the max-cut (n = m = 500) and control-shaped (blocks 100 + 50, m =
+1326) workloads ("solve_to_gap_other_configs"), each beside the reference
+build's own solve of the same file.  The headline passes run with no
+per-kernel instrumentation; the kernel breakdown and the roofline come from
+a separate, profiled run of the same passes.
 
 One JSON line on rank 0.  Multi-GPU runs are replicas (the single solve
 does not shard): every rank solves its own copy, value sums the ranks' work
-over the slowest rank's time.  --impl reference times the reference build
-(oracle/_ref) on the host cores instead.
+over the slowest rank's time.  --impl reference times the reference build's
+stock main loop (oracle/_ref) on all host cores on the same m = 9980
+workload: one pass after one untimed pass (about a minute each).
 """
 from __future__ import annotations
 
@@ -40,7 +46,10 @@ import time
 
 ROOT = pathlib.Path(__file__).resolve().parent
 WORKLOAD = dict(name="theta", nv=200, p=0.5, seed=2)
-CPU_SAMPLE = dict(name="theta", nv=120, p=0.5, seed=2)  # m = 3571
+SMALL_THETA = dict(name="theta", nv=120, p=0.5, seed=2)  # m = 3571
+# the other full-size shapes, solved to gap 1e-25 beside the headline
+MAXCUT = dict(name="maxcut", n=500, p=0.02, seed=1)  # n = m = 500, F3 Schur
+CONTROL = dict(name="control", sizes=(100, 50), m=1326, seed=3)  # F1 Schur
 EPS = 1e-25
 
 
@@ -61,13 +70,28 @@ def problems():
     return importlib.import_module("sdpa_dd_b200.problems")
 
 
+def workload_label(w):
+    if w["name"] == "theta":
+        return f"theta-shaped SDP nv={w['nv']} p={w['p']} seed={w['seed']}"
+    if w["name"] == "maxcut":
+        return f"max-cut-shaped SDP n={w['n']} p={w['p']} seed={w['seed']}"
+    return f"control-shaped SDP blocks {w['sizes']} m={w['m']} seed={w['seed']}"
+
+
 def write_workload(w, directory):
     P = problems()
-    path = pathlib.Path(directory) / f"{w['name']}_nv{w['nv']}_s{w['seed']}.dat-s"
+    key = "_".join(f"{k}{v}" for k, v in sorted(w.items()) if k != "name").replace(" ", "").replace(",", "-")
+    path = pathlib.Path(directory) / f"{w['name']}_{key}.dat-s"
     if not path.exists():
+        if w["name"] == "theta":
+            text = P.theta(nv=w["nv"], p=w["p"], seed=w["seed"])
+        elif w["name"] == "maxcut":
+            text = P.maxcut(n=w["n"], p=w["p"], seed=w["seed"])
+        else:
+            text = P.control_like(sizes=w["sizes"], m=w["m"], seed=w["seed"])
         tmp = str(path) + f".tmp{os.getpid()}"
         with open(tmp, "w") as f:
-            f.write(P.theta(nv=w["nv"], p=w["p"], seed=w["seed"]))
+            f.write(text)
         os.replace(tmp, path)
     param = P.write_param(str(pathlib.Path(directory) / "bench.param"), eps=EPS)
     return path, param
@@ -129,22 +153,28 @@ def trailing_flops(m, nb=64):
 
 
 def cpu_reference(sample, warmup, steps, threads):
-    """Time the reference build (oracle/_ref/sdpa_ref_iter) on the host."""
+    """Time the reference build's stock main loop (oracle/_ref/sdpa_ref_iter)
+    on the host: `warmup` untimed passes, then `steps` timed ones."""
     P = problems()
     exe = ROOT / "oracle" / "_ref" / "sdpa_ref_iter"
     if not exe.exists():
         return None, "oracle/_ref/sdpa_ref_iter is not built"
-    with tempfile.TemporaryDirectory() as td:
-        data, param = write_workload(sample, td)
-        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-        r = subprocess.run([str(exe), str(data), param, str(warmup), str(steps)], capture_output=True, text=True, env=env)
-        if r.returncode != 0:
-            return None, f"reference run failed: {r.stderr.strip()[-200:]}"
-        out = json.loads(r.stdout.strip().splitlines()[-1])
-    e = P.theta_edges(sample["nv"], sample["p"], sample["seed"])
-    schur, chol = P.theta_work(sample["nv"], e)
+    workdir = pathlib.Path(tempfile.gettempdir()) / f"sddd_bench_ref_{os.getuid()}"
+    workdir.mkdir(exist_ok=True)
+    data, param = write_workload(sample, workdir)
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    r = subprocess.run([str(exe), str(data), param, str(warmup), str(steps)], capture_output=True, text=True, env=env)
+    if r.returncode != 0:
+        return None, f"reference run failed: {r.stderr.strip()[-200:]}"
+    out = json.loads(r.stdout.strip().splitlines()[-1])
     secs = out["pass_s"]
-    return {"value": (schur + chol) * len(secs) / sum(secs) / 1e9, "m": out["m"], "threads": out["threads"], "pass_s": secs}, None
+    res = {"m": out["m"], "threads": out["threads"], "pass_s": secs, "schur_s": out.get("schur_s"), "chol_s": out.get("chol_s"),
+           "setup_s": out.get("setup_s")}
+    if sample["name"] == "theta":
+        e = P.theta_edges(sample["nv"], sample["p"], sample["seed"])
+        schur, chol = P.theta_work(sample["nv"], e)
+        res["value"] = (schur + chol) * len(secs) / sum(secs) / 1e9
+    return res, None
 
 
 BATCH = {"count": 256, "seed": 4, "cpu_sample": 8}
@@ -181,9 +211,15 @@ def batch_measure(sddd, device, rank, world, args):
         res = bt.solve(par, with_grad=True) if mine else []
         dt = allmax(world, time.perf_counter() - t)
     phases = [sddd.PHASES[r.phase] for r in res]
-    out = {"workload": f"{BATCH['count']} dense random SDPs, n ~ U[10,80], m ~ U[20,200], seed {BATCH['seed']}, gap {EPS:g}, with d(c.x)/dc",
-           "solves_per_s": len(paths) / dt, "seconds": dt, "ranks": world, "pdOPT_rank0": phases.count("pdOPT"),
-           "problems_rank0": len(mine),
+    n_opt = int(allsum(world, phases.count("pdOPT")))
+    counts = {}
+    for ph in phases:
+        counts[ph] = counts.get(ph, 0) + 1
+    out = {"workload": f"{BATCH['count']} dense random SDPs, n ~ U[10,80], m ~ U[20,200], seed {BATCH['seed']}, epsilon {EPS:g}, with d(c.x)/dc",
+           "solves_per_s": len(paths) / dt,
+           "solves_per_s_basis": "every problem run to the end of its main loop, whatever its final phase (phases below)",
+           "pdopt_solves_per_s": n_opt / dt, "pdOPT": n_opt, "seconds": dt, "ranks": world,
+           "phases_rank0": counts, "problems_rank0": len(mine),
            "mean_iterations_rank0": (sum(r.iterations for r in res) / len(res)) if res else None}
     exe = ROOT / "oracle" / "_ref" / "sdpa_dd"
     if rank == 0 and world == 1 and not args.no_cpu_baseline and exe.exists():
@@ -197,12 +233,22 @@ def batch_measure(sddd, device, rank, world, args):
             t0 = time.perf_counter()
             subprocess.run([str(exe), "-ds", str(path), "-o", str(path) + ".ref.out", "-p", param_path], capture_output=True,
                            env=dict(os.environ, OMP_NUM_THREADS="1"), check=False)
-            return time.perf_counter() - t0
+            dt_q = time.perf_counter() - t0
+            import re
+            mt = re.search(r"phase.value = (\w+)", pathlib.Path(str(path) + ".ref.out").read_text())
+            return dt_q, mt.group(1) if mt else None
 
         with cf.ThreadPoolExecutor(max_workers=min(cores, len(pick))) as ex:
-            secs = list(ex.map(run, pick))
+            runs = list(ex.map(run, pick))
+        secs = [r[0] for r in runs]
         mean_s = sum(secs) / len(secs)
+        ref_ph = [r[1] for r in runs]
+        ours_ph = {}
+        if world == 1:
+            pos = {q: i for i, q in enumerate(mine)}
+            ours_ph = {str(q): phases[pos[q]] for q in pick}
         out["cpu_reference"] = {"solves_per_s": cores / mean_s, "cores": cores, "kind": "reference",
+                                "phases": {str(q): ph for q, ph in zip(pick, ref_ph)}, "phases_ours_same_problems": ours_ph,
                                 "sample": f"oracle/_ref sdpa_dd on {len(pick)} of the problems (seeded pick), one thread each; "
                                           f"rate = cores / mean single-thread solve time ({mean_s:.2f} s), without gradients"}
     return out
@@ -226,6 +272,16 @@ def barrier(world):
         dist.barrier()
 
 
+def allsum(world, v):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def allmax(world, v):
     if world == 1:
         return v
@@ -236,28 +292,96 @@ def allmax(world, v):
     return float(t.item())
 
 
+# The reference arm's bounded sample of the headline workload: one main-loop
+# pass at m = 9980 takes about a minute on 16 host cores, so it times
+# REF_STEPS passes after REF_WARMUP untimed ones, whatever --steps/--warmup.
+REF_WARMUP, REF_STEPS = 1, 1
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    res, why = cpu_reference(CPU_SAMPLE, args.warmup, args.steps, threads)
+    res, why = cpu_reference(WORKLOAD, REF_WARMUP, REF_STEPS, threads)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": why}))
         return 0
-    sample = f"theta-shaped SDP nv={CPU_SAMPLE['nv']} p={CPU_SAMPLE['p']} (m={res['m']}), {args.steps} main-loop passes after {args.warmup}"
+    sample = (f"{workload_label(WORKLOAD)} (m={res['m']}): {REF_STEPS} timed pass(es) of the stock main loop after {REF_WARMUP} untimed, "
+              f"{res['threads']} OpenMP threads (bounded sample: ~1 min per pass)")
     line = {
         "impl": "reference",
         "metric": "Schur+Chol dd-GFLOP/s per Newton iteration",
         "value": res["value"], "unit": "dd-GFLOP/s", "higher_is_better": True,
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": world, "steps": REF_STEPS, "warmup": REF_WARMUP,
         "ms_per_step": 1e3 * sum(res["pass_s"]) / len(res["pass_s"]),
         "scaling": "weak", "vs_baseline": None, "dtype": "dd (f64 pairs)", "data": "synthetic",
-        "config": {"workload": sample, "reference": "oracle/_ref (SDPA-DD 7.1.3 built from its sources, OpenMP)"},
+        "config": {"workload": workload_label(WORKLOAD), "m": res["m"], "step": "one main-loop pass",
+                   "reference": "oracle/_ref (SDPA-DD 7.1.3 built from its sources, OpenMP)"},
+        "reference_timers_s_per_step": {"make_bMat": res["schur_s"], "cholesky_bMat": res["chol_s"]},
         "cpu_baseline": {"value": res["value"], "unit": "dd-GFLOP/s", "cores": res["threads"], "kind": "reference", "sample": sample},
         "e2e": {"value": res["value"], "unit": "dd-GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
+
+
+def _dd_dec(v):
+    from decimal import Decimal, getcontext
+    getcontext().prec = 60
+    return Decimal(v.hi) + Decimal(v.lo)
+
+
+def other_solves(sddd, args, local, world):
+    """The max-cut (n = m = 500) and control-shaped (blocks 100 + 50, m =
+    1326) workloads solved to relative gap 1e-25 in both forms, each against
+    the reference build's own solve of the same file (one OpenMP thread,
+    tests/golden/large_solves.json: phase, iterations, dd objectives) and
+    its time to gap on the host cores (iterations x one timed pass of its
+    stock main loop)."""
+    import torch
+    golden = {}
+    gfile = ROOT / "tests" / "golden" / "large_solves.json"
+    if gfile.exists():
+        golden = json.loads(gfile.read_text())
+    out = {}
+    workdir = pathlib.Path(tempfile.gettempdir()) / f"sddd_bench_{os.getuid()}_{local}"
+    workdir.mkdir(exist_ok=True)
+    for key, w, gname in (("maxcut_n500", MAXCUT, "maxcut_n500"), ("control_100_50_m1326", CONTROL, "control_100_50_m1326")):
+        data, param_path = write_workload(w, workdir)
+        par = sddd.param(param_path)
+        ent = {"workload": workload_label(w)}
+        g = golden.get(gname)
+        with sddd.Context(local) as c:
+            c.read_problem(data, sparse=True, kappa=1.2)
+            ent["m"] = c.m
+            for label, slices in (("tc_split", args.tc), ("plain", 0)):
+                if label == "tc_split" and not args.tc:
+                    continue
+                if c.L.sddd_set_tc_split(c.h, slices) != 0:
+                    raise RuntimeError(c.L.sddd_last_error(c.h).decode())
+                barrier(world)
+                torch.cuda.synchronize()
+                t1 = time.perf_counter()
+                r = c.solve(par)
+                torch.cuda.synchronize()
+                dt = allmax(world, (time.perf_counter() - t1) * 1e3) / 1e3
+                e = {"seconds": dt, "iterations": r.iterations, "phase": sddd.PHASES[r.phase], "relative_gap": r.relative_gap.hi}
+                if g:
+                    from decimal import Decimal
+                    for nm in ("objValPrimal", "objValDual"):
+                        want = Decimal(g[nm][0]) + Decimal(g[nm][1])
+                        e[f"{nm}_rel_diff_vs_reference"] = float(abs(_dd_dec(getattr(r, nm)) - want) / max(abs(want), Decimal(1)))
+                ent[label] = e
+        if g:
+            ent["reference"] = {"phase": g["phase"], "iterations": g["iterations"], "source": "tests/golden/large_solves.json (one OpenMP thread)"}
+        if local == 0 and not args.no_cpu_baseline and g:
+            res, why = cpu_reference(w, 0, 1, os.cpu_count() or 1)
+            if res is not None:
+                ent["reference"].update({"pass_s": res["pass_s"][0], "cores": res["threads"],
+                                         "time_to_gap_s": g["iterations"] * res["pass_s"][0],
+                                         "time_to_gap_basis": "reference iterations x one timed pass of its stock main loop (setup excluded)"})
+        out[key] = ent
+    return out
 
 
 KERNELS = ("potrf_trailing_update", "potrf_trailing_update_tc", "potrf_panel", "potrf_diag", "trsv", "schur_build", "min_eig")
@@ -299,16 +423,18 @@ def run_ours(args, world, rank, local):
             if rc != 0:
                 raise RuntimeError(f"solver stopped at its first iteration (rc={rc})")
 
-    def timed_passes(steps, warmup, clocks=False):
-        """device time of `steps` main-loop passes (max over ranks), the
-        per-kernel times and the kernel launches inside the region"""
+    def timed_passes(steps, warmup, clocks=False, profile=False):
+        """device time of `steps` main-loop passes (max over ranks) and the
+        kernel launches inside the region; with profile, the per-kernel
+        times (event pairs around every kernel group: a separate run, never
+        the headline's)"""
         restart()
         for _ in range(warmup):
             iterate()
         barrier(world)
         torch.cuda.synchronize()
         clk = Clocks(local) if (clocks and rank == 0) else None
-        L.sddd_profile(ctx.h, 1)
+        L.sddd_profile(ctx.h, 1 if profile else 0)
         L.sddd_profile_reset(ctx.h)
         launches0 = L.sddd_launch_count()
         ev0 = torch.cuda.Event(enable_timing=True)
@@ -322,25 +448,32 @@ def run_ours(args, world, rank, local):
         barrier(world)
         clk_res = clk.stop() if clk else None
         kern = {}
-        for name in KERNELS:
-            t = ctypes.c_double()
-            n = ctypes.c_long()
-            L.sddd_profile_read(ctx.h, name.encode(), ctypes.byref(t), ctypes.byref(n))
-            kern[name] = (t.value, n.value)
-        L.sddd_profile(ctx.h, 0)
+        if profile:
+            for name in KERNELS:
+                t = ctypes.c_double()
+                n = ctypes.c_long()
+                L.sddd_profile_read(ctx.h, name.encode(), ctypes.byref(t), ctypes.byref(n))
+                kern[name] = (t.value, n.value)
+            L.sddd_profile(ctx.h, 0)
         return allmax(world, ev0.elapsed_time(ev1)), kern, launches, clk_res
 
-    # ---- headline: the tensor-core split form, device-resident
+    # ---- headline: the tensor-core split form, device-resident, no profiling
     set_tc(args.tc)
-    ms_max, kern, launches, clk = timed_passes(args.steps, args.warmup, clocks=True)
+    ms_max, _, launches, clk = timed_passes(args.steps, args.warmup, clocks=True)
     value = world * args.steps * step_flops / (ms_max * 1e-3) / 1e9
-    # ---- end to end through the C ABI with host buffers (same form)
+    # per-kernel breakdown of the same passes, in a separate profiled run
+    prof_ms, kern, _, _ = timed_passes(args.steps, 1, profile=True)
+    # ---- end to end through the C ABI with host buffers (same form), from
+    # a fresh start so the timed passes stay inside one solve
     n_space = L.sddd_space_len(ctx.h)
     m = ctx.m
     X = torch.empty(2 * n_space, dtype=torch.float64).pin_memory()
     Z = torch.empty(2 * n_space, dtype=torch.float64).pin_memory()
     y = torch.empty(2 * m, dtype=torch.float64).pin_memory()
     px, pz, py = (ctypes.c_void_p(t.data_ptr()) for t in (X, Z, y))
+    restart()
+    for _ in range(args.warmup):
+        iterate()
     L.sddd_get_point(ctx.h, px, py, pz)
     h2d = d2h = 16 * (2 * n_space + m)
     barrier(world)
@@ -351,7 +484,8 @@ def run_ours(args, world, rank, local):
     for _ in range(args.steps):
         if L.sddd_set_point(ctx.h, px, py, pz) != 0:
             raise RuntimeError("set_point failed")
-        iterate()
+        if L.sddd_iterate(ctx.h) != 0:
+            raise RuntimeError("the solve ended inside the timed end-to-end passes")
         L.sddd_get_point(ctx.h, px, py, pz)
     e1.record(stream)
     torch.cuda.synchronize()
@@ -362,7 +496,8 @@ def run_ours(args, world, rank, local):
     plain = None
     if args.tc:
         set_tc(0)
-        p_ms, p_kern, _, _ = timed_passes(args.steps, 1)
+        p_ms, _, _, _ = timed_passes(args.steps, 1)
+        _, p_kern, _, _ = timed_passes(args.steps, 1, profile=True)
         plain = {"value": world * args.steps * step_flops / (p_ms * 1e-3) / 1e9, "ms_per_step": p_ms / args.steps,
                  "kernel_ms_per_step": {k: v[0] / args.steps for k, v in p_kern.items()}}
         set_tc(args.tc)
@@ -381,10 +516,17 @@ def run_ours(args, world, rank, local):
             torch.cuda.synchronize()
             dt = allmax(world, (time.perf_counter() - t1) * 1e3) / 1e3
             solves[label] = {"seconds": dt, "iterations": r.iterations, "phase": sddd.PHASES[r.phase],
-                             "relative_gap": r.relative_gap.hi, "objValPrimal": r.objValPrimal.hi}
+                             "relative_gap": r.relative_gap.hi, "objValPrimal": r.objValPrimal.hi, "_obj": _dd_dec(r.objValPrimal)}
         set_tc(args.tc)
         if "tc_split" in solves:
             solves["speedup_tc_over_plain"] = solves["plain"]["seconds"] / solves["tc_split"]["seconds"]
+        solves["objValPrimal_diff_tc_vs_plain"] = None
+        if "tc_split" in solves:
+            from decimal import Decimal
+            a, b = solves["tc_split"].pop("_obj"), solves["plain"].pop("_obj")
+            solves["objValPrimal_diff_tc_vs_plain"] = float(abs(a - b) / max(abs(b), Decimal(1)))
+        else:
+            solves["plain"].pop("_obj")
     # ---- roofline of the dominant kernel
     tr_fl, tr_launch = trailing_flops(m)
     fp64 = ctypes.c_double()
@@ -426,15 +568,25 @@ def run_ours(args, world, rank, local):
                     "peak_source": f"measured FP64 FMA rate {fp64.value:.0f} GFLOP/s / 20 FP64 instructions per dd multiply-add pair (2 dd-flops)",
                     "launches_per_step": t_n / args.steps, "ddflops_per_launch": tr_fl / tr_launch}
     batched = None if args.no_batch else batch_measure(sddd, local, rank, world, args)
-    cpu = None
+    others = None if args.no_solve else other_solves(sddd, args, local, world)
+    cpu = cpu_small = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        res, why = cpu_reference(CPU_SAMPLE, 0, 1, threads)
+        res, why = cpu_reference(WORKLOAD, 0, 1, threads)
         if res is not None:
             cpu = {"value": res["value"], "unit": "dd-GFLOP/s", "cores": res["threads"], "kind": "reference",
-                   "sample": f"oracle/_ref on a theta-shaped SDP nv={CPU_SAMPLE['nv']} (m={res['m']}), one main-loop pass, {res['threads']} OpenMP threads"}
+                   "sample": f"oracle/_ref stock main loop on the same workload ({workload_label(WORKLOAD)}, m={res['m']}): one pass, "
+                             f"{res['threads']} OpenMP threads",
+                   "pass_s": res["pass_s"][0], "make_bMat_s": res["schur_s"][0], "cholesky_bMat_s": res["chol_s"][0]}
+            if solves and "tc_split" in solves:
+                solves["reference_time_to_gap_s"] = solves["tc_split"]["iterations"] * res["pass_s"][0]
+                solves["reference_time_to_gap_basis"] = "iterations of this solve x one timed pass of the reference's stock main loop"
         else:
             cpu = {"value": None, "unit": "dd-GFLOP/s", "cores": 0, "kind": "reference", "sample": why}
+        res, why = cpu_reference(SMALL_THETA, 0, 1, threads)
+        if res is not None:
+            cpu_small = {"value": res["value"], "unit": "dd-GFLOP/s", "cores": res["threads"], "kind": "reference",
+                         "sample": f"{workload_label(SMALL_THETA)} (m={res['m']}), one pass (a smaller config, for comparison only)"}
     if rank == 0:
         line = {
             "metric": "Schur+Chol dd-GFLOP/s per Newton iteration",
@@ -448,11 +600,14 @@ def run_ours(args, world, rank, local):
                        "eps": EPS, "setup_s": setup_s},
             "step_ddflops": {"schur": schur.value, "cholesky": chol.value},
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()},
+            "kernel_breakdown_basis": f"a separate run of {args.steps} passes with per-kernel event pairs ({prof_ms / args.steps:.1f} ms per pass there)",
             "plain_dd": plain,
             "solve_to_gap": solves,
+            "solve_to_gap_other_configs": others,
             "batched": batched,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "cpu_baseline_m3571": cpu_small,
             "e2e": {"value": e2e_value, "unit": "dd-GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
             "clocks": clk,

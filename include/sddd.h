@@ -158,7 +158,7 @@ int sddd_clear_initial_point(sddd_ctx *ctx);
  * own reader (sdpa_io.cpp:152-283) take, every number with 34 significant
  * digits, so a later solve can start from it (warm start, checkpoint).  The
  * reference writes only the high doubles of its result (sdpa_io.cpp:1205-
- * 1234, SURVEY's full-precision result I/O); read back, this file gives the
+ * 1234); read back, this file gives the
  * dd point to a few units in its last place.  sparse != 0: "target block i
  * j value" lines (diagonal always, other zeros left out); else dense. */
 int sddd_write_point(sddd_ctx *ctx, const char *path, int sparse);

@@ -88,6 +88,9 @@ struct RefSolver {
     dd_real muAtStep, thetaPAtStep, thetaDAtStep;
     dd_real objPAtStep, objDAtStep;
     int phaseAtStep = 0;
+    // false: ref_step runs the stock loop body only (no copies of B, g and
+    // the predictor direction, no extra eigenvalue calls), for timing
+    bool capture = true;
 };
 
 } // namespace
@@ -334,15 +337,17 @@ int ref_step(void *h) {
     Newton &nt = *s->newton;
     // Newton::Mehrotra(PREDICTOR) split open (sdpa_newton.cpp:1345-1384)
     nt.Make_gVec(Newton::PREDICTOR, s->inputData, s->currentPt, s->currentRes, s->mu, s->beta, s->phase, s->work, s->com);
-    s->gPred.copyFrom(nt.gVec);
+    if (s->capture) s->gPred.copyFrom(nt.gVec);
     nt.Make_bMat(s->inputData, s->currentPt, s->work, s->com);
-    s->bCaptured.copyFrom(nt.bMat);
+    if (s->capture) s->bCaptured.copyFrom(nt.bMat);
     if (!nt.compute_DyVec(Newton::PREDICTOR, s->inputData, s->currentPt, s->work, s->com)) return 2;
     nt.compute_DzMat(s->inputData, s->currentRes, s->phase, s->com);
     nt.compute_DxMat(s->currentPt, s->work, s->com);
-    s->dxPred.copyFrom(nt.DxMat);
-    s->dyPred.copyFrom(nt.DyVec);
-    s->dzPred.copyFrom(nt.DzMat);
+    if (s->capture) {
+        s->dxPred.copyFrom(nt.DxMat);
+        s->dyPred.copyFrom(nt.DyVec);
+        s->dzPred.copyFrom(nt.DzMat);
+    }
     s->alpha.MehrotraPredictor(s->inputData, s->currentPt, s->phase, nt, s->work, s->com);
     s->alphaPredP = s->alpha.primal;
     s->alphaPredD = s->alpha.dual;
@@ -350,8 +355,10 @@ int ref_step(void *h) {
     s->betaCorr = s->beta.value;
     if ((s->phase.value == SolveInfo::pdFEAS) && ((s->beta.value > 5) || (s->solveInfo.objValPrimal < s->solveInfo.objValDual))) return 3;
     nt.Mehrotra(Newton::CORRECTOR, s->inputData, s->currentPt, s->currentRes, s->mu, s->beta, s->reduction, s->phase, s->work, s->com);
-    s->minEigX = Jal::getMinEigen(s->currentPt.invCholeskyX, nt.DxMat, s->work);
-    s->minEigZ = Jal::getMinEigen(s->currentPt.invCholeskyZ, nt.DzMat, s->work);
+    if (s->capture) {
+        s->minEigX = Jal::getMinEigen(s->currentPt.invCholeskyX, nt.DxMat, s->work);
+        s->minEigZ = Jal::getMinEigen(s->currentPt.invCholeskyZ, nt.DzMat, s->work);
+    }
     s->alpha.MehrotraCorrector(s->inputData, s->currentPt, s->phase, s->reduction, nt, s->mu, s->theta, s->work, s->param, s->com);
     s->muAtStep = s->mu.current;
     s->thetaPAtStep = s->theta.primal;
@@ -479,6 +486,19 @@ int ref_scalar(void *h, int what, double *out) {
     }
     st(out, v);
     return 0;
+}
+
+// on != 0 (the default): ref_step keeps copies of the last pass's
+// intermediates; 0: it runs the stock loop body only.
+void ref_set_capture(void *h, int on) { ((RefSolver *)h)->capture = on != 0; }
+
+// The reference's own accumulated timers (ComputeTime, sdpa_parts.h):
+// out[0] "Make bMat" seconds (sdpa_newton.cpp:1243), out[1] "Cholesky bMat"
+// seconds (sdpa_newton.cpp:1299).
+void ref_times(void *h, double *out) {
+    RefSolver *s = (RefSolver *)h;
+    out[0] = s->com.makebMat;
+    out[1] = s->com.choleskybMat;
 }
 
 // Phase (SolveInfo::phaseType as int) and iteration counter.

@@ -4,10 +4,11 @@
 //   sdpa_ref_iter DATA.dat-s PARAM.sdpa WARMUP STEPS [KAPPA]
 //
 // Sets the problem up exactly as pinpal (sdpa_main.cpp:43-292), runs WARMUP
-// untimed passes of its main loop, then STEPS timed passes, and prints one
-// JSON object: per-pass wall seconds and the reference's own ComputeTime
-// deltas for the Schur build ("Make bMat", sdpa_newton.cpp:1223-1244) and
-// the Cholesky of B ("Cholesky bMat", sdpa_newton.cpp:1246-1278).
+// untimed passes of its main loop, then STEPS timed passes of the stock loop
+// body (sdpa_main.cpp:294-376, no captured copies), and prints one JSON
+// object: per-pass wall seconds and the reference's own ComputeTime deltas
+// per pass for the Schur build ("Make bMat", sdpa_newton.cpp:1223-1244) and
+// the Cholesky of B ("Cholesky bMat", sdpa_newton.cpp:1246-1299).
 #include <sdpa_io.h>
 #include <chrono>
 #include <cstdio>
@@ -19,6 +20,8 @@ extern "C" {
 void *ref_open(const char *dataFile, const char *paramFile, double kappa);
 int ref_step(void *h);
 int ref_dims(void *h, int *out, int cap);
+void ref_set_capture(void *h, int on);
+void ref_times(void *h, double *out);
 }
 
 int main(int argc, char **argv) {
@@ -35,6 +38,7 @@ int main(int argc, char **argv) {
         return 1;
     }
     double tsetup = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    ref_set_capture(h, 0);
     int dims[64];
     ref_dims(h, dims, 64);
     for (int i = 0; i < warm; ++i)
@@ -42,12 +46,10 @@ int main(int argc, char **argv) {
             std::fprintf(stderr, "solver stopped during warm-up\n");
             return 1;
         }
-    std::vector<double> wall;
-    // ComputeTime lives in the opaque solver; read it back through the
-    // struct layout is not possible from here, so time the passes and
-    // re-time the two phases with the reference's own static timers is not
-    // exposed either: report wall per pass only.
+    std::vector<double> wall, schur, chol;
     for (int i = 0; i < steps; ++i) {
+        double t0[2], t1[2];
+        ref_times(h, t0);
         auto a = std::chrono::steady_clock::now();
         int rc = ref_step(h);
         double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count();
@@ -55,10 +57,20 @@ int main(int argc, char **argv) {
             std::fprintf(stderr, "solver stopped at timed pass %d (rc=%d)\n", i, rc);
             return 1;
         }
+        ref_times(h, t1);
         wall.push_back(dt);
+        schur.push_back(t1[0] - t0[0]);
+        chol.push_back(t1[1] - t0[1]);
     }
-    std::printf("{\"m\": %d, \"nblock\": %d, \"threads\": %d, \"setup_s\": %.6f, \"pass_s\": [", dims[0], dims[1], omp_get_max_threads(), tsetup);
-    for (size_t i = 0; i < wall.size(); ++i) std::printf("%s%.6f", i ? ", " : "", wall[i]);
-    std::printf("]}\n");
+    auto list = [](const char *key, const std::vector<double> &v) {
+        std::printf(", \"%s\": [", key);
+        for (size_t i = 0; i < v.size(); ++i) std::printf("%s%.6f", i ? ", " : "", v[i]);
+        std::printf("]");
+    };
+    std::printf("{\"m\": %d, \"nblock\": %d, \"threads\": %d, \"setup_s\": %.6f", dims[0], dims[1], omp_get_max_threads(), tsetup);
+    list("pass_s", wall);
+    list("schur_s", schur);
+    list("chol_s", chol);
+    std::printf("}\n");
     return 0;
 }

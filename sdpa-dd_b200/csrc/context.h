@@ -161,7 +161,7 @@ struct Context {
     // Schur work: F_i and G_i of FG owners (largest block)
     DBuf<dd_t> Fbuf, Gbuf;
     // small scratch
-    DBuf<dd_t> scal;   // device scalars
+    DBuf<dd_t> scal;   // device scalars: max(64, nSDP + 8) result slots
     DBuf<dd_t> red;    // reduction scratch
     DBuf<int> info;
     DBuf<dd_t> rdiag;
@@ -177,7 +177,6 @@ struct Context {
     DBuf<int8_t> tc_slice_buf;
     DBuf<int> tc_exps, tc_err;
     OzakiWork tc;
-    std::vector<dd_t> h_scal;
     // a user-given initial point (the reference's -id / -is), used by the
     // solver's start in place of lambda I
     bool has_init = false;

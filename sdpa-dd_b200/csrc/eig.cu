@@ -360,10 +360,13 @@ dd_t min_eig(Context &c, const Space &L, const Space &D) {
         }
         DBuf<int> &ids = c.eig_ids_small;
         ids.upload(small, st);
-        small_min_eig_kernel<<<(unsigned)small.size(), 32, 0, st>>>(ids.p, c.d_sizes.p, c.d_off.p, c.W1.buf.p, c.scal.p + 32);
+        // results after the big blocks' slots: big.size() + small.size()
+        // = nSDP slots, which c.scal always holds
+        dd_t *res = c.scal.p + big.size();
+        small_min_eig_kernel<<<(unsigned)small.size(), 32, 0, st>>>(ids.p, c.d_sizes.p, c.d_off.p, c.W1.buf.p, res);
         CK_LAUNCH();
         std::vector<dd_t> h(small.size());
-        d2h(c, h.data(), c.scal.p + 32, sizeof(dd_t) * small.size());
+        d2h(c, h.data(), res, sizeof(dd_t) * small.size());
         vals.insert(vals.end(), h.begin(), h.end());
     }
     // blocks in order: re-sort the values by block index

@@ -6,9 +6,11 @@
 // process with a fixed memory budget) cannot let a library call cudaMalloc,
 // which fails once the pool holds the memory, or cudaFree, which
 // synchronises the whole device and stalls that caller's other streams.
-// sddd_min_eig allocates its block list and Lanczos vectors on every call;
-// this entry point runs the same kernels on a scratch array that is part of
-// the library image instead.
+// sddd_min_eig keeps its block list and Lanczos vectors in context buffers
+// that grow on demand, so it allocates on a context's first call and on any
+// call with a larger block, and it needs a context (whose creation
+// allocates) at all; this entry point runs the same kernels on a scratch
+// array that is part of the library image instead.
 //
 // Scratch: one file-scope __device__ array of NOALLOC_SCRATCH_DD dd values
 // (about 320 KiB), which every GPU that loads the library holds until the

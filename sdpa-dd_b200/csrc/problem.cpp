@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <atomic>
+#include <system_error>
 #include <thread>
 
 #include "common.cuh"
@@ -290,8 +291,15 @@ Problem read_problem_text(const std::string &text, bool sparse) {
         if (nth == 1) {
             convert(0, ne);
         } else {
+            // a thread that cannot be created leaves its share (and every
+            // later one) to the calling thread
             std::vector<std::thread> pool;
-            for (unsigned t = 0; t < nth; ++t) pool.emplace_back(convert, ne * t / nth, ne * (t + 1) / nth);
+            unsigned started = 0;
+            try {
+                for (; started < nth; ++started) pool.emplace_back(convert, ne * started / nth, ne * (started + 1) / nth);
+            } catch (const std::system_error &) {
+            }
+            if (started < nth) convert(ne * started / nth, ne);
             for (auto &th : pool) th.join();
         }
         if (failed) throw Error(ERR_IO, "input data: out of memory while reading the values");

@@ -34,6 +34,7 @@ __all__ = [
     "maxcut",
     "theta",
     "with_lp",
+    "blocks_with_lp",
     "control_like",
     "batch",
     "workload",
@@ -50,6 +51,11 @@ class _Writer:
     def __init__(self, m: int, blocks: list[int], c: np.ndarray, title: str):
         self.buf = io.StringIO()
         w = self.buf.write
+        # the reference reads the title line into a 256-byte buffer
+        # (sdpa_io.cpp:127, lengthOfString) and parses the rest of a longer
+        # line as data
+        if len(title) > 200:
+            title = title[:197] + "..."
         w(f'"{title}"\n')
         w(f"{m} = mDIM\n{len(blocks)} = nBLOCK\n")
         w(" ".join(str(b) for b in blocks) + " = bLOCKsTRUCT\n")
@@ -70,7 +76,7 @@ class _Writer:
         return self.buf.getvalue()
 
 
-def _dense_blocks(rng, m: int, sizes: list[int], scale_by_n: bool):
+def _dense_blocks(rng, m: int, sizes: list[int], scale_by_n: bool, with_x0: bool = False):
     """F_k per block ~ N(0,1) (or N(0,1)/sqrt(n)), symmetric; x0 ~ N(0,1);
     X0 = I + G G^T / n per block; F_0 = sum_k F_k x0_k - X0; c_k = tr F_k
     so that Y = I is dual feasible and x0 is primal feasible."""
@@ -87,6 +93,8 @@ def _dense_blocks(rng, m: int, sizes: list[int], scale_by_n: bool):
         F0.append(np.tensordot(x0, A, axes=1) - X0)
         c += np.trace(A, axis1=1, axis2=2)
         Fs.append(A)
+    if with_x0:
+        return c, F0, Fs, x0
     return c, F0, Fs
 
 
@@ -135,6 +143,36 @@ def with_lp(n: int = 30, q: int = 24, m: int = 40, seed: int = 7) -> str:
         w.dense_upper(k + 1, 1, A[k])
         nz = np.nonzero(a[k])[0]
         w.entries(k + 1, 2, nz, nz, a[k, nz])
+    return w.text()
+
+
+def blocks_with_lp(sizes=(30,), q: int = 0, m: int = 40, seed: int = 8) -> str:
+    """Dense SDP blocks of the given orders (the config-0 construction per
+    block, entries N(0,1)/sqrt(n)) and, with q > 0, an LP block of q entries
+    (coefficients N(0,1) on about half of them, slacks 1 + U(0,1) at x0):
+    strictly feasible on both sides (Y = I, y_lp = 1 is dual feasible).
+    Many small blocks exercise the per-block paths (inner products, step
+    lengths) beyond a handful of blocks."""
+    rng = np.random.default_rng(seed)
+    sizes = [int(n) for n in sizes]
+    c, F0, Fs, x0 = _dense_blocks(rng, m, sizes, scale_by_n=True, with_x0=True)
+    blocks = list(sizes)
+    if q > 0:
+        a = rng.standard_normal((m, q)) * (rng.random((m, q)) < 0.5)
+        f0 = x0 @ a - (1.0 + rng.random(q))
+        c = c + a.sum(axis=1)
+        blocks.append(-q)
+    w = _Writer(m, blocks, c, f"{len(sizes)} SDP blocks + LP {q}, m={m} seed={seed}")
+    for b in range(len(sizes)):
+        w.dense_upper(0, b + 1, F0[b])
+    if q > 0:
+        w.entries(0, len(sizes) + 1, range(q), range(q), f0)
+    for k in range(m):
+        for b in range(len(sizes)):
+            w.dense_upper(k + 1, b + 1, Fs[b][k])
+        if q > 0:
+            nz = np.nonzero(a[k])[0]
+            w.entries(k + 1, len(sizes) + 1, nz, nz, a[k, nz])
     return w.text()
 
 

@@ -1,0 +1,168 @@
+"""The full-size workloads against the reference build.
+
+* Whole solves of the max-cut shape (n = m = 500, F3 Schur), the
+  control shape (blocks 100 + 50, m = 1326, F1 Schur) and a theta shape
+  (120 vertices, m = 3571, F3 + F2 Schur), in the plain dd form and in
+  the tensor-core split form, against the reference's own solves
+  (tests/golden/large_solves.json, made by tests/golden/make_large_golden.py
+  with oracle/_ref): under the bar of tests/test_gpu_solve.py -- mu after
+  every pass within max(1e-25, 10 x the reference's own run-to-run spread)
+  up to the first pass where that spread exceeds 1e-20, the phase (and the
+  iteration count, where every reference run agrees), and objectives within
+  max(1e-24, 10 x the reference runs' spread).
+* The Schur matrix of the headline workload (theta-shaped, 200 vertices,
+  m = 9980, 1.6 GB) at an interior point, bit for bit against the
+  reference's Make_bMat (oracle/_ref, run in the test process), and its
+  Cholesky factor in the split form within 1e-27 of the largest entry of
+  the plain dd factor.
+"""
+import ctypes
+import importlib.util
+import json
+from decimal import Decimal, getcontext
+
+import numpy as np
+import pytest
+
+from conftest import DD, ROOT, RefSolver, load_pkg, ptr
+from test_oracle import same
+
+pytestmark = pytest.mark.gpu
+getcontext().prec = 60
+GFILE = ROOT / "tests" / "golden" / "large_solves.json"
+GOLDEN = json.loads(GFILE.read_text()) if GFILE.exists() else {}
+
+
+def _mk():
+    spec = importlib.util.spec_from_file_location("mkl", ROOT / "tests" / "golden" / "make_large_golden.py")
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    return mk
+
+
+MK = _mk()
+
+
+def _dec(x):
+    return Decimal(x[0]) + Decimal(x[1])
+
+
+def _rel(a, b):
+    return abs(a - b) / max(abs(b), Decimal(1))
+
+
+@pytest.mark.parametrize("form", ["plain", "tc16"])
+@pytest.mark.parametrize("name", sorted(GOLDEN))
+def test_large_solve_matches_reference(name, form, workdir):
+    sddd = load_pkg()
+    make, eps = MK.CASES[name]
+    data = workdir / f"large_{name}.dat-s"
+    if not data.exists():
+        data.write_text(make())
+    par = sddd.param(MK.P.write_param(str(workdir / f"large_{name}.param"), eps=eps))
+    g = GOLDEN[name]
+    with sddd.Context(0) as c:
+        c.read_problem(data, sparse=True, kappa=1.2)
+        assert c.L.sddd_set_tc_split(c.h, 16 if form == "tc16" else 0) == 0
+        c.call("sddd_solver_start", ctypes.byref(par))
+        mus = []
+        res = sddd.SdddResult()
+        while c.L.sddd_iterate(c.h) == 0:
+            c.call("sddd_solver_result", ctypes.byref(res))
+            mus.append(Decimal(res.mu.hi) + Decimal(res.mu.lo))
+        r = c.solve(par)
+    spread = g["mu_spread"]
+    chaos = next((q for q, s_ in enumerate(spread) if s_ > 1e-20), len(spread))
+    assert chaos >= 3, chaos
+    for q in range(min(chaos, len(mus))):
+        want = _dec(g["mu_trajectory"][q])
+        tol = max(Decimal("1e-25"), 10 * Decimal(spread[q]))
+        assert abs(mus[q] - want) / abs(want) <= tol, (q, mus[q], want, spread[q])
+    phase = sddd.PHASES[r.phase]
+    if all(v["phase"] == g["phase"] and v["iterations"] == g["iterations"] for v in g["variants"]):
+        assert phase == g["phase"], (phase, g["phase"])
+        assert r.iterations == g["iterations"], (r.iterations, g["iterations"])
+    else:
+        assert phase in {g["phase"]} | {v["phase"] for v in g["variants"]}, phase
+    for nm in ("objValPrimal", "objValDual"):
+        want = _dec(g[nm])
+        spr = max([_rel(_dec(v[nm]), want) for v in g["variants"]], default=Decimal(0))
+        got = Decimal(getattr(r, nm).hi) + Decimal(getattr(r, nm).lo)
+        print(f"{name} {form}: {nm} off by {float(_rel(got, want)):.1e} (reference spread {float(spr):.1e})")
+        assert _rel(got, want) <= max(Decimal("1e-24"), 10 * spr), (nm, got, want)
+
+
+def _spd_block(rng, n, shift):
+    """A symmetric positive definite n x n dd matrix (column-major), with
+    random low parts."""
+    G = rng.standard_normal((n, n))
+    A = shift * np.eye(n) + G @ G.T / n
+    out = np.zeros((n, n), DD)
+    out["hi"] = A
+    lo = A * rng.uniform(-1, 1, (n, n)) * 1e-17
+    out["lo"] = 0.5 * (lo + lo.T)
+    return np.ascontiguousarray(out.ravel(order="F"))
+
+
+@pytest.fixture(scope="module")
+def theta_m9980(workdir):
+    P = MK.P
+    path = workdir / "theta_nv200.dat-s"
+    if not path.exists():
+        path.write_text(P.theta(nv=200, p=0.5, seed=2))
+    rng = np.random.default_rng(9980)
+    X = _spd_block(rng, 200, 1.0)
+    Z = _spd_block(rng, 200, 2.0)
+    return path, X, Z
+
+
+def test_theta_m9980_schur_matrix_matches_reference(theta_m9980, ref_lib):
+    sddd = load_pkg()
+    path, X, Z = theta_m9980
+    ref = RefSolver(ref_lib, path)
+    try:
+        m = ref.m
+        assert m == 9980
+        y = np.zeros(m, DD)
+        y["hi"] = np.random.default_rng(1).standard_normal(m)
+        assert ref_lib.ref_set_point(ref.h, ptr(X), ptr(y), ptr(Z)) == 0
+        want = ref.schur()
+    finally:
+        ref.close()
+    with sddd.Context(0) as c:
+        c.read_problem(path, sparse=True, kappa=1.2)
+        assert c.set_point(X, y, Z) == 0
+        c.call("sddd_schur_build")
+        got = c.get("B")
+    r_ = same(got, want)
+    assert r_, r_
+
+
+def test_theta_m9980_split_factor_close_to_plain(theta_m9980):
+    import torch
+    sddd = load_pkg()
+    path, X, Z = theta_m9980
+    with sddd.Context(0) as c:
+        c.read_problem(path, sparse=True, kappa=1.2)
+        m = c.m
+        y = np.zeros(m, DD)
+        assert c.set_point(X, y, Z) == 0
+        c.call("sddd_schur_build")
+        B = torch.from_numpy(c.get("B").view(np.float64)).cuda()
+        B2 = B.clone()
+        assert c.L.sddd_Rpotrf(c.h, m, ctypes.c_void_p(B.data_ptr()), m) == 0
+        assert c.L.sddd_set_tc_split(c.h, 16) == 0
+        assert c.L.sddd_Rpotrf(c.h, m, ctypes.c_void_p(B2.data_ptr()), m) == 0
+        c.L.sddd_set_tc_split(c.h, 0)
+        torch.cuda.synchronize()
+        # lower triangles, hi + lo as one float64 difference (the values
+        # agree to far more than 2^-53 of the largest entry)
+        Lp = B.view(m, m, 2)  # [column][row] (column-major)
+        Ls = B2.view(m, m, 2)
+        rows = torch.arange(m, device="cuda")
+        lower = rows[None, :] >= rows[:, None]  # [col][row]: row >= col
+        d = ((Ls[..., 0] - Lp[..., 0]) + (Ls[..., 1] - Lp[..., 1])).abs() * lower
+        big = (Lp[..., 0].abs() * lower).max().item()
+        worst = d.max().item()
+    print(f"theta m=9980: split factor within {worst / big:.1e} of the plain factor's largest entry")
+    assert worst <= 1e-27 * big, (worst, big)

@@ -5,7 +5,7 @@ reference's dd results bit for bit (+0 and -0 compared equal):
   - the 18 dd operation shapes against QD;
   - dd GEMM / Cholesky / triangular solves against the oracle;
   - at real iterates of small seeded problems (dense F1, max-cut F3,
-    theta F2+F3, two-block F1): L_X^-1, L_Z^-1, Z^-1, the residuals, the
+    theta F2+F3, two-block F1, 80 small blocks): L_X^-1, L_Z^-1, Z^-1, the residuals, the
     Schur matrix B, the predictor and corrector right-hand sides and the
     directions Dx, Dy, Dz of the reference's own pinpal state.
 The step-length eigenvalue (Lanczos / small-block path) must agree within
@@ -29,6 +29,9 @@ SMALL = {
     "theta": lambda P: P.theta(nv=24, p=0.5, seed=12),
     "control": lambda P: P.control_like(sizes=(9, 6), m=25, seed=13),
     "dense_big": lambda P: P.dense_random(n=50, m=40, seed=14),
+    # 80 dense blocks of orders 2..8 (more per-block results than the
+    # solver's earlier fixed scratch held)
+    "blocks80": lambda P: P.blocks_with_lp(sizes=np.random.default_rng(21).integers(2, 9, 80), q=0, m=60, seed=21),
 }
 
 
