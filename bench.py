@@ -636,7 +636,7 @@ def profile_case(args):
             raise RuntimeError(L.sddd_last_error(ctx.h).decode())
         torch.cuda.synchronize()
         t = time.perf_counter()
-        info = L.sddd_Rpotrf(ctx.h, m, ctypes.c_void_p(dd.data_ptr()), m)
+        info = L.sddd_Rpotrf(ctx.h, b"L", m, ctypes.c_void_p(dd.data_ptr()), m)
         torch.cuda.synchronize()
         print(json.dumps({"case": "potrf", "m": m, "info": info, "s": time.perf_counter() - t}))
     return 0 if info == 0 else 1

@@ -266,11 +266,43 @@ int sddd_get_tc_split(const sddd_ctx *ctx);
  * P n x k with k <= 64) through the same slice products. */
 int sddd_Rsyrk_tc(sddd_ctx *ctx, long n, long k, const sddd_dd *P, long ldp, sddd_dd *C, long ldc, int slices);
 
-/* -- dd kernels on device memory (MPLAPACK-like; pointers are device
- *    pointers to column-major sddd_dd) -- */
-int sddd_Rgemm(sddd_ctx *ctx, char transa, char transb, long m, long n, long k, sddd_dd *A, long lda, sddd_dd *B, long ldb, sddd_dd *C, long ldc);
-int sddd_Rpotrf(sddd_ctx *ctx, long n, sddd_dd *A, long lda); /* lower, returns info */
-int sddd_Rtrsv(sddd_ctx *ctx, char trans, long n, sddd_dd *L, long lda, sddd_dd *x);
+/* -- bounded waits (no counterpart in the reference) --
+ * Every device wait of the context's kernels (the triangular solves' waits
+ * for another CTA's block, the split kernel's barrier waits) gives up after
+ * `seconds` (default 2, range 1e-4..60): the kernel records the block or
+ * barrier, lets its copies in flight land and returns, and the call that
+ * launched it returns SDDD_ERR_CUDA naming it; the context stays usable. */
+int sddd_set_wait_limit(sddd_ctx *ctx, double seconds);
+/* Tests of that path: the triangular solves never publish the completion
+ * flag of 64-entry block `block` (-1: publish all, the default), so every
+ * wait for it runs out.  Not for production use. */
+int sddd_test_withhold_block(sddd_ctx *ctx, int block);
+
+/* -- dd kernels on device memory: the MPLAPACK seam --
+ * The argument lists of MPLAPACK's dd routines (mplapack/mpblas_dd.h:47,54,
+ * mplapack/mplapack_dd.h:41) with the context first; pointers are device
+ * pointers to column-major sddd_dd.  Bad arguments return SDDD_ERR_ARG
+ * naming the routine and the 1-based position the reference's Mxerbla_dd
+ * would report (in its order of checks); valid forms SDPA never calls
+ * return SDDD_ERR_UNSUPPORTED.  Results are the reference's bit for bit
+ * (with the tensor-core split off). */
+/* Rgemm (mpblas_dd.h:54, mplapack/Rgemm_omp.cpp): C = alpha op(A) op(B)
+ * + beta C, transa/transb 'N', 'T' or 'C'. */
+int sddd_Rgemm(sddd_ctx *ctx, char transa, char transb, long m, long n, long k, sddd_dd alpha, const sddd_dd *A, long lda, const sddd_dd *B, long ldb,
+               sddd_dd beta, sddd_dd *C, long ldc);
+/* Rpotrf (mplapack_dd.h:41, mplapack/Rpotrf.cpp), uplo 'L': returns info
+ * (0, or the 1-based column where A stopped being positive definite).
+ * With the tensor-core split on, its trailing updates are slice products. */
+int sddd_Rpotrf(sddd_ctx *ctx, char uplo, long n, sddd_dd *A, long lda);
+/* Rtrsv (mpblas_dd.h:47, mplapack/Rtrsv.cpp), uplo 'L', trans 'N'/'T'/'C',
+ * diag 'N', incx 1: x = op(A)^-1 x. */
+int sddd_Rtrsv(sddd_ctx *ctx, char uplo, char trans, char diag, long n, const sddd_dd *A, long lda, sddd_dd *x, long incx);
+/* Solve A X = B from the factor of sddd_Rpotrf (LAPACK's Rpotrs; the
+ * reference's MPLAPACK subset has none, SDPA calls Rtrsv twice), uplo 'L',
+ * nrhs columns of B.  Split off: the two Rtrsv of each column, bit for bit.
+ * Split on: blocked solves with the 64 x 64 diagonal blocks of the factor
+ * inverted once per call (no division on the critical path). */
+int sddd_Rpotrs(sddd_ctx *ctx, char uplo, long n, long nrhs, const sddd_dd *A, long lda, sddd_dd *B, long ldb);
 /* Elementwise dd operation on n device values: 0 a+b, 1 a+=b, 2/3 a-b,
  * 4 a*b, 5 a*=b, 6 a/b, 7 sqrt(a), 8 a*b.hi, 9 a+b.hi, 10 a-b.hi,
  * 11 a.hi-b, 12 a/b.hi, 13 a.hi/b, 14 -a, 15 |a|, 16 a^2, 17 a.hi+b.hi

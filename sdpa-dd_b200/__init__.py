@@ -84,10 +84,13 @@ def lib() -> ctypes.CDLL:
         "sddd_iterate": (ci, [vp]),
         "sddd_solver_result": (ci, [vp, ctypes.POINTER(SdddResult)]),
         "sddd_cli_main": (ci, [ci, vp]),
-        "sddd_Rgemm": (ci, [vp, cc, cc, cl, cl, cl, vp, cl, vp, cl, vp, cl]),
-        "sddd_Rpotrf": (ci, [vp, cl, vp, cl]),
-        "sddd_Rtrsv": (ci, [vp, cc, cl, vp, cl, vp]),
+        "sddd_Rgemm": (ci, [vp, cc, cc, cl, cl, cl, SdddDD, vp, cl, vp, cl, SdddDD, vp, cl]),
+        "sddd_Rpotrf": (ci, [vp, cc, cl, vp, cl]),
+        "sddd_Rtrsv": (ci, [vp, cc, cc, cc, cl, vp, cl, vp, cl]),
+        "sddd_Rpotrs": (ci, [vp, cc, cl, cl, vp, cl, vp, cl]),
         "sddd_set_tc_split": (ci, [vp, ci]),
+        "sddd_set_wait_limit": (ci, [vp, cd]),
+        "sddd_test_withhold_block": (ci, [vp, ci]),
         "sddd_get_tc_split": (ci, [vp]),
         "sddd_Rsyrk_tc": (ci, [vp, cl, cl, vp, cl, vp, cl, ci]),
         "sddd_dd_op": (ci, [vp, ci, cl, vp, vp, vp]),

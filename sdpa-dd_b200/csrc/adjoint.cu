@@ -104,10 +104,7 @@ int adjoint(Context &c, const dd_t *g_x, const dd_t *g_Y, const dd_t *g_X, dd_t 
     const int info = schur_factor(c);
     if (info != 0) return info;
     CK(cudaMemcpyAsync(c.adj_u.p, c.adj_v.p, sizeof(dd_t) * c.m, cudaMemcpyDeviceToDevice, st));
-    TrsvSync &sync = trsv_sync(c, c.m);
-    trsv_lower(st, 'N', c.B.p, c.m, c.m, c.adj_u.p, sync, c.shared_gpu);
-    trsv_lower(st, 'T', c.B.p, c.m, c.m, c.adj_u.p, sync, c.shared_gpu);
-    trsv_check(st, sync);
+    solve_B(c, c.adj_u.p);
     // R_g = g_Z' + sym(X A^T(u) Z^-1) = g_Z' - sym(X (-A^T(u)) Z^-1)
     sum_yA(c, c.adj_u.p, c.Dz, 0, nullptr, nullptr);
     triple(c, c.X, c.Dz, c.invZ, c.adj_T);

@@ -29,10 +29,14 @@ namespace sddd {
 // Tile: BM x BN outputs per CTA, BK-deep k slices staged in shared memory,
 // TM x TN outputs per thread.  Shared tiles are k-major and padded by one
 // element so that transposed tile loads do not collide on banks.
+// MODE GEMM_AB_PRE (Rgemm_NN/NT_omp with alpha): each B value is multiplied
+// by alpha as it is staged ("temp = alpha * B(l,j)"), then c += temp * a
+// from the (beta-scaled) C; GEMM_AB_POST (Rgemm_TN/TT_omp): the products
+// are summed from zero and C += alpha * sum.
 template <int BM, int BN, int BK, int TM, int TN, bool TA, bool TB, int MODE>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN))
     gemm_kernel(int M, int N, int K, const dd_t *__restrict__ A, long lda, long sA, const dd_t *__restrict__ B, long ldb, long sB, dd_t *C,
-                long ldc, long sC, int lower) {
+                long ldc, long sC, int lower, dd_t alpha) {
     constexpr int TX = BN / TN, TY = BM / TM, NT = TX * TY;
     __shared__ double2 As[BK][BM + 1];
     __shared__ double2 Bs[BK][BN + 1];
@@ -49,7 +53,7 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
 #pragma unroll
         for (int c = 0; c < TN; ++c) {
             int gi = i0 + ty + TY * r, gj = j0 + tx + TX * c;
-            if (MODE == GEMM_STORE || gi >= M || gj >= N)
+            if (MODE == GEMM_STORE || MODE == GEMM_AB_POST || gi >= M || gj >= N)
                 acc[r][c] = dd_zero();
             else
                 acc[r][c] = ld_dd(C + gi + ldc * (long)gj);
@@ -81,6 +85,10 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
             int gj = j0 + jj, gk = k0 + kk;
             double2 v = make_double2(0.0, 0.0);
             if (gj < N && gk < K) v = *reinterpret_cast<const double2 *>(TB ? B + gj + ldb * (long)gk : B + gk + ldb * (long)gj);
+            if (MODE == GEMM_AB_PRE) {
+                const dd_t t = dd_mul(alpha, dd_make(v.x, v.y));
+                v = make_double2(t.hi, t.lo);
+            }
             Bs[kk][jj] = v;
         }
         __syncthreads();
@@ -112,17 +120,47 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
 #pragma unroll
         for (int c = 0; c < TN; ++c) {
             int gi = i0 + ty + TY * r, gj = j0 + tx + TX * c;
-            if (gi < M && gj < N && (!lower || gi >= gj)) st_dd(C + gi + ldc * (long)gj, acc[r][c]);
+            if (gi < M && gj < N && (!lower || gi >= gj)) {
+                dd_t *cp = C + gi + ldc * (long)gj;
+                st_dd(cp, MODE == GEMM_AB_POST ? dd_acc(ld_dd(cp), dd_mul(alpha, acc[r][c])) : acc[r][c]);
+            }
         }
 }
 
 template <bool TA, bool TB, int MODE>
 static void gemm_launch(cudaStream_t st, int M, int N, int K, const dd_t *A, long lda, long sA, const dd_t *B, long ldb, long sB, dd_t *C, long ldc,
-                        long sC, int batch, bool lower) {
+                        long sC, int batch, bool lower, dd_t alpha = dd_t{1.0, 0.0}) {
     constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4;
     dim3 grid(ceil_div(N, BN), ceil_div(M, BM), batch);
-    gemm_kernel<BM, BN, BK, TM, TN, TA, TB, MODE><<<grid, (BM / TM) * (BN / TN), 0, st>>>(M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, lower ? 1 : 0);
+    gemm_kernel<BM, BN, BK, TM, TN, TA, TB, MODE>
+        <<<grid, (BM / TM) * (BN / TN), 0, st>>>(M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, lower ? 1 : 0, alpha);
     CK_LAUNCH();
+}
+
+// C = beta C as Rgemm's first loop: zero for beta == 0, unchanged for
+// beta == 1, else beta * C(i,j).
+__global__ void gemm_beta_kernel(dd_t *C, long ldc, int M, int N, dd_t beta) {
+    const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (e >= (long)M * N) return;
+    dd_t *cp = C + e % M + ldc * (e / M);
+    st_dd(cp, (beta.hi == 0.0 && beta.lo == 0.0) ? dd_zero() : dd_mul(beta, ld_dd(cp)));
+}
+
+void gemm_ab(cudaStream_t st, char ta, char tb, int M, int N, int K, dd_t alpha, const dd_t *A, long lda, const dd_t *B, long ldb, dd_t beta, dd_t *C,
+             long ldc) {
+    const bool one_beta = beta.hi == 1.0 && beta.lo == 0.0;
+    const bool zero_alpha = alpha.hi == 0.0 && alpha.lo == 0.0;
+    if (M <= 0 || N <= 0 || ((zero_alpha || K <= 0) && one_beta)) return; // Rgemm's quick return
+    if (!one_beta) {
+        gemm_beta_kernel<<<ceil_div((long)M * N, 256), 256, 0, st>>>(C, ldc, M, N, beta);
+        CK_LAUNCH();
+    }
+    if (zero_alpha || K <= 0) return;
+    const bool a = ta == 'T', b = tb == 'T';
+    if (!a && !b) gemm_launch<false, false, GEMM_AB_PRE>(st, M, N, K, A, lda, 0, B, ldb, 0, C, ldc, 0, 1, false, alpha);
+    else if (!a && b) gemm_launch<false, true, GEMM_AB_PRE>(st, M, N, K, A, lda, 0, B, ldb, 0, C, ldc, 0, 1, false, alpha);
+    else if (a && !b) gemm_launch<true, false, GEMM_AB_POST>(st, M, N, K, A, lda, 0, B, ldb, 0, C, ldc, 0, 1, false, alpha);
+    else gemm_launch<true, true, GEMM_AB_POST>(st, M, N, K, A, lda, 0, B, ldb, 0, C, ldc, 0, 1, false, alpha);
 }
 
 void gemm(cudaStream_t st, char ta, char tb, int mode, int M, int N, int K, const dd_t *A, long lda, long sA, const dd_t *B, long ldb, long sB,
@@ -423,8 +461,9 @@ void zero_upper(cudaStream_t st, dd_t *A, long lda, int n) {
 // Warp 0 holds the 64 entries of the current block, two per lane, and runs
 // the chains; the other warps stage the next tile of L in shared memory
 // (padded leading dimension 65: conflict-free for rows and columns).
-// A CTA waits for a block with an acquire load bounded by a 2 s budget;
-// on expiry it records the block in the error word and returns.
+// A CTA waits for a block with an acquire load bounded by the solve's wait
+// budget (2 s by default); on expiry it records the block in the error word
+// and returns.  Tests of that path name a block whose flag is withheld.
 constexpr int TRSV_B = 64;
 constexpr int TRSV_LD = 65;
 constexpr int TRSV_THREADS = 256;
@@ -437,6 +476,8 @@ struct TrsvArgs {
     int n, nblk, epoch;
     dd_t *x;
     int *flags, *err;
+    unsigned long long wait_ns;
+    int withhold; // a block whose flag is never published (-1: none)
 };
 
 __device__ __forceinline__ int ld_acquire_gpu(const int *p) {
@@ -459,7 +500,7 @@ __device__ bool trsv_wait(const TrsvArgs &a, int blk) {
         const unsigned long long t0 = global_ns();
         unsigned iter = 0;
         while (ld_acquire_gpu(a.flags + blk) != a.epoch) {
-            if (ld_acquire_gpu(a.err) != 0 || ++iter > (1u << 26) || global_ns() - t0 > 2000000000ull) {
+            if (ld_acquire_gpu(a.err) != 0 || ++iter > (1u << 26) || global_ns() - t0 > a.wait_ns) {
                 atomicCAS(a.err, 0, blk + 1);
                 ok = 0;
                 break;
@@ -562,7 +603,7 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_fwd_wave_kernel(TrsvArgs a)
             if (i1 < a.n) st_dd(a.x + i1, v1);
             __threadfence();
             __syncwarp();
-            if (lane == 0) st_release_gpu(a.flags + c, a.epoch);
+            if (lane == 0 && c != a.withhold) st_release_gpu(a.flags + c, a.epoch);
         }
         __syncthreads();
     }
@@ -633,7 +674,7 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_bwd_wave_kernel(TrsvArgs a)
             if (j1 < a.n) st_dd(a.x + j1, v1);
             __threadfence();
             __syncwarp();
-            if (lane == 0) st_release_gpu(a.flags + c, a.epoch);
+            if (lane == 0 && c != a.withhold) st_release_gpu(a.flags + c, a.epoch);
         }
         __syncthreads();
     }
@@ -657,7 +698,7 @@ void trsv_lower(cudaStream_t st, char trans, const dd_t *L, long lda, int n, dd_
     if (nblk > sync.capacity || !sync.flags) throw Error(ERR_ARG, "trsv: progress flags hold fewer blocks than the solve needs");
     PROF_SCOPE("trsv", st);
     if (++sync.epoch <= 0) sync.epoch = 1;
-    TrsvArgs a{L, lda, n, nblk, sync.epoch, x, sync.flags, sync.flags + sync.capacity};
+    TrsvArgs a{L, lda, n, nblk, sync.epoch, x, sync.flags, sync.flags + sync.capacity, sync.wait_ns, sync.withhold};
     const void *k = trans == 'N' ? (const void *)trsv_fwd_wave_kernel : (const void *)trsv_bwd_wave_kernel;
     static thread_local int cap[2][64] = {};
     int dev = 0;
@@ -694,7 +735,8 @@ void trsv_check(cudaStream_t st, const TrsvSync &sync) {
     }
     err = *h;
     if (err != 0)
-        throw Error(ERR_CUDA, "trsv: a block waited more than 2 s for block " + std::to_string(err - 1) + " (solve abandoned)");
+        throw Error(ERR_CUDA, "trsv: a wait ran out of its " + std::to_string(sync.wait_ns / 1000000ull) + " ms budget for block " + std::to_string(err - 1) +
+                                  " (solve abandoned)");
 }
 
 // ======================================================= triangular inverse

@@ -7,7 +7,7 @@ namespace sddd {
 
 struct OzakiWork;
 
-enum GemmMode { GEMM_STORE = 0, GEMM_SUB = 1, GEMM_ACC = 2 };
+enum GemmMode { GEMM_STORE = 0, GEMM_SUB = 1, GEMM_ACC = 2, GEMM_AB_PRE = 3, GEMM_AB_POST = 4 };
 constexpr int POTRF_NB = 64;
 
 // C = op(A) op(B) (STORE: sum from zero; SUB: C - p_0 - p_1 - ...;
@@ -18,6 +18,13 @@ void gemm(cudaStream_t st, char ta, char tb, int mode, int M, int N, int K, cons
 // In-place lower Cholesky; *info_dev = 0 or the failing 1-based column.
 // rdiag_dev holds POTRF_NB dd of scratch.  With tc, the trailing updates
 // run as tensor-core slice products (ozaki.h) instead of dd GEMMs.
+// C = alpha op(A) op(B) + beta C with MPLAPACK Rgemm's operation order
+// (mplapack/Rgemm_omp.cpp and Rgemm_{NN,NT,TN,TT}_omp.cpp): C is scaled by
+// beta first (zeroed for beta == 0, untouched for beta == 1); then for
+// 'N' A each C(i,j) takes c += (alpha B(l,j)) A(i,l) for l ascending, for
+// 'T' A c += alpha (sum_l A(l,i) B(l,j)).  op: 'N' or 'T'.
+void gemm_ab(cudaStream_t st, char ta, char tb, int M, int N, int K, dd_t alpha, const dd_t *A, long lda, const dd_t *B, long ldb, dd_t beta, dd_t *C,
+             long ldc);
 void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag_dev, OzakiWork *tc = nullptr);
 void zero_upper(cudaStream_t st, dd_t *A, long lda, int n);
 // Progress words of the one-launch triangular solve: one flag per 64-entry
@@ -29,6 +36,8 @@ struct TrsvSync {
     int epoch = 0;
     int *h_err = nullptr; // pinned host word for reading the error word (or null)
     cudaEvent_t wait_ev = nullptr; // blocking-sync event to wait on (or null: stream sync)
+    unsigned long long wait_ns = 2000000000ull; // budget of one wait for a block
+    int withhold = -1; // tests of the bounded waits: this block's flag is never published
 };
 // x = L^-1 x ('N') or L^-T x ('T'), L lower, as Rtrsv("Lower", trans, "NonUnit").
 // shared_gpu: other streams keep the GPU busy (a batch worker); short
@@ -37,6 +46,14 @@ void trsv_lower(cudaStream_t st, char trans, const dd_t *L, long lda, int n, dd_
 // Throws when a solve since the flags were zeroed gave up waiting
 // (synchronises st).
 void trsv_check(cudaStream_t st, const TrsvSync &sync);
+// W_c = L(c,c)^-1 for the 64 x 64 diagonal blocks of L (order n): W holds
+// ceil(n/64) blocks of 64 x 64 (leading dimension 64), zero above the
+// diagonal.
+void trsv_diag_inverse(cudaStream_t st, const dd_t *L, long lda, int n, dd_t *W);
+// x = L^-1 x ('N') or L^-T x ('T') by blocks, with W from
+// trsv_diag_inverse: one cooperative launch; the same progress words and
+// error reporting (trsv_check) as trsv_lower.  Not Rtrsv's operation order.
+void trsv_blocked(cudaStream_t st, char trans, const dd_t *L, long lda, int n, const dd_t *W, dd_t *x, TrsvSync &sync);
 void inv_lower(cudaStream_t st, const dd_t *L, long lda, int n, dd_t *X, long ldx);
 void trmm_lt(cudaStream_t st, const dd_t *M, long ldm, int n, dd_t *B, long ldb);
 void symmetrize(cudaStream_t st, dd_t *A, int n);

@@ -606,19 +606,48 @@ int sddd_work(const sddd_ctx *cctx, double *schur_ddflops, double *chol_ddflops)
     });
 }
 
-int sddd_Rgemm(sddd_ctx *ctx, char ta, char tb, long m, long n, long k, sddd_dd *A, long lda, sddd_dd *B, long ldb, sddd_dd *C, long ldc) {
+namespace {
+inline char up(char c) { return (c >= 'a' && c <= 'z') ? (char)(c - 'a' + 'A') : c; }
+inline dd_t from(sddd_dd v) { return dd_t{v.hi, v.lo}; }
+// MPLAPACK's argument errors (Mxerbla_dd: the routine's name and the
+// 1-based position of the first bad argument) as an SDDD_ERR_ARG.
+[[noreturn]] void bad_arg(const char *routine, int pos, const char *what) {
+    throw sddd::Error(SDDD_ERR_ARG, std::string(routine) + ": parameter " + std::to_string(pos) + " (" + what + ") is invalid");
+}
+} // namespace
+
+int sddd_Rgemm(sddd_ctx *ctx, char transa, char transb, long m, long n, long k, sddd_dd alpha, const sddd_dd *A, long lda, const sddd_dd *B, long ldb,
+               sddd_dd beta, sddd_dd *C, long ldc) {
     return guarded(ctx, [&] {
         if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
-        sddd::gemm(ctx->c->stream, ta, tb, sddd::GEMM_STORE, (int)m, (int)n, (int)k, reinterpret_cast<dd_t *>(A), lda, 0, reinterpret_cast<dd_t *>(B), ldb, 0,
-                   reinterpret_cast<dd_t *>(C), ldc, 0, 1, false);
+        const char ta = up(transa), tb = up(transb);
+        const bool nota = ta == 'N', notb = tb == 'N';
+        const long nrowa = nota ? m : k, nrowb = notb ? k : n;
+        // the checks and their order of mplapack/Rgemm_omp.cpp
+        if (!nota && ta != 'C' && ta != 'T') bad_arg("Rgemm", 1, "transa");
+        if (!notb && tb != 'C' && tb != 'T') bad_arg("Rgemm", 2, "transb");
+        if (m < 0) bad_arg("Rgemm", 3, "m");
+        if (n < 0) bad_arg("Rgemm", 4, "n");
+        if (k < 0) bad_arg("Rgemm", 5, "k");
+        if (lda < std::max(1L, nrowa)) bad_arg("Rgemm", 8, "lda");
+        if (ldb < std::max(1L, nrowb)) bad_arg("Rgemm", 10, "ldb");
+        if (ldc < std::max(1L, m)) bad_arg("Rgemm", 13, "ldc");
+        sddd::gemm_ab(ctx->c->stream, nota ? 'N' : 'T', notb ? 'N' : 'T', (int)m, (int)n, (int)k, from(alpha), reinterpret_cast<const dd_t *>(A), lda,
+                      reinterpret_cast<const dd_t *>(B), ldb, from(beta), reinterpret_cast<dd_t *>(C), ldc);
         CK(cudaStreamSynchronize(ctx->c->stream));
         return SDDD_OK;
     });
 }
 
-int sddd_Rpotrf(sddd_ctx *ctx, long n, sddd_dd *A, long lda) {
+int sddd_Rpotrf(sddd_ctx *ctx, char uplo, long n, sddd_dd *A, long lda) {
     return guarded(ctx, [&] {
         if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
+        const char u = up(uplo);
+        if (u != 'L' && u != 'U') bad_arg("Rpotrf", 1, "uplo");
+        if (n < 0) bad_arg("Rpotrf", 2, "n");
+        if (lda < std::max(1L, n)) bad_arg("Rpotrf", 4, "lda");
+        if (u == 'U') throw sddd::Error(SDDD_ERR_UNSUPPORTED, "Rpotrf: only uplo = 'L' (the form SDPA calls) is implemented");
+        if (n == 0) return SDDD_OK;
         sddd::Context &c = *ctx->c;
         if (!c.info.p) c.info.alloc(4);
         if (!c.rdiag.p) c.rdiag.alloc(256);
@@ -631,6 +660,22 @@ int sddd_Rpotrf(sddd_ctx *ctx, long n, sddd_dd *A, long lda) {
         if (tc) sddd::ozaki_check(c.stream, *tc);
         return info;
     });
+}
+
+int sddd_set_wait_limit(sddd_ctx *ctx, double seconds) {
+    if (!ctx || !ctx->c) return SDDD_ERR_ARG;
+    if (!(seconds >= 1e-4 && seconds <= 60.0)) {
+        ctx->err = "sddd_set_wait_limit: seconds must lie in [1e-4, 60]";
+        return SDDD_ERR_ARG;
+    }
+    ctx->c->wait_ns = (unsigned long long)(seconds * 1e9);
+    return SDDD_OK;
+}
+
+int sddd_test_withhold_block(sddd_ctx *ctx, int block) {
+    if (!ctx || !ctx->c || block < -1) return SDDD_ERR_ARG;
+    ctx->c->withhold_block = block;
+    return SDDD_OK;
 }
 
 int sddd_set_tc_split(sddd_ctx *ctx, int slices) {
@@ -660,12 +705,61 @@ int sddd_Rsyrk_tc(sddd_ctx *ctx, long n, long k, const sddd_dd *P, long ldp, sdd
     });
 }
 
-int sddd_Rtrsv(sddd_ctx *ctx, char trans, long n, sddd_dd *L, long lda, sddd_dd *x) {
+int sddd_Rtrsv(sddd_ctx *ctx, char uplo, char trans, char diag, long n, const sddd_dd *A, long lda, sddd_dd *x, long incx) {
     return guarded(ctx, [&] {
         if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
+        const char u = up(uplo), t = up(trans), d = up(diag);
+        // the checks and their order of mplapack/Rtrsv.cpp
+        if (u != 'U' && u != 'L') bad_arg("Rtrsv", 1, "uplo");
+        if (t != 'N' && t != 'T' && t != 'C') bad_arg("Rtrsv", 2, "trans");
+        if (d != 'U' && d != 'N') bad_arg("Rtrsv", 3, "diag");
+        if (n < 0) bad_arg("Rtrsv", 4, "n");
+        if (lda < std::max(1L, n)) bad_arg("Rtrsv", 6, "lda");
+        if (incx == 0) bad_arg("Rtrsv", 8, "incx");
+        if (u != 'L' || d != 'N' || incx != 1)
+            throw sddd::Error(SDDD_ERR_UNSUPPORTED, "Rtrsv: only uplo = 'L', diag = 'N', incx = 1 (the form SDPA calls) is implemented");
+        if (n == 0) return SDDD_OK;
         sddd::TrsvSync &sync = sddd::trsv_sync(*ctx->c, (int)n);
-        sddd::trsv_lower(ctx->c->stream, trans, reinterpret_cast<dd_t *>(L), lda, (int)n, reinterpret_cast<dd_t *>(x), sync);
+        sddd::trsv_lower(ctx->c->stream, t == 'N' ? 'N' : 'T', reinterpret_cast<const dd_t *>(A), lda, (int)n, reinterpret_cast<dd_t *>(x), sync);
         sddd::trsv_check(ctx->c->stream, sync);
+        return SDDD_OK;
+    });
+}
+
+int sddd_Rpotrs(sddd_ctx *ctx, char uplo, long n, long nrhs, const sddd_dd *A, long lda, sddd_dd *B, long ldb) {
+    return guarded(ctx, [&] {
+        if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
+        const char u = up(uplo);
+        if (u != 'L' && u != 'U') bad_arg("Rpotrs", 1, "uplo");
+        if (n < 0) bad_arg("Rpotrs", 2, "n");
+        if (nrhs < 0) bad_arg("Rpotrs", 3, "nrhs");
+        if (lda < std::max(1L, n)) bad_arg("Rpotrs", 5, "lda");
+        if (ldb < std::max(1L, n)) bad_arg("Rpotrs", 7, "ldb");
+        if (u == 'U') throw sddd::Error(SDDD_ERR_UNSUPPORTED, "Rpotrs: only uplo = 'L' is implemented");
+        if (n == 0 || nrhs == 0) return SDDD_OK;
+        sddd::Context &c = *ctx->c;
+        const dd_t *L = reinterpret_cast<const dd_t *>(A);
+        sddd::TrsvSync &sync = sddd::trsv_sync(c, (int)n);
+        if (c.tc_slices > 0) {
+            // the split form's blocked solves; the inverted diagonal blocks
+            // take the context's buffer (a Newton solve in progress
+            // recomputes them at its next factorisation)
+            c.winv_valid = false;
+            c.trsv_winv.alloc((size_t)sddd::ceil_div(n, 64L) * 64 * 64);
+            sddd::trsv_diag_inverse(c.stream, L, lda, (int)n, c.trsv_winv.p);
+            for (long r = 0; r < nrhs; ++r) {
+                dd_t *x = reinterpret_cast<dd_t *>(B) + ldb * r;
+                sddd::trsv_blocked(c.stream, 'N', L, lda, (int)n, c.trsv_winv.p, x, sync);
+                sddd::trsv_blocked(c.stream, 'T', L, lda, (int)n, c.trsv_winv.p, x, sync);
+            }
+        } else {
+            for (long r = 0; r < nrhs; ++r) {
+                dd_t *x = reinterpret_cast<dd_t *>(B) + ldb * r;
+                sddd::trsv_lower(c.stream, 'N', L, lda, (int)n, x, sync);
+                sddd::trsv_lower(c.stream, 'T', L, lda, (int)n, x, sync);
+            }
+        }
+        sddd::trsv_check(c.stream, sync);
         return SDDD_OK;
     });
 }

@@ -101,6 +101,7 @@ OzakiWork &tc_work(Context &c, int n, int slices) {
         CK(cudaEventCreateWithFlags(&c.tc.ev_diag, cudaEventDisableTiming));
     }
     c.tc.slices_used = slices;
+    c.tc.wait_ns = c.wait_ns;
     return c.tc;
 }
 
@@ -112,6 +113,8 @@ TrsvSync &trsv_sync(Context &c, int n) {
         CK(cudaMemsetAsync(c.trsv_flags.p, 0, sizeof(int) * ((size_t)nblk + 1), c.stream));
         c.trsv = TrsvSync{c.trsv_flags.p, nblk, 0, static_cast<int *>(c.h_pin), c.sync_ev};
     }
+    c.trsv.wait_ns = c.wait_ns;
+    c.trsv.withhold = c.withhold_block;
     return c.trsv;
 }
 

@@ -171,9 +171,20 @@ struct Context {
     DBuf<int> eig_ids_big, eig_ids_small;
     DBuf<dd_t> eig_work;
     TrsvSync trsv;
+    // budget of every bounded device wait of this context's kernels (the
+    // triangular solves' block flags, the split kernel's barriers), and a
+    // block whose completion flag the triangular solves withhold (-1: none;
+    // set only by tests of the bounded waits)
+    unsigned long long wait_ns = 2000000000ull;
+    int withhold_block = -1;
     // tensor-core split of the Cholesky trailing updates of B: slices per
     // value (8..16), 0 = plain dd GEMMs (the reference's operation order)
     int tc_slices = 0;
+    // inverses of the 64 x 64 diagonal blocks of the split form's factor of
+    // B (the blocked solves' W_c); valid from a successful split
+    // factorisation until the next factorisation
+    DBuf<dd_t> trsv_winv;
+    bool winv_valid = false;
     DBuf<int8_t> tc_slice_buf;
     DBuf<int> tc_exps, tc_err;
     OzakiWork tc;

@@ -164,19 +164,37 @@ void make_rhs(Context &c, bool corrector, dd_t beta_mu, bool dual_infeasible) {
 int schur_factor(Context &c) {
     CK(cudaMemsetAsync(c.info.p, 0, sizeof(int), c.stream));
     OzakiWork *tc = c.tc_slices > 0 ? &tc_work(c, c.m, c.tc_slices) : nullptr;
+    c.winv_valid = false;
     potrf(c.stream, c.B.p, c.m, c.m, c.info.p, c.rdiag.p, tc);
     int info = 0;
     d2h(c, &info, c.info.p, sizeof(int));
-    if (tc) ozaki_check(c.stream, *tc);
+    if (tc) {
+        ozaki_check(c.stream, *tc);
+        if (info == 0) {
+            // the split form's solves go by blocks (trsv_blocked)
+            c.trsv_winv.alloc((size_t)ceil_div(c.m, 64) * 64 * 64);
+            trsv_diag_inverse(c.stream, c.B.p, c.m, c.m, c.trsv_winv.p);
+            c.winv_valid = true;
+        }
+    }
     return info;
+}
+
+void solve_B(Context &c, dd_t *x) {
+    TrsvSync &sync = trsv_sync(c, c.m);
+    if (c.winv_valid) {
+        trsv_blocked(c.stream, 'N', c.B.p, c.m, c.m, c.trsv_winv.p, x, sync);
+        trsv_blocked(c.stream, 'T', c.B.p, c.m, c.m, c.trsv_winv.p, x, sync);
+    } else {
+        trsv_lower(c.stream, 'N', c.B.p, c.m, c.m, x, sync, c.shared_gpu);
+        trsv_lower(c.stream, 'T', c.B.p, c.m, c.m, x, sync, c.shared_gpu);
+    }
+    trsv_check(c.stream, sync);
 }
 
 void solve_dy(Context &c) {
     CK(cudaMemcpyAsync(c.Dy.p, c.g.p, sizeof(dd_t) * c.m, cudaMemcpyDeviceToDevice, c.stream));
-    TrsvSync &sync = trsv_sync(c, c.m);
-    trsv_lower(c.stream, 'N', c.B.p, c.m, c.m, c.Dy.p, sync, c.shared_gpu);
-    trsv_lower(c.stream, 'T', c.B.p, c.m, c.m, c.Dy.p, sync, c.shared_gpu);
-    trsv_check(c.stream, sync);
+    solve_B(c, c.Dy.p);
 }
 
 void make_dz_dx(Context &c, bool dual_infeasible) {

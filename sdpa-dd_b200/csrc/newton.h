@@ -20,6 +20,10 @@ void schur_build(Context &c);
 int schur_factor(Context &c);
 // Dy = B^-1 g from the factor (Lal::solveSystems, sdpa_linear.cpp:639-651).
 void solve_dy(Context &c);
+// x = B^-1 x from the factor of B in place: the reference's two Rtrsv
+// (bit for bit) after a plain factorisation, blocked solves with the
+// inverted diagonal blocks after a split one.
+void solve_B(Context &c, dd_t *x);
 // Newton::compute_DzMat + compute_DxMat (sdpa_newton.cpp:1318-1343).
 void make_dz_dx(Context &c, bool dual_infeasible);
 // Inner products of the reference's Lal::let(ret, '=', a, '.', b).

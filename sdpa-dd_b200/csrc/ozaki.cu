@@ -42,7 +42,8 @@
 // K-major, non-swizzled canonical layout of the MMA's shared-memory
 // descriptors (LBO 128 bytes between the two K chunks of one MMA, SBO 512
 // bytes between row groups), so a tile's stacked B slices are contiguous.
-// Every mbarrier wait is bounded (2 s); on expiry the CTA records a code in
+// Every mbarrier wait is bounded (the context's wait budget, 2 s by
+// default); on expiry the CTA records a code in
 // the error word, stops issuing, waits (bounded) for what it issued and
 // frees its tensor memory.
 #include "ozaki.h"
@@ -50,6 +51,7 @@
 #include <algorithm>
 #include <string>
 
+#include "bulk.cuh"
 #include "prof.h"
 
 namespace sddd {
@@ -76,48 +78,22 @@ static_assert(OZ_SMEM <= 232448 - 256, "split kernel: shared memory above the pe
 __host__ __device__ constexpr uint32_t oz_idesc(int n) {
     return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(OZ_ROWS_A >> 4) << 24);
 }
-constexpr unsigned long long OZ_WAIT_NS = 2000000000ull;
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ unsigned long long oz_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t *b) { asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory"); }
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *b, uint32_t parity) {
-    uint32_t ok;
-    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-                 : "=r"(ok)
-                 : "r"(smem_u32(b)), "r"(parity)
-                 : "memory");
-    return ok != 0;
-}
+__device__ __forceinline__ unsigned long long oz_ns() { return globaltimer_ns(); }
 // Waits for the phase with the given parity to complete; false when the CTA
 // is aborting or the wait ran out (then the CTA aborts with `code`).
-__device__ bool oz_wait(uint64_t *b, uint32_t parity, volatile int *abort_flag, int *err, int code) {
+__device__ bool oz_wait(uint64_t *b, uint32_t parity, volatile int *abort_flag, int *err, int code, unsigned long long wait_ns) {
     if (mbar_try_wait(b, parity)) return true;
     const unsigned long long t0 = oz_ns();
     while (!mbar_try_wait(b, parity)) {
         if (*abort_flag) return false;
-        if (oz_ns() - t0 > OZ_WAIT_NS) {
+        if (oz_ns() - t0 > wait_ns) {
             *abort_flag = 1;
             atomicCAS(err, 0, code);
             return false;
         }
     }
     return true;
-}
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)), "l"(src),
-                 "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
 }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -142,6 +118,7 @@ struct OzArgs {
     int skip; // rows below skip are not written (their block is updated elsewhere)
     long tiles;
     int *err;
+    unsigned long long wait_ns; // budget of one mbarrier wait
 };
 
 // Tiles of the lower triangle, row-block major: row block I (128 rows) has
@@ -206,10 +183,10 @@ __device__ __forceinline__ void oz_issue_tile_rt(int ns, uint32_t dbuf, uint64_t
 // A wait that ignores the abort flag (still bounded): used on the way out,
 // where copies and MMAs already issued must finish before the CTA releases
 // its shared and tensor memory.
-__device__ void oz_wait_out(uint64_t *b, uint32_t parity, int *err) {
+__device__ void oz_wait_out(uint64_t *b, uint32_t parity, int *err, unsigned long long wait_ns) {
     const unsigned long long t0 = oz_ns();
     while (!mbar_try_wait(b, parity)) {
-        if (oz_ns() - t0 > OZ_WAIT_NS) {
+        if (oz_ns() - t0 > wait_ns) {
             atomicCAS(err, 0, 5);
             return;
         }
@@ -252,23 +229,23 @@ __device__ void oz_producer(const OzArgs &a, OzShared &S, uint8_t *smA, uint8_t 
         if (I != curA) {
             // every MMA of the previous tile reads A
             if (n > 0) {
-                ok = oz_wait(&S.bfree[(n - 1) % OZ_STAGES], (uint32_t)(((n - 1) / OZ_STAGES) & 1), abort_flag, a.err, 1);
+                ok = oz_wait(&S.bfree[(n - 1) % OZ_STAGES], (uint32_t)(((n - 1) / OZ_STAGES) & 1), abort_flag, a.err, 1, a.wait_ns);
                 if (!ok) break;
             }
             mbar_expect_tx(&S.barA, (uint32_t)(ns * OZ_A_BYTES));
             for (int s = 0; s < ns; ++s)
                 bulk_g2s(smA + (size_t)s * OZ_A_BYTES, a.slices + s * a.slice_stride + (long)I * OZ_A_BYTES, OZ_A_BYTES, &S.barA);
             pendA = true;
-            ok = oz_wait(&S.barA, phA, abort_flag, a.err, 2);
+            ok = oz_wait(&S.barA, phA, abort_flag, a.err, 2, a.wait_ns);
             if (!ok) break;
             phA ^= 1u;
             pendA = false;
             curA = I;
         }
-        ok = oz_wait(&S.barB[st], (uint32_t)((n / OZ_STAGES) & 1), abort_flag, a.err, 3);
+        ok = oz_wait(&S.barB[st], (uint32_t)((n / OZ_STAGES) & 1), abort_flag, a.err, 3, a.wait_ns);
         if (!ok) break;
         nb = n + 1;
-        ok = oz_wait(&S.tempty[b], (uint32_t)(((n >> 1) & 1) ^ 1), abort_flag, a.err, 4);
+        ok = oz_wait(&S.tempty[b], (uint32_t)(((n >> 1) & 1) ^ 1), abort_flag, a.err, 4, a.wait_ns);
         if (!ok) break;
         tc_fence_after();
         const uint64_t descB = descB0 + (uint64_t)(((size_t)st * OZ_TILE_B) >> 4);
@@ -284,7 +261,7 @@ __device__ void oz_producer(const OzArgs &a, OzShared &S, uint8_t *smA, uint8_t 
         if (np < ntile) {
             const int sp = (int)(np % OZ_STAGES);
             if (np >= OZ_STAGES) {
-                ok = oz_wait(&S.bfree[sp], (uint32_t)(((np - OZ_STAGES) / OZ_STAGES) & 1), abort_flag, a.err, 1);
+                ok = oz_wait(&S.bfree[sp], (uint32_t)(((np - OZ_STAGES) / OZ_STAGES) & 1), abort_flag, a.err, 1, a.wait_ns);
                 if (!ok) break;
             }
             load_B(Jp, sp);
@@ -295,11 +272,11 @@ __device__ void oz_producer(const OzArgs &a, OzShared &S, uint8_t *smA, uint8_t 
     }
     // On the way out every issued copy lands and every issued MMA completes
     // (bounded waits) before the CTA frees its memory.
-    if (pendA) oz_wait_out(&S.barA, phA, a.err);
-    for (long k = nb; k < np; ++k) oz_wait_out(&S.barB[k % OZ_STAGES], (uint32_t)((k / OZ_STAGES) & 1), a.err);
+    if (pendA) oz_wait_out(&S.barA, phA, a.err, a.wait_ns);
+    for (long k = nb; k < np; ++k) oz_wait_out(&S.barB[k % OZ_STAGES], (uint32_t)((k / OZ_STAGES) & 1), a.err, a.wait_ns);
     if (issued) {
         tc_commit(&S.fin);
-        oz_wait_out(&S.fin, 0, a.err);
+        oz_wait_out(&S.fin, 0, a.err, a.wait_ns);
     }
 }
 
@@ -373,7 +350,7 @@ __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_e
     // are warp-collective)
     auto wait_full = [&](int b, uint32_t parity) {
         int okw = 1;
-        if (lane == 0) okw = oz_wait(&S.tfull[b], parity, abort_flag, a.err, 6) ? 1 : 0;
+        if (lane == 0) okw = oz_wait(&S.tfull[b], parity, abort_flag, a.err, 6, a.wait_ns) ? 1 : 0;
         return __shfl_sync(0xffffffffu, okw, 0) != 0;
     };
     for (long n = 0; n < t_end - t_begin; ++n) {
@@ -545,6 +522,7 @@ void ozaki_syrk_sub_lower(cudaStream_t st, const dd_t *P, long ldp, int n, int k
     a.nJ = (int)ceil_div(n, OZ_COLS_B);
     a.skip = skip;
     a.err = w.err;
+    a.wait_ns = w.wait_ns;
     long tiles = 0;
     for (int I = 0; I < a.nI; ++I) tiles += std::min((long)(OZ_ROWS_A / OZ_COLS_B) * (I + 1), (long)a.nJ);
     a.tiles = tiles;

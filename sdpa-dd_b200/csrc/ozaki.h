@@ -22,6 +22,7 @@ struct OzakiWork {
     cudaEvent_t wait_ev = nullptr; // blocking-sync event to wait on (or null: stream sync)
     int row_cap = 0;
     int slices_used = 16;     // 7-bit slices per value (8..16)
+    unsigned long long wait_ns = 2000000000ull; // budget of one mbarrier wait
     // the Cholesky's lookahead: the next diagonal block is factored on
     // `side` while the trailing update runs (ev_pre: its block is ready;
     // ev_diag: it is factored)

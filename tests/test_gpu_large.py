@@ -12,9 +12,10 @@
   max(1e-24, 10 x the reference runs' spread).
 * The Schur matrix of the headline workload (theta-shaped, 200 vertices,
   m = 9980, 1.6 GB) at an interior point, bit for bit against the
-  reference's Make_bMat (oracle/_ref, run in the test process), and its
+  reference's Make_bMat (oracle/_ref, run in the test process), its
   Cholesky factor in the split form within 1e-27 of the largest entry of
-  the plain dd factor.
+  the plain dd factor, and B^-1 g through the split factor's blocked solves
+  within 1e-20 (relative) of the plain factor's Rtrsv solves.
 """
 import ctypes
 import importlib.util
@@ -150,11 +151,20 @@ def test_theta_m9980_split_factor_close_to_plain(theta_m9980):
         c.call("sddd_schur_build")
         B = torch.from_numpy(c.get("B").view(np.float64)).cuda()
         B2 = B.clone()
-        assert c.L.sddd_Rpotrf(c.h, m, ctypes.c_void_p(B.data_ptr()), m) == 0
+        g = torch.randn(m, 2, dtype=torch.float64, device="cuda", generator=torch.Generator(device="cuda").manual_seed(3))
+        g[:, 1] = 0.0
+        xp, xs = g.clone(), g.clone()
+        assert c.L.sddd_Rpotrf(c.h, b"L", m, ctypes.c_void_p(B.data_ptr()), m) == 0
+        assert c.L.sddd_Rpotrs(c.h, b"L", m, 1, ctypes.c_void_p(B.data_ptr()), m, ctypes.c_void_p(xp.data_ptr()), m) == 0
         assert c.L.sddd_set_tc_split(c.h, 16) == 0
-        assert c.L.sddd_Rpotrf(c.h, m, ctypes.c_void_p(B2.data_ptr()), m) == 0
+        assert c.L.sddd_Rpotrf(c.h, b"L", m, ctypes.c_void_p(B2.data_ptr()), m) == 0
+        # blocked solves: 156 blocks of 64, more than one per co-resident CTA
+        assert c.L.sddd_Rpotrs(c.h, b"L", m, 1, ctypes.c_void_p(B2.data_ptr()), m, ctypes.c_void_p(xs.data_ptr()), m) == 0
         c.L.sddd_set_tc_split(c.h, 0)
         torch.cuda.synchronize()
+        ex = (((xs[:, 0] - xp[:, 0]) + (xs[:, 1] - xp[:, 1])).abs().max() / xp[:, 0].abs().max()).item()
+        print(f"theta m=9980: split factor + blocked solve within {ex:.1e} of the plain factor + Rtrsv solve")
+        assert ex <= 1e-20, ex
         # lower triangles, hi + lo as one float64 difference (the values
         # agree to far more than 2^-53 of the largest entry)
         Lp = B.view(m, m, 2)  # [column][row] (column-major)

@@ -19,6 +19,10 @@ import numpy as np
 import pytest
 
 from conftest import DD, RefSolver, as_dd, load_pkg, ptr
+
+
+def sddd_dd(hi, lo):
+    return load_pkg().SdddDD(hi, lo)
 from test_oracle import adversarial, rand_dd, same, spd
 
 pytestmark = pytest.mark.gpu
@@ -91,21 +95,44 @@ def ctx(sddd):
 
 
 @pytest.mark.parametrize("m,n,k", [(1, 1, 1), (7, 5, 3), (65, 33, 17), (130, 70, 129)])
-@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T")])
-def test_device_gemm_matches_rgemm(ctx, oracle_lib, m, n, k, ta, tb):
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T"), ("T", "T")])
+@pytest.mark.parametrize("ab", ["one_zero", "random", "zero_alpha", "one_beta"])
+def test_device_gemm_matches_rgemm(ctx, ref_lib, m, n, k, ta, tb, ab):
+    """sddd_Rgemm (MPLAPACK's argument list) against the reference's own
+    Rgemm (oracle/_ref), alpha and beta included, bit for bit."""
     import torch
     rng = np.random.default_rng(m + 7 * n + 13 * k)
     ra, ca = (m, k) if ta == "N" else (k, m)
     rb, cb = (k, n) if tb == "N" else (n, k)
-    A, B = rand_dd(rng, ra * ca), rand_dd(rng, rb * cb)
-    dA, dB = to_dev(A), to_dev(B)
-    dC = torch.zeros(2 * m * n, dtype=torch.float64, device="cuda")
-    ctx.L.sddd_Rgemm(ctx.h, ta.encode(), tb.encode(), m, n, k, ctypes.c_void_p(dA.data_ptr()), ra, ctypes.c_void_p(dB.data_ptr()), rb,
-                     ctypes.c_void_p(dC.data_ptr()), m)
-    want = np.zeros(m * n, DD)
-    oracle_lib.o_gemm(ctypes.c_char(ta.encode()), ctypes.c_char(tb.encode()), ctypes.c_long(m), ctypes.c_long(n), ctypes.c_long(k), ptr(A),
-                      ctypes.c_long(ra), ptr(B), ctypes.c_long(rb), ptr(want), ctypes.c_long(m))
+    A, B, C = rand_dd(rng, ra * ca), rand_dd(rng, rb * cb), rand_dd(rng, m * n)
+    alpha, beta = {"one_zero": ((1.0, 0.0), (0.0, 0.0)), "zero_alpha": ((0.0, 0.0), (0.75, 0.0)), "one_beta": ((-2.5, 1e-17), (1.0, 0.0)),
+                   "random": ((rng.standard_normal(), 3e-18), (rng.standard_normal(), -2e-18))}[ab]
+    dA, dB, dC = to_dev(A), to_dev(B), to_dev(C)
+    rc = ctx.L.sddd_Rgemm(ctx.h, ta.encode(), tb.encode(), m, n, k, sddd_dd(*alpha), ctypes.c_void_p(dA.data_ptr()), ra,
+                          ctypes.c_void_p(dB.data_ptr()), rb, sddd_dd(*beta), ctypes.c_void_p(dC.data_ptr()), m)
+    assert rc == 0, ctx.L.sddd_last_error(ctx.h)
+    want = C.copy()
+    al, be = np.array([alpha], DD), np.array([beta], DD)
+    ref_lib.ref_Rgemm(ta.encode(), tb.encode(), ctypes.c_long(m), ctypes.c_long(n), ctypes.c_long(k), ptr(al), ptr(A), ctypes.c_long(ra), ptr(B),
+                      ctypes.c_long(rb), ptr(be), ptr(want), ctypes.c_long(m))
     assert same(from_dev(dC, m * n), want)
+
+
+def test_dd_blas_argument_checks(ctx):
+    """Bad arguments are reported with the position the reference's
+    Mxerbla_dd names; forms SDPA never calls are refused, not guessed."""
+    one = sddd_dd(1.0, 0.0)
+    assert ctx.L.sddd_Rgemm(ctx.h, b"X", b"N", 2, 2, 2, one, None, 2, None, 2, one, None, 2) == -1
+    assert b"parameter 1" in ctx.L.sddd_last_error(ctx.h)
+    assert ctx.L.sddd_Rgemm(ctx.h, b"N", b"N", 4, 2, 2, one, None, 3, None, 2, one, None, 4) == -1
+    assert b"parameter 8" in ctx.L.sddd_last_error(ctx.h)
+    assert ctx.L.sddd_Rtrsv(ctx.h, b"L", b"N", b"N", 3, None, 3, None, 0) == -1
+    assert b"parameter 8" in ctx.L.sddd_last_error(ctx.h)
+    assert ctx.L.sddd_Rtrsv(ctx.h, b"U", b"N", b"N", 3, None, 3, None, 1) == -7
+    assert ctx.L.sddd_Rpotrf(ctx.h, b"Q", 3, None, 3) == -1
+    assert ctx.L.sddd_Rpotrf(ctx.h, b"U", 3, None, 3) == -7
+    assert ctx.L.sddd_Rpotrs(ctx.h, b"L", 3, 1, None, 2, None, 3) == -1
+    assert b"parameter 5" in ctx.L.sddd_last_error(ctx.h)
 
 
 @pytest.mark.parametrize("n", [1, 5, 63, 64, 65, 130, 257])
@@ -117,7 +144,7 @@ def test_device_potrf_trsv_match(ctx, oracle_lib, n):
     info = oracle_lib.o_potrf(ctypes.c_long(n), ptr(want), ctypes.c_long(n))
     assert info == 0
     dA = to_dev(A)
-    got_info = ctx.L.sddd_Rpotrf(ctx.h, n, ctypes.c_void_p(dA.data_ptr()), n)
+    got_info = ctx.L.sddd_Rpotrf(ctx.h, b"L", n, ctypes.c_void_p(dA.data_ptr()), n)
     assert got_info == 0
     got = from_dev(dA, n * n).reshape(n, n)
     w = want.reshape(n, n)
@@ -129,7 +156,7 @@ def test_device_potrf_trsv_match(ctx, oracle_lib, n):
         x = b.copy()
         oracle_lib.o_trsv(ctypes.c_char(tr.encode()), ctypes.c_long(n), ptr(want), ctypes.c_long(n), ptr(x))
         dx = to_dev(b)
-        ctx.L.sddd_Rtrsv(ctx.h, tr.encode(), n, ctypes.c_void_p(dA.data_ptr()), n, ctypes.c_void_p(dx.data_ptr()))
+        ctx.L.sddd_Rtrsv(ctx.h, b"L", tr.encode(), b"N", n, ctypes.c_void_p(dA.data_ptr()), n, ctypes.c_void_p(dx.data_ptr()), 1)
         assert same(from_dev(dx, n), x), tr
 
 
@@ -152,7 +179,7 @@ def test_device_trsv_wavefront_matches_rtrsv(ctx, oracle_lib, n, lda):
         x = b.copy()
         oracle_lib.o_trsv(ctypes.c_char(tr.encode()), ctypes.c_long(n), ptr(L), ctypes.c_long(lda), ptr(x))
         dx = to_dev(b)
-        assert ctx.L.sddd_Rtrsv(ctx.h, tr.encode(), n, ctypes.c_void_p(dL.data_ptr()), lda, ctypes.c_void_p(dx.data_ptr())) == 0
+        assert ctx.L.sddd_Rtrsv(ctx.h, b"L", tr.encode(), b"N", n, ctypes.c_void_p(dL.data_ptr()), lda, ctypes.c_void_p(dx.data_ptr()), 1) == 0
         assert same(from_dev(dx, n), x), tr
 
 
@@ -164,7 +191,7 @@ def test_device_potrf_reports_failing_column(ctx, oracle_lib):
     want = A.copy()
     i1 = oracle_lib.o_potrf(ctypes.c_long(n), ptr(want), ctypes.c_long(n))
     dA = to_dev(A)
-    i2 = ctx.L.sddd_Rpotrf(ctx.h, n, ctypes.c_void_p(dA.data_ptr()), n)
+    i2 = ctx.L.sddd_Rpotrf(ctx.h, b"L", n, ctypes.c_void_p(dA.data_ptr()), n)
     assert i1 == i2 == 98
 
 

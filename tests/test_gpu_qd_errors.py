@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 from conftest import DD, load_pkg, ptr
+from test_oracle import same
 
 pytestmark = pytest.mark.gpu
 
@@ -94,23 +95,33 @@ def test_cholesky_and_solve_errors_against_qd(ref_lib, cond):
         for slices in (0, 16, 12):
             assert c.L.sddd_set_tc_split(c.h, slices) == 0
             dA, dx = to_dev(A), to_dev(g)
-            assert c.L.sddd_Rpotrf(c.h, n, ctypes.c_void_p(dA.data_ptr()), n) == 0
-            assert c.L.sddd_Rtrsv(c.h, b"N", n, ctypes.c_void_p(dA.data_ptr()), n, ctypes.c_void_p(dx.data_ptr())) == 0
-            assert c.L.sddd_Rtrsv(c.h, b"T", n, ctypes.c_void_p(dA.data_ptr()), n, ctypes.c_void_p(dx.data_ptr())) == 0
+            assert c.L.sddd_Rpotrf(c.h, b"L", n, ctypes.c_void_p(dA.data_ptr()), n) == 0
+            assert c.L.sddd_Rtrsv(c.h, b"L", b"N", b"N", n, ctypes.c_void_p(dA.data_ptr()), n, ctypes.c_void_p(dx.data_ptr()), 1) == 0
+            assert c.L.sddd_Rtrsv(c.h, b"L", b"T", b"N", n, ctypes.c_void_p(dA.data_ptr()), n, ctypes.c_void_p(dx.data_ptr()), 1) == 0
+            # the same factor through sddd_Rpotrs: the two Rtrsv with the
+            # split off, the blocked solves (inverted diagonal blocks) on
+            dxp = to_dev(g)
+            assert c.L.sddd_Rpotrs(c.h, b"L", n, 1, ctypes.c_void_p(dA.data_ptr()), n, ctypes.c_void_p(dxp.data_ptr()), n) == 0
             L = from_dev(dA, n * n)
             x = from_dev(dx, n)
+            xp = from_dev(dxp, n)
+            if slices == 0:
+                assert same(xp, x)
             eL = maxdiff(ref_lib, L, Lq, lower=1, order=n)
             ex = maxdiff(ref_lib, x, xq)
-            rows.append((slices, eL, ex))
+            exp_ = maxdiff(ref_lib, xp, xq)
+            rows.append((slices, eL, ex, exp_))
         c.L.sddd_set_tc_split(c.h, 0)
-    for slices, eL, ex in rows:
+    for slices, eL, ex, exp_ in rows:
         form = "plain dd" if slices == 0 else f"split, {slices} slices"
-        print(f"cond {cond:.0e} order {n}, {form}: factor {eL:.2e}, solve {ex:.2e}")
+        print(f"cond {cond:.0e} order {n}, {form}: factor {eL:.2e}, solve {ex:.2e}, Rpotrs {exp_:.2e}")
     # factor: a backward-stable dd Cholesky is off by ~eps_dd * cond^(1/2)
     # relative (eps_dd = 2^-104 ~ 5e-32); the solve by ~eps_dd * cond
     eps = 2.0 ** -104
     plain, s16, s12 = rows
     assert plain[1] < 100 * eps * np.sqrt(cond) and plain[2] < 100 * eps * cond
     assert s16[1] < 100 * eps * np.sqrt(cond) and s16[2] < 100 * eps * cond
+    # the blocked solve of the split form: as accurate as the substitution
+    assert s16[3] < 100 * eps * cond
     # 12 slices carry 85 bits: its factor is off by ~2^-84 relative
     assert s12[1] < 100 * 2.0 ** -84 * np.sqrt(cond)

@@ -122,10 +122,10 @@ def test_potrf_tc_matches_plain(ctx, n):
     A = _spd(rng, n)
     dA1, dA2 = to_dev(A), to_dev(A)
     assert ctx.L.sddd_set_tc_split(ctx.h, 0) == 0
-    assert ctx.L.sddd_Rpotrf(ctx.h, n, ctypes.c_void_p(dA1.data_ptr()), n) == 0
+    assert ctx.L.sddd_Rpotrf(ctx.h, b"L", n, ctypes.c_void_p(dA1.data_ptr()), n) == 0
     assert ctx.L.sddd_set_tc_split(ctx.h, 16) == 0
     try:
-        info = ctx.L.sddd_Rpotrf(ctx.h, n, ctypes.c_void_p(dA2.data_ptr()), n)
+        info = ctx.L.sddd_Rpotrf(ctx.h, b"L", n, ctypes.c_void_p(dA2.data_ptr()), n)
     finally:
         ctx.L.sddd_set_tc_split(ctx.h, 0)
     assert info == 0
@@ -144,10 +144,10 @@ def test_potrf_tc_reports_failing_column(ctx):
     A = _spd(rng, n)
     A["hi"][200 * n + 200] = -5.0
     dA1, dA2 = to_dev(A), to_dev(A)
-    i1 = ctx.L.sddd_Rpotrf(ctx.h, n, ctypes.c_void_p(dA1.data_ptr()), n)
+    i1 = ctx.L.sddd_Rpotrf(ctx.h, b"L", n, ctypes.c_void_p(dA1.data_ptr()), n)
     ctx.L.sddd_set_tc_split(ctx.h, 16)
     try:
-        i2 = ctx.L.sddd_Rpotrf(ctx.h, n, ctypes.c_void_p(dA2.data_ptr()), n)
+        i2 = ctx.L.sddd_Rpotrf(ctx.h, b"L", n, ctypes.c_void_p(dA2.data_ptr()), n)
     finally:
         ctx.L.sddd_set_tc_split(ctx.h, 0)
     assert i1 == i2 == 201
