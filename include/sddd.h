@@ -278,6 +278,15 @@ int sddd_set_wait_limit(sddd_ctx *ctx, double seconds);
  * wait for it runs out.  Not for production use. */
 int sddd_test_withhold_block(sddd_ctx *ctx, int block);
 
+/* C(i,j) = sum_k W(i,k) V(j,k) for i >= j (device pointers; W and V n x k
+ * with row i at W + i * ldw, the k values contiguous; C column-major, only
+ * its lower triangle written) through the split products: each row scaled
+ * once over all k and cut into `slices` signed 7-bit slices, every diagonal
+ * of slice products summed exactly in int32 on the tensor cores (k <= 32767),
+ * rebuilt in dd.  The Schur complement's F1 pair products in the split form
+ * (no counterpart in the reference). */
+int sddd_Rdot_pairs_tc(sddd_ctx *ctx, long n, long k, const sddd_dd *W, long ldw, const sddd_dd *V, long ldv, sddd_dd *C, long ldc, int slices);
+
 /* -- dd kernels on device memory: the MPLAPACK seam --
  * The argument lists of MPLAPACK's dd routines (mplapack/mpblas_dd.h:47,54,
  * mplapack/mplapack_dd.h:41) with the context first; pointers are device

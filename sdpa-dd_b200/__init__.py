@@ -93,6 +93,7 @@ def lib() -> ctypes.CDLL:
         "sddd_test_withhold_block": (ci, [vp, ci]),
         "sddd_get_tc_split": (ci, [vp]),
         "sddd_Rsyrk_tc": (ci, [vp, cl, cl, vp, cl, vp, cl, ci]),
+        "sddd_Rdot_pairs_tc": (ci, [vp, cl, cl, vp, cl, vp, cl, vp, cl, ci]),
         "sddd_dd_op": (ci, [vp, ci, cl, vp, vp, vp]),
         "sddd_host_dd_op": (ci, [ci, cl, vp, vp, vp]),
         "sddd_host_dd_read": (ci, [ctypes.c_char_p, vp]),

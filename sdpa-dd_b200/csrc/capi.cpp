@@ -705,6 +705,21 @@ int sddd_Rsyrk_tc(sddd_ctx *ctx, long n, long k, const sddd_dd *P, long ldp, sdd
     });
 }
 
+int sddd_Rdot_pairs_tc(sddd_ctx *ctx, long n, long k, const sddd_dd *W, long ldw, const sddd_dd *V, long ldv, sddd_dd *C, long ldc, int slices) {
+    return guarded(ctx, [&] {
+        if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
+        if (n < 0 || k < 1 || k > sddd::OG_MAX_K || ldw < k || ldv < k || ldc < std::max(1L, n) || slices < 8 || slices > sddd::OZ_MAX_SLICES)
+            throw sddd::Error(SDDD_ERR_ARG, "sddd_Rdot_pairs_tc: need 1 <= k <= 32767, ldw, ldv >= k, ldc >= n and 8 <= slices <= 16");
+        if (n == 0) return SDDD_OK;
+        sddd::Context &c = *ctx->c;
+        sddd::OzakiGemmWork &w = sddd::tcg_work(c, (int)n, k, slices);
+        sddd::ozaki_gemm_lower(c.stream, reinterpret_cast<const dd_t *>(W), ldw, reinterpret_cast<const dd_t *>(V), ldv, (int)n, k,
+                               reinterpret_cast<dd_t *>(C), ldc, w);
+        sddd::ozaki_gemm_check(c.stream, w);
+        return SDDD_OK;
+    });
+}
+
 int sddd_Rtrsv(sddd_ctx *ctx, char uplo, char trans, char diag, long n, const sddd_dd *A, long lda, sddd_dd *x, long incx) {
     return guarded(ctx, [&] {
         if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");

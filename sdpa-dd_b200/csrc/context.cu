@@ -105,6 +105,34 @@ OzakiWork &tc_work(Context &c, int n, int slices) {
     return c.tc;
 }
 
+OzakiGemmWork &tcg_work(Context &c, int n, long K, int slices) {
+    const size_t bytes = ozaki_gemm_slice_bytes(n, K, slices);
+    const int rows = (int)(ceil_div(n, 128) * 128);
+    if (bytes > c.tcg.slice_bytes || rows > c.tcg.rows_cap || !c.tcg.err) {
+        CK(cudaStreamSynchronize(c.stream));
+        c.tcg_sw.alloc(bytes);
+        c.tcg_sv.alloc(bytes);
+        c.tcg_ew.alloc((size_t)rows);
+        c.tcg_ev.alloc((size_t)rows);
+        if (!c.tcg_err.p) {
+            c.tcg_err.alloc(1);
+            CK(cudaMemsetAsync(c.tcg_err.p, 0, sizeof(int), c.stream));
+        }
+        c.tcg.sw = c.tcg_sw.p;
+        c.tcg.sv = c.tcg_sv.p;
+        c.tcg.slice_bytes = std::max(bytes, c.tcg.slice_bytes);
+        c.tcg.ew = c.tcg_ew.p;
+        c.tcg.ev = c.tcg_ev.p;
+        c.tcg.rows_cap = std::max(rows, c.tcg.rows_cap);
+        c.tcg.err = c.tcg_err.p;
+        c.tcg.h_err = static_cast<int *>(c.h_pin);
+        c.tcg.wait_ev = c.sync_ev;
+    }
+    c.tcg.slices = slices;
+    c.tcg.wait_ns = c.wait_ns;
+    return c.tcg;
+}
+
 TrsvSync &trsv_sync(Context &c, int n) {
     const int nblk = (int)ceil_div(n, 64);
     if (nblk > c.trsv.capacity || !c.trsv.flags) {

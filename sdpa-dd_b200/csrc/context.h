@@ -188,6 +188,12 @@ struct Context {
     DBuf<int8_t> tc_slice_buf;
     DBuf<int> tc_exps, tc_err;
     OzakiWork tc;
+    // the split of the Schur complement's F1 pair products (W^T V over K =
+    // n^2): slices, row exponents, error word, and the pair values
+    DBuf<int8_t> tcg_sw, tcg_sv;
+    DBuf<int> tcg_ew, tcg_ev, tcg_err;
+    DBuf<dd_t> tcg_pairs;
+    OzakiGemmWork tcg;
     // a user-given initial point (the reference's -id / -is), used by the
     // solver's start in place of lambda I
     bool has_init = false;
@@ -219,6 +225,9 @@ TrsvSync &trsv_sync(Context &c, int n);
 // The split workspace for an order-n factorisation with `slices` slices
 // (grown as needed).
 OzakiWork &tc_work(Context &c, int n, int slices);
+// The split workspace for an n x n pair product over K values (grown as
+// needed).
+OzakiGemmWork &tcg_work(Context &c, int n, long K, int slices);
 
 // Marks the context as one of many sharing the GPU (a batch worker): short
 // triangular solves in one CTA; with blocking_waits, host waits block on an

@@ -39,4 +39,30 @@ void ozaki_syrk_sub_lower(cudaStream_t st, const dd_t *P, long ldp, int n, int k
 // Throws when a launch since the last check gave up waiting (synchronises st).
 void ozaki_check(cudaStream_t st, const OzakiWork &w);
 
+// The split of a long product C(i,j) = sum_k W(i,k) V(j,k), i >= j (the
+// Schur complement's F1 pair products): W and V n x K, row r at
+// W + r * ldw (K contiguous dd); C n x n column-major, lower triangle
+// stored.  K <= OG_MAX_K (every diagonal of slice products accumulates
+// exactly in int32 over the whole K).
+constexpr long OG_MAX_K = 32767;
+struct OzakiGemmWork {
+    int8_t *sw = nullptr, *sv = nullptr; // slices of W and V
+    size_t slice_bytes = 0;              // bytes of each slice buffer
+    int *ew = nullptr, *ev = nullptr;    // row exponents (rows_cap each)
+    int rows_cap = 0;
+    int *err = nullptr;
+    int *h_err = nullptr;
+    cudaEvent_t wait_ev = nullptr;
+    int slices = 16;
+    unsigned long long wait_ns = 2000000000ull;
+};
+// Workspace bytes of one slice buffer for n rows, K values and S slices.
+inline size_t ozaki_gemm_slice_bytes(int n, long K, int slices) {
+    const long rows = (long)((n + 127) / 128) * 128, kpad = (K + 63) / 64 * 64;
+    return (size_t)slices * rows * kpad;
+}
+void ozaki_gemm_lower(cudaStream_t st, const dd_t *W, long ldw, const dd_t *V, long ldv, int n, long K, dd_t *C, long ldc, OzakiGemmWork &w);
+// Throws when a launch since the last check gave up waiting (synchronises st).
+void ozaki_gemm_check(cudaStream_t st, const OzakiGemmWork &w);
+
 } // namespace sddd

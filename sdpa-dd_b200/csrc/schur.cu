@@ -19,6 +19,7 @@
 //   - sparse partners of F1/F2 owners and all F3 pairs: one thread (F1, F3)
 //     or one warp (F2) per pair.
 #include "context.h"
+#include "ozaki.h"
 #include "blas.h"
 #include "newton.h"
 #include "devops.cuh"
@@ -193,6 +194,18 @@ __global__ void schur_f2_sparse_kernel(BlockView bv, const int *ownFG, int nfg, 
     }
 }
 
+// --------------------------------- dense partners from the split products
+// pairs[r + nfg d] = G_r . A_d (d <= r) of a block whose constraints are all
+// dense F1/F2 owners (sorted position = owner index = dense index): added to
+// B(i,j) and B(j,i) as the reference adds each pair's value.
+__global__ void schur_scatter_pairs_kernel(BlockView bv, int nfg, const dd_t *pairs, dd_t *B, int m) {
+    const int r = blockIdx.y;
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d > r) return;
+    const int i = bv.con[bv.perm[r]], j = bv.con[bv.perm[d]];
+    b_add(B, m, i, j, ld_dd(pairs + r + (long)nfg * d));
+}
+
 // ----------------------------------------------------------- F3 owners
 // calF3 (sdpa_newton.cpp:937-977), one thread per pair.
 __global__ void schur_f3_kernel(BlockView bv, const int *ownF3, int nf3, const dd_t *X, const dd_t *invZ, dd_t *B, int m) {
@@ -265,7 +278,18 @@ void schur_build(Context &c) {
             gemm(st, 'N', 'N', GEMM_STORE, n, n, n, X, n, 0, c.Fbuf.p, n, nn, c.Gbuf.p, n, nn, nfg, false);
             // dense partners
             const int ndense = bd.nc - bd.nsparse;
-            if (ndense > 0) {
+            if (c.tc_slices > 0 && bd.nsparse == 0 && nfg == bd.nc && bd.fg_dense_contig && nn <= OG_MAX_K) {
+                // every pair of the block is one n^2-term product G_r . A_d:
+                // the INT8 tensor-core split of W^T V, W = [vec G_r],
+                // V = [vec A_d], then the pairs into B
+                OzakiGemmWork &w = tcg_work(c, nfg, nn, c.tc_slices);
+                c.tcg_pairs.alloc((size_t)nfg * nfg);
+                const long o0 = bd.h_dense_off[bd.h_perm[0]];
+                ozaki_gemm_lower(st, c.Gbuf.p, nn, bd.dense.p + o0, nn, nfg, nn, c.tcg_pairs.p, nfg, w);
+                dim3 grid(ceil_div(nfg, 128), nfg);
+                schur_scatter_pairs_kernel<<<grid, 128, 0, st>>>(bv, nfg, c.tcg_pairs.p, c.B.p, m);
+                CK_LAUNCH();
+            } else if (ndense > 0) {
                 // Every pair is one sequential dot over the n^2 entries.  With
                 // few pairs (small m) 64 x 64 tiles of 16 pairs per thread
                 // leave the GPU nearly idle on long chains; one pair per
@@ -300,6 +324,7 @@ void schur_build(Context &c) {
             CK_LAUNCH();
         }
     }
+    if (c.tcg.err) ozaki_gemm_check(st, c.tcg);
 }
 
 } // namespace sddd

@@ -108,6 +108,91 @@ def test_syrk_tc_matches_exact(ctx, n, k, ldc, slices):
         assert np.array_equal(got[:, n:].view(np.float64), C0.reshape(n, ldc)[:, n:].view(np.float64))
 
 
+@pytest.mark.parametrize("n,k,slices", [(1, 1, 16), (33, 700, 16), (150, 100, 16), (5, 32767, 16), (70, 333, 12)])
+def test_dot_pairs_tc_matches_exact(ctx, n, k, slices):
+    """sddd_Rdot_pairs_tc (the Schur complement's F1 pair products) against
+    exact integer arithmetic: rows of W scaled over several binades, a zero
+    row, tiny entries; the bound is the split's truncation (7S+1 bits of each
+    row's scale, k terms) plus the dd rebuild."""
+    rng = np.random.default_rng(2000 + n + k + slices)
+    W = np.zeros((n, k), DD)
+    W["hi"] = rng.standard_normal((n, k)) * np.exp2(rng.integers(-6, 7, (n, 1)))
+    W["lo"] = W["hi"] * rng.uniform(-1, 1, (n, k)) * 1e-17
+    V = np.zeros((n, k), DD)
+    V["hi"] = rng.standard_normal((n, k))
+    V["lo"] = V["hi"] * rng.uniform(-1, 1, (n, k)) * 1e-17
+    if n > 3:
+        W[2, :] = (0.0, 0.0)
+        W[3, : k // 2]["hi"] *= 2.0 ** -20
+        W[3, : k // 2]["lo"] *= 2.0 ** -20
+    C = np.zeros((n, n), DD)  # [j, i]: column-major
+    C["hi"] = 7.0  # entries above the diagonal stay untouched
+    dW, dV, dC = to_dev(W.ravel()), to_dev(V.ravel()), to_dev(C.ravel())
+    rc = ctx.L.sddd_Rdot_pairs_tc(ctx.h, n, k, ctypes.c_void_p(dW.data_ptr()), k, ctypes.c_void_p(dV.data_ptr()), k, ctypes.c_void_p(dC.data_ptr()),
+                                  n, slices)
+    assert rc == 0, ctx.L.sddd_last_error(ctx.h)
+    got = from_dev(dC, n * n).reshape(n, n)  # [j, i]
+    Wi, Vi = exact_int(W), exact_int(V)
+    prod = Wi.dot(Vi.T)  # [i, j] at scale 2^(2 SCALE)
+    wmax, vmax = np.abs(W["hi"]).max(axis=1), np.abs(V["hi"]).max(axis=1)
+    Gi = exact_int(got.T)  # [i, j]
+    worst = 0.0
+    for i in range(n):
+        for j in range(n):
+            if j > i:
+                assert got[j, i]["hi"] == 7.0 and got[j, i]["lo"] == 0.0, (i, j)
+                continue
+            err = abs((Gi[i, j] << SCALE) - prod[i, j]) / 2.0 ** (2 * SCALE)
+            bound = k * 2.0 ** -(7 * slices - 6) * wmax[i] * vmax[j] + 2.0 ** -104 * abs(float(prod[i, j]) / 2.0 ** (2 * SCALE))
+            assert err <= bound + 1e-300, (i, j, err, bound)
+            if bound > 0:
+                worst = max(worst, err / bound)
+    print(f"n={n} k={k} S={slices}: worst error {worst:.2e} of its bound")
+
+
+def test_schur_tc_error_against_qd(ref_lib):
+    """The Schur matrix of an all-dense block (the F1 pair products on the
+    tensor cores) against the qd_real oracle, beside the plain dd form."""
+    sddd = load_pkg()
+    rng = np.random.default_rng(8)
+    n, m = 40, 90
+    As = rng.standard_normal((m, n, n)) / np.sqrt(n)
+    As = (As + As.transpose(0, 2, 1)) / 2
+    iu, ju = np.triu_indices(n)
+    kk = np.concatenate([np.full(len(iu), q + 1) for q in range(m)])
+    val = np.zeros(len(kk), DD)
+    val["hi"] = np.concatenate([As[q][iu, ju] for q in range(m)])
+    b = np.zeros(m, DD)
+    b["hi"] = rng.standard_normal(m)
+    G = rng.standard_normal((n, n))
+    X = np.zeros(n * n, DD)
+    X["hi"] = (np.eye(n) + G @ G.T / n).T.ravel()
+    H = rng.standard_normal((n, n))
+    Z = np.zeros(n * n, DD)
+    Z["hi"] = (np.eye(n) + H @ H.T / n).T.ravel()
+    out = {}
+    with sddd.Context(0) as c:
+        c.upload(m, [n], b, kk, np.ones_like(kk), np.tile(iu + 1, m), np.tile(ju + 1, m), val)
+        assert c.set_point(X, np.zeros(m, DD), Z) == 0
+        for slices in (0, 16):
+            assert c.L.sddd_set_tc_split(c.h, slices) == 0
+            c.call("sddd_schur_build")
+            out[slices] = c.get("B")
+        Zi = c.get("invZ")
+    Adense = np.zeros(m * n * n, DD)
+    Adense["hi"] = np.concatenate([As[q].T.ravel() for q in range(m)])
+    Bq = np.zeros(4 * m * m)
+    ref_lib.qd_schur_dense(ctypes.c_long(n), ctypes.c_long(m), ptr(Adense), ptr(X), ptr(Zi), ptr(Bq))
+    err = {}
+    for slices, B in out.items():
+        o = np.zeros(2)
+        ref_lib.qd_maxdiff(ctypes.c_long(m * m), ptr(np.ascontiguousarray(B)), ptr(Bq), ctypes.c_int(0), ctypes.c_long(0), ptr(o))
+        err[slices] = o[0] / o[1]
+        print(f"Schur matrix (n={n}, m={m}) vs qd, {'plain dd' if slices == 0 else 'split, 16 slices'}: {err[slices]:.2e}")
+    assert err[0] < 1e-30
+    assert err[16] < 1e-28
+
+
 def _spd(rng, n):
     G = rng.standard_normal((n, n)) / np.sqrt(n)
     A = G @ G.T + np.eye(n)
