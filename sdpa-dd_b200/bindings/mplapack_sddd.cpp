@@ -72,8 +72,14 @@ void fail(const char *routine, int rc) {
     std::abort();
 }
 
+// A copy from pageable memory may still be in flight when cudaMemcpy
+// returns, and the library's kernels run on a non-blocking stream: wait for
+// the device before the call that reads the data.
 void h2d(void *d, const void *h, size_t bytes) {
     if (bytes && cudaMemcpy(d, h, bytes, cudaMemcpyHostToDevice) != cudaSuccess) fail("cudaMemcpy", SDDD_ERR_CUDA);
+}
+void h2d_done() {
+    if (cudaDeviceSynchronize() != cudaSuccess) fail("cudaDeviceSynchronize", SDDD_ERR_CUDA);
 }
 void d2h(void *h, const void *d, size_t bytes) {
     if (bytes && cudaMemcpy(h, d, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) fail("cudaMemcpy", SDDD_ERR_CUDA);
@@ -102,6 +108,7 @@ void Rgemm(const char *transa, const char *transb, mplapackint const m, mplapack
     h2d(da, a, ba);
     h2d(db, b, bb);
     h2d(dc, c, bc);
+    h2d_done();
     const sddd_dd al{alpha.x[0], alpha.x[1]}, be{beta.x[0], beta.x[1]};
     const int rc = sddd_Rgemm(g.ctx, transa ? transa[0] : '?', transb ? transb[0] : '?', m, n, k, al, (const sddd_dd *)da, lda,
                               (const sddd_dd *)db, ldb, be, (sddd_dd *)dc, ldc);
@@ -115,6 +122,7 @@ void Rpotrf(const char *uplo, mplapackint const n, dd_real *a, mplapackint const
     const size_t bytes = extent(lda, n, n);
     void *da = g.a.get(bytes + 16);
     h2d(da, a, bytes);
+    h2d_done();
     const int rc = sddd_Rpotrf(g.ctx, uplo ? uplo[0] : '?', n, (sddd_dd *)da, lda);
     if (rc < 0) fail("Rpotrf", rc);
     d2h(a, da, bytes);
@@ -125,10 +133,11 @@ void Rtrsv(const char *uplo, const char *trans, const char *diag, mplapackint co
            mplapackint const incx) {
     Gpu &g = gpu();
     std::lock_guard<std::mutex> lock(g.mu);
-    const size_t ba = extent(lda, n, n), bx = extent(1, n, 1);
+    const size_t ba = extent(lda, n, n), bx = n > 0 ? sizeof(dd_real) * (size_t)n : 0;
     void *da = g.a.get(ba + 16), *dx = g.b.get(bx + 16);
     h2d(da, a, ba);
     if (incx == 1) h2d(dx, x, bx);
+    h2d_done();
     const int rc = sddd_Rtrsv(g.ctx, uplo ? uplo[0] : '?', trans ? trans[0] : '?', diag ? diag[0] : '?', n, (const sddd_dd *)da, lda, (sddd_dd *)dx,
                               incx);
     if (rc != SDDD_OK) fail("Rtrsv", rc);

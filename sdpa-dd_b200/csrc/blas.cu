@@ -734,6 +734,11 @@ void trsv_check(cudaStream_t st, const TrsvSync &sync) {
         CK(cudaStreamSynchronize(st));
     }
     err = *h;
+    if (err != 0) {
+        // clear the error word, so that the next solve starts afresh
+        CK(cudaMemsetAsync(sync.flags + sync.capacity, 0, sizeof(int), st));
+        CK(cudaStreamSynchronize(st));
+    }
     if (err != 0)
         throw Error(ERR_CUDA, "trsv: a wait ran out of its " + std::to_string(sync.wait_ns / 1000000ull) + " ms budget for block " + std::to_string(err - 1) +
                                   " (solve abandoned)");

@@ -287,47 +287,28 @@ __device__ __forceinline__ void tc_ld2(uint32_t taddr, int32_t *r) {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(taddr));
 }
 
-// Exact x 2^-K as a double for integer |x| < 2^51 (the magic-number
-// conversion): the double M = 1.5 * 2^(52-K) has ulp 2^-K, so its bits plus
-// x are the double M + x 2^-K (the significand holds 2^51 + x), from which
-// M is subtracted exactly.
-template <int K>
-__device__ __forceinline__ double oz_i2d(long long x) {
-    constexpr long long bits = ((long long)(1023 + 52 - K) << 52) | (1LL << 51);
-    return __dsub_rn(__longlong_as_double(x + bits), __longlong_as_double(bits));
-}
-
-// Group g of diagonals (d = 2+4g .. 5+4g) of one entry from its diagonal
-// values v[0..15] (diagonal d at v[d-2]; those beyond S+1 are zero):
-// V = 2^21 A_d + 2^14 A_d+1 + 2^7 A_d+2 + A_d+3, exact (|V| < 2^44; the
-// pairs 2^7 A + A' < 2^30 are exact in int32).  Its value is
-// V 2^-(35 + 28 g) in units of 2^(e_i + e_j).
-__device__ __forceinline__ long long oz_group(const int32_t (*v)[2], int g, int c) {
-    const int32_t p0 = v[4 * g][c] * 128 + v[4 * g + 1][c], p1 = v[4 * g + 2][c] * 128 + v[4 * g + 3][c];
-    return (long long)p0 * 16384 + p1;
-}
-
-// Exact sum of the diagonals of one entry as a dd, from its diagonal
-// values v[0..15] (diagonal d at v[d-2]; those beyond S+1 are zero), in
-// units of 2^(e_i + e_j).  With the groups V_g (oz_group) the value is
-// V0 2^-35 + V1 2^-63 + V2 2^-91 + V3 2^-119.  Groups 2 and 3 fold into an
-// int64 carry in units of 2^-104 (V3 rounded: at most 2^-105, |carry| <
-// 2^58); T = V0 2^69 + V1 2^41 + carry (|T| < 2^109, |V0| < 2^40) is
-// formed exactly as a 128-bit integer H 2^64 + L and cut into
-// t2 2^84 + t1 2^42 + t0 (0 <= t0, t1 < 2^42, |t2| < 2^25), three exact
-// doubles; TwoSum of the top two, the third added to the error (exact but
-// for 2^-106 of the value) and a FastTwoSum give the dd.
+// Sum of the diagonals of one entry as a dd, from its diagonal values
+// v[0..15] (diagonal d at v[d-2]; those beyond S+1 are zero), in units of
+// 2^(e_i + e_j): value = sum_d A_d 2^-7d.  Pairs P_k = 2^7 A_2k+2 + A_2k+3
+// are exact in int32 (|P| < 2^30) and in a double; groups G_j = 2^14 P_2j +
+// P_2j+1 are exact doubles (|G| < 2^44, one FMA each), so value = 2^-35
+// (G0 + G1 2^-28 + G2 2^-56 + G3 2^-84).  Two TwoSums leave only the
+// rounding of the two smallest parts' sum and of the final low part:
+// within 2^-106 of the value plus 2^-140 absolute.
 __device__ __forceinline__ void oz_entry_dd(const int32_t (*v)[2], int c, double &hi, double &lo) {
-    const long long V0 = oz_group(v, 0, c), V1 = oz_group(v, 1, c);
-    const long long carry = oz_group(v, 2, c) * 8192 + ((oz_group(v, 3, c) + 16384) >> 15);
-    const unsigned long long l1 = (unsigned long long)V1 << 41, L = l1 + (unsigned long long)carry;
-    const long long H = V0 * 32 + (V1 >> 23) + (carry >> 63) + (L < l1 ? 1 : 0);
-    const long long t0 = (long long)(L & 0x3FFFFFFFFFFULL);
-    const long long t1 = (long long)((L >> 42) | ((unsigned long long)(H & 0xFFFFF) << 22));
-    const long long t2 = H >> 20;
-    const double d2 = oz_i2d<20>(t2), d1 = oz_i2d<62>(t1), d0 = oz_i2d<104>(t0);
-    double e, s = ddm::two_sum(d2, d1, e);
-    hi = ddm::fast_two_sum(s, e + d0, lo);
+    double G[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int32_t p0 = v[4 * j][c] * 128 + v[4 * j + 1][c], p1 = v[4 * j + 2][c] * 128 + v[4 * j + 3][c];
+        G[j] = __fma_rn((double)p0, 16384.0, (double)p1);
+    }
+    const double a = G[0], b = G[1] * 0x1p-28, cc = G[2] * 0x1p-56, d = G[3] * 0x1p-84;
+    double e1, s1 = ddm::two_sum(a, b, e1);
+    double e2, s2 = ddm::two_sum(e1, cc, e2);
+    double l, h = ddm::two_sum(s1, s2, l);
+    h = ddm::fast_two_sum(h, l + (e2 + d), l);
+    hi = h * 0x1p-35;
+    lo = l * 0x1p-35;
 }
 
 // Epilogue warps 1-16: warp w reads tensor-memory lanes 32 (w mod 4) .. +31
@@ -551,7 +532,12 @@ void ozaki_check(cudaStream_t st, const OzakiWork &w) {
         CK(cudaStreamSynchronize(st));
     }
     err = *h;
-    if (err != 0) throw Error(ERR_CUDA, "ozaki: a tensor-core split update gave up waiting (code " + std::to_string(err) + ")");
+    if (err != 0) {
+        // clear the error word, so that the next launch starts afresh
+        CK(cudaMemsetAsync(w.err, 0, sizeof(int), st));
+        CK(cudaStreamSynchronize(st));
+        throw Error(ERR_CUDA, "ozaki: a tensor-core split update gave up waiting (code " + std::to_string(err) + ")");
+    }
 }
 
 } // namespace sddd

@@ -491,7 +491,12 @@ void ozaki_gemm_check(cudaStream_t st, const OzakiGemmWork &w) {
         CK(cudaStreamSynchronize(st));
     }
     err = *h;
-    if (err != 0) throw Error(ERR_CUDA, "ozaki gemm: a tensor-core split product gave up waiting (code " + std::to_string(err) + ")");
+    if (err != 0) {
+        // clear the error word, so that the next launch starts afresh
+        CK(cudaMemsetAsync(w.err, 0, sizeof(int), st));
+        CK(cudaStreamSynchronize(st));
+        throw Error(ERR_CUDA, "ozaki gemm: a tensor-core split product gave up waiting (code " + std::to_string(err) + ")");
+    }
 }
 
 } // namespace sddd

@@ -6,8 +6,12 @@
 // are inverted once per factorisation (trsv_diag_inverse, one CTA per
 // block, all blocks at once), and a solve is a wavefront of 64-entry
 // blocks in which no step divides or waits on a single entry:
-//   'N'  x_c = W_c (b_c - sum_{p<c} L(c,p) x_p)
-//   'T'  x_c = W_c^T (b_c - sum_{p>c} L(p,c)^T x_p)      (W_c = L(c,c)^-1)
+//   'N'  v_c = b_c - sum_{p<c} L(c,p) x_p,   x_c = W_c v_c
+//   'T'  v_c = b_c - sum_{p>c} L(p,c)^T x_p, x_c = W_c^T v_c   (W_c = L(c,c)^-1)
+// followed by one step of iterative refinement against L(c,c) itself,
+// x_c += W_c (v_c - L(c,c) x_c) (transposed for 'T'), which brings the
+// block's solve to the accuracy of a substitution even where L(c,c) is far
+// from orthogonal (the Schur matrix near the optimum).
 // One cooperative launch per solve: CTA k owns blocks k, k + G, ... (in
 // solve order).  For each of its blocks it streams the tiles L(c,p) (or
 // L(p,c)) and finally W_c into shared memory with bulk copies (one copy per
@@ -15,8 +19,9 @@
 // mbarrier), waits for block p's flag (release/acquire, bounded), and all
 // 256 threads multiply: thread (r, q) sums the 16 products of row r (or
 // column r) in quarter q of the tile into its own running dd sum, so a tile
-// costs a 16-step chain and the critical path per block is one tile, one
-// 4-way combination and the W_c product.  L is read once per solve.
+// costs a 16-step chain and the critical path per block is one tile and
+// three 64 x 64 products (W_c, L(c,c), W_c), each a 16-step chain and a
+// 4-way combination.  L is read once per solve.
 //
 // Every wait is bounded (the solve's wait budget, 2 s by default); a CTA
 // that gives up records the awaited block in the error word (read by
@@ -41,7 +46,7 @@ struct TbShared {
     int fail;
     long fail_at; // the first tile not consumed when the CTA gave up
 };
-constexpr size_t TB_SMEM = sizeof(double2) * ((size_t)TB_STAGES * TB_TILE + TB + 4 * TB) + 128;
+constexpr size_t TB_SMEM = sizeof(double2) * ((size_t)TB_STAGES * TB_TILE + 3 * TB + 4 * TB) + 128;
 static_assert(TB_SMEM <= 232448, "blocked solve: shared memory above the per-CTA limit");
 
 struct TbArgs {
@@ -55,8 +60,8 @@ struct TbArgs {
     int withhold; // a block whose flag is never published (-1: none)
 };
 
-// The k-th tile block c reads: 'N' L(c, k) for k < c, then W_c; 'T'
-// L(nblk-1-k, c) for k < nblk-1-c, then W_c.  Column j of the tile (rows
+// The k-th tile block c reads: 'N' L(c, k) for k < c, 'T' L(nblk-1-k, c)
+// for k < nblk-1-c; then L(c,c) and W_c (ntiles = 'N' c + 2, 'T' nblk-c+1).  Column j of the tile (rows
 // r0 .. r0+rows-1 of column c0 + j) goes to T + j * TB_LD.
 struct TileSrc {
     const dd_t *base; // column 0, row 0
@@ -70,6 +75,11 @@ __device__ __forceinline__ TileSrc tb_tile(const TbArgs &a, int c, int k, int nt
     if (k == ntiles - 1) {
         s.base = a.W + (long)c * TB * TB;
         s.ld = TB;
+        s.rows = nbc;
+        s.cols = nbc;
+    } else if (k == ntiles - 2) {
+        s.base = a.L + (long)c * TB + a.lda * (long)(c * TB);
+        s.ld = a.lda;
         s.rows = nbc;
         s.cols = nbc;
     } else if (a.trans == 0) {
@@ -126,11 +136,37 @@ __device__ __forceinline__ dd_t sm_dd(const double2 *T, int i) {
     return dd_make(v.x, v.y);
 }
 
+__device__ __forceinline__ double2 tb_pack(dd_t v) { return make_double2(v.hi, v.lo); }
+
+// The four quarters' partial sums of entry i: (p0 + p1) + (p2 + p3).
+__device__ __forceinline__ dd_t tb_sum4(const double2 *part, int i) {
+    return dd_add(dd_add(sm_dd(part, i), sm_dd(part, TB + i)), dd_add(sm_dd(part, 2 * TB + i), sm_dd(part, 3 * TB + i)));
+}
+
+// Thread (r, q)'s part of row r of M y ('N') or of column r of M^T y ('T')
+// over the terms t2 of quarter q (t2 < nb); with lower, only M(i,j), i >= j.
+__device__ __forceinline__ double2 tb_matvec(const double2 *M, const double2 *y, int r, int q, int nb, int trans, bool lower) {
+    dd_t w = dd_zero();
+    if (r < nb) {
+        int lo = q * 16, hi = min(lo + 16, nb);
+        if (trans == 0) {
+            if (lower) hi = min(hi, r + 1);
+            for (int t2 = lo; t2 < hi; ++t2) w = dd_add(w, dd_mul(sm_dd(M, r + t2 * TB_LD), sm_dd(y, t2)));
+        } else {
+            if (lower) lo = max(lo, r);
+            for (int t2 = lo; t2 < hi; ++t2) w = dd_add(w, dd_mul(sm_dd(M, t2 + r * TB_LD), sm_dd(y, t2)));
+        }
+    }
+    return tb_pack(w);
+}
+
 __global__ void __launch_bounds__(TB_THREADS, 1) trsv_blocked_kernel(TbArgs a) {
     extern __shared__ __align__(128) double2 tb_sm[];
     double2 *tiles = tb_sm;                      // TB_STAGES x TB_TILE
-    double2 *xs = tiles + TB_STAGES * TB_TILE;   // TB: x of block p, then the residual of block c
-    double2 *part = xs + TB;                     // 4 x TB partial sums
+    double2 *xs = tiles + TB_STAGES * TB_TILE;   // TB: x of block p, then the residual v of block c
+    double2 *x0 = xs + TB;                       // TB: W_c v
+    double2 *rs = x0 + TB;                       // TB: v - L(c,c) x0
+    double2 *part = rs + TB;                     // 4 x TB partial sums
     TbShared &S = *reinterpret_cast<TbShared *>(part + 4 * TB);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int r = tid & (TB - 1), q = tid >> 6; // row (or column) of the tile, quarter of its other index
@@ -145,7 +181,7 @@ __global__ void __launch_bounds__(TB_THREADS, 1) trsv_blocked_kernel(TbArgs a) {
     for (int k = blockIdx.x; k < a.nblk; k += gridDim.x) {
         const int c = a.trans == 0 ? k : a.nblk - 1 - k;
         const int nbc = min(TB, a.n - c * TB);
-        const int ntiles = a.trans == 0 ? c + 1 : a.nblk - c;
+        const int ntiles = a.trans == 0 ? c + 2 : a.nblk - c + 1;
         if (warp == 0)
             for (int t = 0; t < TB_STAGES && t < ntiles; ++t) {
                 const int st = (int)((g + t) % TB_STAGES);
@@ -160,7 +196,7 @@ __global__ void __launch_bounds__(TB_THREADS, 1) trsv_blocked_kernel(TbArgs a) {
             const bool last = t == ntiles - 1;
             const int p = a.trans == 0 ? t : a.nblk - 1 - t; // block whose x this tile multiplies
             if (tid == 0) {
-                bool ok = last || tb_wait_flag(a, p);
+                bool ok = t >= ntiles - 2 || tb_wait_flag(a, p);
                 int code = p + 1; // the block waited for
                 if (ok) {
                     ok = tb_wait_bar(&S.bar[st], (uint32_t)((gt / TB_STAGES) & 1), a.wait_ns);
@@ -174,7 +210,7 @@ __global__ void __launch_bounds__(TB_THREADS, 1) trsv_blocked_kernel(TbArgs a) {
             }
             __syncthreads();
             if (S.fail) break;
-            if (!last) {
+            if (t < ntiles - 2) {
                 const int nbp = min(TB, a.n - p * TB);
                 if (tid < TB) xs[tid] = tid < nbp ? __ldcg(reinterpret_cast<const double2 *>(a.x) + (long)p * TB + tid) : make_double2(0.0, 0.0);
                 __syncthreads();
@@ -188,37 +224,33 @@ __global__ void __launch_bounds__(TB_THREADS, 1) trsv_blocked_kernel(TbArgs a) {
                         for (int t2 = lo; t2 < hi; ++t2) acc = dd_add(acc, dd_mul(sm_dd(T, t2 + r * TB_LD), sm_dd(xs, t2)));
                     }
                 }
-            } else {
-                // residual of block c: b_c - (sum of the four partial sums)
+            } else if (last) {
+                // T = W_c; the previous stage holds L(c,c)
+                const double2 *Lc = tiles + (int)((gt - 1) % TB_STAGES) * TB_TILE;
+                // residual of block c: v = b_c - (sum of the four partial sums)
                 part[q * TB + r] = make_double2(acc.hi, acc.lo);
                 __syncthreads();
                 if (tid < TB) {
                     dd_t v = dd_zero();
-                    if (tid < nbc) {
-                        const dd_t s01 = dd_add(sm_dd(part, tid), sm_dd(part, TB + tid));
-                        const dd_t s23 = dd_add(sm_dd(part, 2 * TB + tid), sm_dd(part, 3 * TB + tid));
-                        v = dd_sub(ld_dd(a.x + (long)c * TB + tid), dd_add(s01, s23));
-                    }
+                    if (tid < nbc) v = dd_sub(ld_dd(a.x + (long)c * TB + tid), tb_sum4(part, tid));
                     xs[tid] = make_double2(v.hi, v.lo);
                 }
                 __syncthreads();
-                // x_c = W_c v ('N') or W_c^T v ('T')
-                dd_t w = dd_zero();
-                if (r < nbc) {
-                    const int lo = q * 16, hi = min(lo + 16, nbc);
-                    if (a.trans == 0) {
-                        for (int t2 = lo; t2 < hi; ++t2) w = dd_add(w, dd_mul(sm_dd(T, r + t2 * TB_LD), sm_dd(xs, t2)));
-                    } else {
-                        for (int t2 = lo; t2 < hi; ++t2) w = dd_add(w, dd_mul(sm_dd(T, t2 + r * TB_LD), sm_dd(xs, t2)));
-                    }
-                }
-                part[q * TB + r] = make_double2(w.hi, w.lo);
+                // x0 = W_c v ('N') or W_c^T v ('T')
+                part[q * TB + r] = tb_matvec(T, xs, r, q, nbc, a.trans, false);
                 __syncthreads();
-                if (tid < nbc) {
-                    const dd_t s01 = dd_add(sm_dd(part, tid), sm_dd(part, TB + tid));
-                    const dd_t s23 = dd_add(sm_dd(part, 2 * TB + tid), sm_dd(part, 3 * TB + tid));
-                    st_dd(a.x + (long)c * TB + tid, dd_add(s01, s23));
-                }
+                if (tid < TB) x0[tid] = tid < nbc ? tb_pack(tb_sum4(part, tid)) : make_double2(0.0, 0.0);
+                __syncthreads();
+                // rs = v - L(c,c) x0 (lower triangle only: the strict upper
+                // part of the tile holds the Schur matrix's own entries)
+                part[q * TB + r] = tb_matvec(Lc, x0, r, q, nbc, a.trans, true);
+                __syncthreads();
+                if (tid < TB) rs[tid] = tid < nbc ? tb_pack(dd_sub(sm_dd(xs, tid), tb_sum4(part, tid))) : make_double2(0.0, 0.0);
+                __syncthreads();
+                // x = x0 + W_c rs
+                part[q * TB + r] = tb_matvec(T, rs, r, q, nbc, a.trans, false);
+                __syncthreads();
+                if (tid < nbc) st_dd(a.x + (long)c * TB + tid, dd_add(sm_dd(x0, tid), tb_sum4(part, tid)));
                 __threadfence();
             }
             __syncthreads(); // stage st and xs are free again

@@ -92,8 +92,8 @@ class RefSolver:
         if not self.h:
             raise RuntimeError("ref_open failed")
         self.h = ctypes.c_void_p(self.h)
-        dims = np.zeros(64, np.int32)
-        lib.ref_dims(self.h, ptr(dims), 64)
+        dims = np.zeros(4096, np.int32)
+        assert lib.ref_dims(self.h, ptr(dims), 4096) > 0
         self.m, self.nsdp, self.nlp, self.ndim = map(int, dims[:4])
         self.blocks = [int(x) for x in dims[4:4 + self.nsdp]]
 
