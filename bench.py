@@ -202,7 +202,7 @@ def batch_measure(sddd, device, rank, world, args):
     par = sddd.param(param_path)
     # independent problems shard over ranks by work, no data-path exchange
     mine = shard.partition_by_work([shard.work_estimate(m, [n]) for _, n, m in paths], world)[rank]
-    with sddd.Batch(device) as bt:
+    with sddd.Batch(device, args.batch_workers) as bt:
         for q in mine:
             path, n, m = paths[q]
             bt.add_file(path, m, n * n)
@@ -218,7 +218,7 @@ def batch_measure(sddd, device, rank, world, args):
     out = {"workload": f"{BATCH['count']} dense random SDPs, n ~ U[10,80], m ~ U[20,200], seed {BATCH['seed']}, epsilon {EPS:g}, with d(c.x)/dc",
            "solves_per_s": len(paths) / dt,
            "solves_per_s_basis": "every problem run to the end of its main loop, whatever its final phase (phases below)",
-           "pdopt_solves_per_s": n_opt / dt, "pdOPT": n_opt, "seconds": dt, "ranks": world,
+           "pdopt_solves_per_s": n_opt / dt, "pdOPT": n_opt, "seconds": dt, "ranks": world, "workers": args.batch_workers or "default",
            "phases_rank0": counts, "problems_rank0": len(mine),
            "mean_iterations_rank0": (sum(r.iterations for r in res) / len(res)) if res else None}
     exe = ROOT / "oracle" / "_ref" / "sdpa_dd"
@@ -654,12 +654,18 @@ def main():
     ap.add_argument("--tc", type=int, default=16, help="slices of the tensor-core split Cholesky (8..16; 0 = plain dd only)")
     ap.add_argument("--no-solve", action="store_true", help="skip the two solves to relative gap 1e-25")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched workload (256 small SDPs)")
+    ap.add_argument("--batch-workers", type=int, default=0, help="host workers of the batched workload (0: the library's default)")
+    ap.add_argument("--batch-only", action="store_true", help="run the batched workload alone and print its figures")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case(args)
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local = dist_init(args)
+    if args.batch_only:
+        args.no_cpu_baseline = True
+        print(json.dumps(batch_measure(load_pkg(), local, rank, world, args)))
+        return 0
     try:
         if args.impl == "reference":
             return run_reference(args, world, rank)

@@ -211,8 +211,12 @@ int sddd_adjoint_grad_F(sddd_ctx *ctx, int k, sddd_dd *grad_Fk);
 
 /* -- batches of independent problems (no counterpart in the reference) --
  * Many SDPs solved on one GPU by a pool of `workers` host threads (<= 0:
- * 32), each with its own context and stream, so the small kernels of many
- * problems run at once.  Every problem is solved exactly as sddd_solve
+ * min(8, host cores)), each with its own context and stream, so the small
+ * kernels of many problems run at once.  The Schur build and Cholesky of B
+ * of the problems with one block of dense constraints (the dense random
+ * kind) run batched across the workers: one captured CUDA graph of
+ * persistent launches per gathering, tile shapes autotuned per size class
+ * (sddd_batch_set_core turns it off; sddd_batch_tuning reports the shapes).  Every problem is solved exactly as sddd_solve
  * solves it (same iterates, bit for bit).  Problems are added from SDPA
  * text or from memory (the arguments of sddd_read_problem /
  * sddd_upload_problem); the add calls return the problem's index.
@@ -234,6 +238,8 @@ int sddd_batch_solve(sddd_batch *b, const sddd_param *param, int with_grad, sddd
 int sddd_batch_status(const sddd_batch *b, int index);
 int sddd_batch_get_point(const sddd_batch *b, int index, sddd_dd *X, sddd_dd *y, sddd_dd *Z);
 int sddd_batch_grad_c(const sddd_batch *b, int index, sddd_dd *grad_c);
+int sddd_batch_set_core(sddd_batch *b, int on);
+const char *sddd_batch_tuning(const sddd_batch *b);
 
 /* -- measurement -- */
 /* Kernels this library has launched in this process so far. */

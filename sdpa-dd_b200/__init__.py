@@ -123,6 +123,8 @@ def lib() -> ctypes.CDLL:
         "sddd_batch_get_point": (ci, [vp, ci, vp, vp, vp]),
         "sddd_batch_grad_c": (ci, [vp, ci, vp]),
         "sddd_adjoint_grad_F": (ci, [vp, ci, vp]),
+        "sddd_batch_set_core": (ci, [vp, ci]),
+        "sddd_batch_tuning": (ctypes.c_char_p, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

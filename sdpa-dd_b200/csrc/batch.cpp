@@ -21,6 +21,7 @@
 
 #include "../../include/sddd.h"
 #include "adjoint.h"
+#include "batched.h"
 #include "capi_internal.h"
 #include "context.h"
 #include "newton.h"
@@ -30,6 +31,8 @@ struct sddd_batch {
     int device = 0;
     int workers = 0;
     bool blocking_waits = false; // more workers than host cores: block instead of spin
+    bool use_core = true;        // eligible problems take the batched Newton core
+    std::string tuning;          // the core's autotuned tile shapes, after a solve
     std::vector<sddd::Problem> probs;
     // per problem, from the last sddd_batch_solve
     std::vector<sddd_result> results;
@@ -77,29 +80,59 @@ int guarded(sddd_batch *b, F &&f) {
     }
 }
 
+// A worker's context, set up for the batch (and for the batched core).
+sddd::Context *worker_context(sddd_batch &B, sddd::CoreEngine *core) {
+    std::unique_ptr<sddd::Context> c(sddd::create_context(B.device));
+    sddd::set_shared_gpu(*c, B.blocking_waits);
+    if (core) {
+        CK(cudaEventCreateWithFlags(&c->core_ready, cudaEventDisableTiming));
+        c->core = core;
+    }
+    return c.release();
+}
+
+// The engine counts a worker as active for the span of one solve.
+struct CoreSpan {
+    sddd::CoreEngine *e;
+    bool on = false;
+    explicit CoreSpan(sddd::CoreEngine *x) : e(x) {
+        if (e) {
+            e->enter();
+            on = true;
+        }
+    }
+    void end() {
+        if (on) e->leave();
+        on = false;
+    }
+    ~CoreSpan() { end(); }
+};
+
 // One worker: its own context; problems by index from `next` in `order`.
-void batch_worker(sddd_batch &B, const std::vector<int> &order, std::atomic<int> &next, const sddd::Param &par, bool with_grad) {
+void batch_worker(sddd_batch &B, const std::vector<int> &order, std::atomic<int> &next, const sddd::Param &par, bool with_grad,
+                  sddd::CoreEngine *core) {
     std::unique_ptr<sddd::Context> ctx;
     try {
-        ctx.reset(sddd::create_context(B.device));
+        ctx.reset(worker_context(B, core));
     } catch (const sddd::Error &e) {
         // no context: leave this worker's share to the others
         return;
     }
-    sddd::set_shared_gpu(*ctx, B.blocking_waits);
-    sddd::Context &c = *ctx;
     for (;;) {
         const int q = next.fetch_add(1);
         if (q >= (int)order.size()) break;
         const int idx = order[q];
+        sddd::Context &c = *ctx;
         try {
             sddd::Problem p = B.probs[idx];
             sddd::upload_problem(c, std::move(p));
             sddd::Solver s(c, par);
+            CoreSpan span(core);
             s.start();
             int rc = 0;
             while ((rc = s.step(nullptr, nullptr)) == 0) {
             }
+            span.end();
             s.finish();
             sddd_fill_result(s, rc, &B.results[idx]);
             B.X[idx].resize(c.space_len);
@@ -127,8 +160,7 @@ void batch_worker(sddd_batch &B, const std::vector<int> &order, std::atomic<int>
             if (e.code == SDDD_ERR_CUDA) {
                 // the context may be unusable: start a fresh one
                 try {
-                    ctx.reset(sddd::create_context(B.device));
-                    sddd::set_shared_gpu(*ctx, B.blocking_waits);
+                    ctx.reset(worker_context(B, core));
                 } catch (const sddd::Error &) {
                     return;
                 }
@@ -213,16 +245,27 @@ int sddd_batch_solve(sddd_batch *b, const sddd_param *param, int with_grad, sddd
         const sddd::Param par = to_param(param);
         std::atomic<int> next{0};
         const int nw = std::max(1, std::min(b->workers, P));
+        std::unique_ptr<sddd::CoreEngine> core;
+        if (b->use_core) core.reset(new sddd::CoreEngine(b->device));
         std::vector<std::thread> pool;
         pool.reserve(nw);
-        for (int t = 0; t < nw; ++t) pool.emplace_back([&] { batch_worker(*b, order, next, par, with_grad != 0); });
+        for (int t = 0; t < nw; ++t) pool.emplace_back([&] { batch_worker(*b, order, next, par, with_grad != 0, core.get()); });
         for (auto &th : pool) th.join();
+        if (core) b->tuning = core->tuning();
         if (results) std::memcpy(results, b->results.data(), sizeof(sddd_result) * P);
         for (int p = 0; p < P; ++p)
             if (b->status[p] < 0) throw sddd::Error(b->status[p], "problem " + std::to_string(p) + ": " + b->errors[p]);
         return SDDD_OK;
     });
 }
+
+int sddd_batch_set_core(sddd_batch *b, int on) {
+    if (!b) return SDDD_ERR_ARG;
+    b->use_core = on != 0;
+    return SDDD_OK;
+}
+
+const char *sddd_batch_tuning(const sddd_batch *b) { return b ? b->tuning.c_str() : ""; }
 
 int sddd_batch_status(const sddd_batch *b, int index) {
     if (!b || index < 0 || index >= (int)b->status.size()) return SDDD_ERR_ARG;

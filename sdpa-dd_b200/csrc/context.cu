@@ -44,6 +44,7 @@ Context::~Context() {
     if (tc.ev_diag) cudaEventDestroy(tc.ev_diag);
     if (tc.side) cudaStreamDestroy(tc.side);
     if (sync_ev) cudaEventDestroy(sync_ev);
+    if (core_ready) cudaEventDestroy(core_ready);
     if (stream) cudaStreamDestroy(stream);
     if (h_pin) cudaFreeHost(h_pin);
 }

@@ -118,8 +118,14 @@ struct Space {
     dd_t *blk(const std::vector<long> &off, int l) const { return buf.p + off[l]; }
 };
 
+class CoreEngine;
+
 struct Context {
     int device = 0;
+    // a batch worker's batched Newton core (batched.h), or null; the event
+    // marks the core's inputs ready on this context's stream
+    CoreEngine *core = nullptr;
+    cudaEvent_t core_ready = nullptr;
     cudaStream_t stream = nullptr;
     bool shared_gpu = false; // a batch worker: other contexts' streams share the GPU
     // pinned host staging for the small device-to-host reads of the solver

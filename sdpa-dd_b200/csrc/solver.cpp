@@ -8,6 +8,7 @@
 #include <cstring>
 #include <vector>
 
+#include "batched.h"
 #include "newton.h"
 
 namespace sddd {
@@ -212,13 +213,23 @@ int Solver::step(FILE *display, FILE *out) {
     cudaEvent_t e0 = clk.mark();
     make_rhs(c, false, dd_mul(beta_value, mu_current), dinf);
     cudaEvent_t e1 = clk.mark();
-    schur_build(c);
-    cudaEvent_t e2 = clk.mark();
-    clk.span(e0, e1, &tm.makegVec);
-    clk.span(e1, e2, &tm.makebMat);
-    const auto th0 = std::chrono::steady_clock::now();
-    int info = schur_factor(c);
-    tm.choleskybMat += std::chrono::duration<double>(std::chrono::steady_clock::now() - th0).count();
+    int info = 0;
+    if (c.core && core_eligible(c)) {
+        // a batch worker: the Schur build and Cholesky run batched with the
+        // other workers' problems (the same operations, entry by entry)
+        clk.span(e0, e1, &tm.makegVec);
+        const auto th0 = std::chrono::steady_clock::now();
+        info = c.core->schur_factor(c);
+        tm.choleskybMat += std::chrono::duration<double>(std::chrono::steady_clock::now() - th0).count();
+    } else {
+        schur_build(c);
+        cudaEvent_t e2 = clk.mark();
+        clk.span(e0, e1, &tm.makegVec);
+        clk.span(e1, e2, &tm.makebMat);
+        const auto th0 = std::chrono::steady_clock::now();
+        info = schur_factor(c);
+        tm.choleskybMat += std::chrono::duration<double>(std::chrono::steady_clock::now() - th0).count();
+    }
     last_cholesky_info = info;
     if (info != 0) {
         if (display) std::fprintf(display, "cholesky miss condition :: not positive definite :: info = %d\n", info);

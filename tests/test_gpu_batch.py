@@ -109,3 +109,42 @@ def test_batch_gradient_is_the_envelope(tmp_path):
             g = bt.grad_c(q)
             err = np.abs((g["hi"] + y["hi"]) + (g["lo"] + y["lo"])).max() / max(1.0, np.abs(y["hi"]).max())
             assert err < 1e-18, (q, err)
+
+
+def test_batched_core_matches_per_problem_core(tmp_path):
+    """The batched Newton core (one captured CUDA graph per gathering of
+    the workers' problems: batched F/G products, tiled pair products in the
+    autotuned shape of each size class, one-CTA Cholesky per problem) gives
+    every problem the bits the per-problem kernels give it: the same batch
+    solved with the core on and off agrees in phase, iteration count,
+    objectives and X, y, Z, problem by problem."""
+    sddd = load_pkg()
+    P = _problems()
+    rng = np.random.default_rng(77)
+    cases = []
+    for q in range(18):
+        n, m = int(rng.integers(10, 41)), int(rng.integers(20, 161))  # size classes m <= 64, <= 128, <= 256
+        path = tmp_path / f"c{q}.dat-s"
+        path.write_text(P.dense_random(n, m, seed=3000 + q))
+        cases.append((path, n, m))
+    par = sddd.param(P.write_param(str(tmp_path / "p.sdpa"), eps=1e-25, max_iter=100))
+    out = {}
+    for core in (1, 0):
+        with sddd.Batch(0, workers=8) as bt:
+            assert bt.L.sddd_batch_set_core(bt.h, core) == 0
+            for path, n, m in cases:
+                bt.add_file(path, m, n * n)
+            res = bt.solve(par, with_grad=False)
+            pts = [bt.point(q) for q in range(len(cases))]
+            tuning = bt.L.sddd_batch_tuning(bt.h).decode()
+            out[core] = (res, pts, tuning)
+    (r1, p1, tuning), (r0, p0, _) = out[1], out[0]
+    print("batched core tile shapes:", tuning)
+    assert "m<=64" in tuning and "m<=128" in tuning
+    for q in range(len(cases)):
+        a, b = r1[q], r0[q]
+        assert (a.phase, a.iterations, a.stop_reason) == (b.phase, b.iterations, b.stop_reason), q
+        assert (a.objValPrimal.hi, a.objValPrimal.lo, a.objValDual.hi, a.objValDual.lo) == (
+            b.objValPrimal.hi, b.objValPrimal.lo, b.objValDual.hi, b.objValDual.lo), q
+        for u, v in zip(p1[q], p0[q]):
+            assert _same(u, v), q
