@@ -377,7 +377,7 @@ void CoreEngine::enter() {
 void CoreEngine::leave() {
     std::unique_lock<std::mutex> lk(mu);
     --active;
-    if (!p->pending.empty() && (int)p->pending.size() >= active) launch_locked();
+    if (!p->pending.empty() && (int)p->pending.size() >= active) launch_or_fail_locked();
     cv.notify_all();
 }
 
@@ -464,6 +464,20 @@ void CoreEngine::launch_locked() {
     I.pending.clear();
 }
 
+// launch_locked; a failure ends the gathering for all its members.
+void CoreEngine::launch_or_fail_locked() {
+    const unsigned long gen = generation;
+    try {
+        launch_locked();
+    } catch (const Error &e) {
+        failed_generation = gen;
+        failed_msg = e.what();
+        p->pending.clear();
+        ++generation;
+    }
+    cv.notify_all();
+}
+
 int CoreEngine::schur_factor(Context &c) {
     CK(cudaMemsetAsync(c.info.p, 0, sizeof(int), c.stream));
     c.winv_valid = false;
@@ -473,17 +487,14 @@ int CoreEngine::schur_factor(Context &c) {
         p->pending.push_back(&c);
         const unsigned long gen = generation;
         if ((int)p->pending.size() >= active || (int)p->pending.size() >= CORE_CAP) {
-            launch_locked();
-            cv.notify_all();
+            launch_or_fail_locked();
         } else {
             while (generation == gen) {
                 const auto deadline = p->first_wait + std::chrono::microseconds(CORE_WAIT_US);
-                if (cv.wait_until(lk, deadline) == std::cv_status::timeout && generation == gen) {
-                    launch_locked();
-                    cv.notify_all();
-                }
+                if (cv.wait_until(lk, deadline) == std::cv_status::timeout && generation == gen) launch_or_fail_locked();
             }
         }
+        if (failed_generation == gen) throw Error(ERR_CUDA, "batched core: " + failed_msg);
     }
     int info = 0;
     d2h(c, &info, c.info.p, sizeof(int));

@@ -38,7 +38,11 @@ class CoreEngine {
     std::condition_variable cv;
     int active = 0;
     unsigned long generation = 0;
+    // a gathering whose launch failed: its members report the error
+    unsigned long failed_generation = ~0ul;
+    std::string failed_msg;
     void launch_locked();
+    void launch_or_fail_locked();
 };
 
 } // namespace sddd
