@@ -293,6 +293,52 @@ int sddd_test_withhold_block(sddd_ctx *ctx, int block);
  * (no counterpart in the reference). */
 int sddd_Rdot_pairs_tc(sddd_ctx *ctx, long n, long k, const sddd_dd *W, long ldw, const sddd_dd *V, long ldv, sddd_dd *C, long ldc, int slices);
 
+/* -- sparse Schur complement --
+ * The reference keeps B dense unless the problem has more than 100
+ * constraints, more than 5 blocks (SDP blocks + LP entries), no block that
+ * touches more than half of the constraints, an aggregate pattern of at most
+ * 0.25 m^2 entries and a factor of at most 0.4 m^2 entries
+ * (Chordal::ordering_bMat, sdpa_chordal.cpp:348-438); then rows of B are
+ * renumbered by a minimum-degree ordering and B is factored and solved in
+ * sparse form (Lal::getCholesky(SparseMatrix&, int*), sdpa_linear.cpp:353-395;
+ * Lal::solveSystems(Vector&, SparseMatrix&, Vector&), :654-810).  The
+ * reference orders with SPOOLES's minimum degree, a library its sources do
+ * not include; here the ordering is an exact minimum degree, ties to the
+ * smallest constraint index.
+ * mode: 0 the reference's thresholds (default), 1 always dense, 2 always
+ * sparse (the reference's "SPARSE computation for debugging" thresholds,
+ * sdpa_chordal.cpp:53-58).  Setting the mode re-plans an attached problem. */
+int sddd_set_schur_mode(sddd_ctx *ctx, int mode);
+typedef struct {
+    int sparse;      /* 1: SPARSE computation, 0: DENSE computation */
+    int m;
+    long aggregate;  /* entries of the aggregate pattern, diagonal included */
+    long extended;   /* 2 nnz(L) - m of the ordering (0 when not ordered) */
+    long nnz;        /* entries of the factor's rows (sparse only) */
+    long ntiles;     /* 64 x 64 tiles the device factor stores (sparse only) */
+    char reason[96]; /* why B stayed dense */
+} sddd_schur_info;
+/* The attached problem's Schur form; with sparse, order[m] (new -> old
+ * constraint), diagonalIndex[m + 1] and column_index[nnz] (the reference's
+ * sparse_bMat layout: row b holds b, then the later rows of the factor's
+ * column b, ascending) when the pointers are not NULL. */
+int sddd_schur_form(const sddd_ctx *ctx, sddd_schur_info *out, int *order, int *diagonalIndex, int *column_index);
+/* The same decision for a problem file, on the host only (no device). */
+int sddd_plan_schur(const char *path, int sparse, int mode, sddd_schur_info *out, int *order, int *diagonalIndex, int *column_index);
+/* The factor of the last sddd_schur_factor in that layout (host sp_ele[nnz];
+ * the diagonal holds 1 / sqrt of the pivot, as the reference stores it). */
+int sddd_sparse_factor_values(sddd_ctx *ctx, sddd_dd *sp_ele);
+/* Lal::getCholesky(SparseMatrix&, int*) on a caller's matrix: structure on
+ * the host (diagonalIndex[m + 1], column_index[nnz]; each row starts with its
+ * diagonal, ascending, closed under elimination - anything else is
+ * SDDD_ERR_ARG), sp_ele[nnz] on the device, factored in place.  Like the
+ * reference it reports no failure: a negative pivot gives a zero row.  Use a
+ * context without a problem. */
+int sddd_sparse_getCholesky(sddd_ctx *ctx, int m, const int *diagonalIndex, const int *column_index, sddd_dd *sp_ele);
+/* Lal::solveSystems(Vector&, SparseMatrix&, Vector&): x (device, m) <-
+ * (L L^T)^-1 x for a factor from sddd_sparse_getCholesky (sp_ele device). */
+int sddd_sparse_solveSystems(sddd_ctx *ctx, int m, const int *diagonalIndex, const int *column_index, const sddd_dd *sp_ele, sddd_dd *x);
+
 /* -- dd kernels on device memory: the MPLAPACK seam --
  * The argument lists of MPLAPACK's dd routines (mplapack/mpblas_dd.h:47,54,
  * mplapack/mplapack_dd.h:41) with the context first; pointers are device

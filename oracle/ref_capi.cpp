@@ -179,6 +179,37 @@ long ref_Rpotrf(const char *uplo, long n, double *A, long lda) {
     Rpotrf(uplo, n, (dd_real *)A, lda, info);
     return (long)info;
 }
+// Lal::getCholesky(SparseMatrix&, int*) (sdpa_linear.cpp:353-395) on a
+// matrix in the sparse_bMat layout: row b holds column_index[diagonalIndex[b]
+// .. diagonalIndex[b+1]) (b first, ascending); vals[nnz] factored in place.
+static void sparse_from(SparseMatrix &A, int m, const int *diagonalIndex, const int *column_index, const double *vals) {
+    const int nnz = diagonalIndex[m];
+    A.initialize(m, m, SparseMatrix::SPARSE, nnz);
+    for (int b = 0; b < m; ++b)
+        for (int q = diagonalIndex[b]; q < diagonalIndex[b + 1]; ++q) {
+            A.row_index[q] = b;
+            A.column_index[q] = column_index[q];
+            A.sp_ele[q] = ld(vals + 2 * q);
+        }
+    A.NonZeroCount = nnz;
+}
+void ref_sparse_getCholesky(int m, const int *diagonalIndex, const int *column_index, double *vals) {
+    SparseMatrix A;
+    sparse_from(A, m, diagonalIndex, column_index, vals);
+    std::vector<int> di(diagonalIndex, diagonalIndex + m + 1);
+    Lal::getCholesky(A, di.data());
+    for (int q = 0; q < diagonalIndex[m]; ++q) st(vals + 2 * q, A.sp_ele[q]);
+}
+// Lal::solveSystems(Vector&, SparseMatrix&, Vector&) (sdpa_linear.cpp:
+// 654-810): x <- (L L^T)^-1 x for a factor from ref_sparse_getCholesky.
+void ref_sparse_solveSystems(int m, const int *diagonalIndex, const int *column_index, const double *vals, double *x) {
+    SparseMatrix A;
+    sparse_from(A, m, diagonalIndex, column_index, vals);
+    Vector b(m), y(m);
+    for (int i = 0; i < m; ++i) b.ele[i] = ld(x + 2 * i);
+    Lal::solveSystems(y, A, b);
+    for (int i = 0; i < m; ++i) st(x + 2 * i, y.ele[i]);
+}
 long ref_Rsteqr(const char *compz, long n, double *d, double *e, double *Z, long ldz, double *work) {
     mplapackint info = 0;
     Rsteqr(compz, n, (dd_real *)d, (dd_real *)e, (dd_real *)Z, ldz, (dd_real *)work, info);
@@ -212,9 +243,31 @@ void ref_lanczos_min_eig(long n, double *L, double *X, double *out) {
     st(out, Lal::getMinEigen(lMat, xMat, Q, o, b, r, q, qold, w, tmp, d1, d2, wv));
 }
 
+// B of the last Make_bMat as a dense m x m matrix in the constraints' own
+// numbering (the sparse form's entries placed through the ordering, both
+// triangles).
+static void capture_B(RefSolver &s) {
+    Newton &nt = *s.newton;
+    if (nt.bMat_type == Newton::DENSE) {
+        s.bCaptured.copyFrom(nt.bMat);
+        return;
+    }
+    const int m = s.m;
+    s.bCaptured.initialize(m, m, DenseMatrix::DENSE);
+    s.bCaptured.setZero();
+    for (int k = 0; k < nt.sparse_bMat.NonZeroCount; ++k) {
+        const int i = nt.ordering[nt.sparse_bMat.row_index[k]], j = nt.ordering[nt.sparse_bMat.column_index[k]];
+        s.bCaptured.de_ele[i + (long)m * j] = nt.sparse_bMat.sp_ele[k];
+        s.bCaptured.de_ele[j + (long)m * i] = nt.sparse_bMat.sp_ele[k];
+    }
+}
+
 // Opens a problem exactly as pinpal does before its main loop.
-// paramFile may be NULL (defaults).  Returns NULL on failure.
-void *ref_open(const char *dataFile, const char *paramFile, double kappa) {
+// paramFile may be NULL (defaults).  schurMode 0 keeps the reference's
+// thresholds of Chordal::initialize (sdpa_chordal.cpp:42-45); 1 and 2 set
+// its "DENSE computation for debugging" and "SPARSE computation for
+// debugging" values (sdpa_chordal.cpp:47-58).  Returns NULL on failure.
+void *ref_open_mode(const char *dataFile, const char *paramFile, double kappa, int schurMode) {
     FILE *fp = fopen(dataFile, "r");
     if (!fp) return nullptr;
     RefSolver *s = new RefSolver();
@@ -271,6 +324,17 @@ void *ref_open(const char *dataFile, const char *paramFile, double kappa) {
     for (int k = 0; k < s->m; ++k) s->inputData.A[k].changeToDense();
     s->newton = new Newton(s->m, s->SDP_nBlock, s->SDP_blockStruct.data(), s->SOCP_nBlock, s->SOCP_blockStruct.data(), s->LP_nBlock);
     Chordal chordal;
+    if (schurMode == 1) {
+        chordal.m_threshold = 10000000;
+        chordal.b_threshold = 1000000;
+        chordal.aggregate_threshold = 0.0;
+        chordal.extend_threshold = 0.0;
+    } else if (schurMode == 2) {
+        chordal.m_threshold = 0;
+        chordal.b_threshold = 0;
+        chordal.aggregate_threshold = 2.0;
+        chordal.extend_threshold = 2.0;
+    }
     FILE *devnull2 = fopen("/dev/null", "w");
     chordal.ordering_bMat(s->m, s->SDP_nBlock + s->SOCP_nBlock + s->LP_nBlock, s->inputData, devnull2);
     s->newton->initialize_bMat(s->m, chordal, s->inputData, devnull2);
@@ -294,6 +358,8 @@ void *ref_open(const char *dataFile, const char *paramFile, double kappa) {
     s->dzPred.initialize(s->SDP_nBlock, s->SDP_blockStruct.data(), s->SOCP_nBlock, s->SOCP_blockStruct.data(), s->LP_nBlock);
     return s;
 }
+
+void *ref_open(const char *dataFile, const char *paramFile, double kappa) { return ref_open_mode(dataFile, paramFile, kappa, 0); }
 
 void ref_close(void *h) {
     RefSolver *s = (RefSolver *)h;
@@ -339,7 +405,7 @@ int ref_step(void *h) {
     nt.Make_gVec(Newton::PREDICTOR, s->inputData, s->currentPt, s->currentRes, s->mu, s->beta, s->phase, s->work, s->com);
     if (s->capture) s->gPred.copyFrom(nt.gVec);
     nt.Make_bMat(s->inputData, s->currentPt, s->work, s->com);
-    if (s->capture) s->bCaptured.copyFrom(nt.bMat);
+    if (s->capture) capture_B(*s);
     if (!nt.compute_DyVec(Newton::PREDICTOR, s->inputData, s->currentPt, s->work, s->com)) return 2;
     nt.compute_DzMat(s->inputData, s->currentRes, s->phase, s->com);
     nt.compute_DxMat(s->currentPt, s->work, s->com);
@@ -443,8 +509,38 @@ int ref_set_point(void *h, const double *X, const double *y, const double *Z) {
 void ref_schur(void *h, double *out) {
     RefSolver *s = (RefSolver *)h;
     s->newton->Make_bMat(s->inputData, s->currentPt, s->work, s->com);
+    capture_B(*s);
     long len = (long)s->m * s->m;
-    for (long i = 0; i < len; ++i) st(out + 2 * i, s->newton->bMat.de_ele[i]);
+    for (long i = 0; i < len; ++i) st(out + 2 * i, s->bCaptured.de_ele[i]);
+}
+
+// 1 when Newton::initialize_bMat chose the sparse Schur form.
+int ref_schur_sparse(void *h) { return ((RefSolver *)h)->newton->bMat_type == Newton::SPARSE ? 1 : 0; }
+
+// The sparse form's layout: ordering[m] (new -> old), diagonalIndex[m + 1],
+// column_index[nnz] (any of them may be NULL).  Returns nnz, or -1 when B
+// is dense.
+long ref_sparse_layout(void *h, int *ordering, int *diagonalIndex, int *column_index) {
+    RefSolver *s = (RefSolver *)h;
+    Newton &nt = *s->newton;
+    if (nt.bMat_type != Newton::SPARSE) return -1;
+    const long nnz = nt.sparse_bMat.NonZeroCount;
+    if (ordering) std::copy(nt.ordering, nt.ordering + s->m, ordering);
+    if (diagonalIndex) std::copy(nt.diagonalIndex, nt.diagonalIndex + s->m + 1, diagonalIndex);
+    if (column_index) std::copy(nt.sparse_bMat.column_index, nt.sparse_bMat.column_index + nnz, column_index);
+    return nnz;
+}
+
+// The sparse form's entries (after a pass: the factor of the last
+// Cholesky).  Returns nnz, or -1 when B is dense.
+long ref_sparse_values(void *h, double *out) {
+    RefSolver *s = (RefSolver *)h;
+    Newton &nt = *s->newton;
+    if (nt.bMat_type != Newton::SPARSE) return -1;
+    const long nnz = nt.sparse_bMat.NonZeroCount;
+    if (out)
+        for (long k = 0; k < nnz; ++k) st(out + 2 * k, nt.sparse_bMat.sp_ele[k]);
+    return nnz;
 }
 
 // Scalars of the last pass / current state:

@@ -1,5 +1,4 @@
 /* Declaration-only stand-in for the SPOOLES header Graph.h (the SPOOLES
- * sources are not available).  The sparse-Schur path that needs SPOOLES is
- * never taken for problems with nBlock <= 5 or m <= 100; every entry point
- * is stubbed in spooles_stub.cpp and aborts if reached. */
+ * sources are not available): the entry points the reference calls are
+ * declared in spooles_types.h and implemented in spooles_shim.cpp. */
 #include "spooles_types.h"

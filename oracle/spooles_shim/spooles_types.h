@@ -1,7 +1,7 @@
 #ifndef ORACLE_SPOOLES_TYPES_H
 #define ORACLE_SPOOLES_TYPES_H
 /* Opaque SPOOLES types and the prototypes the reference calls
- * (sdpa_chordal.cpp, sdpa_newton.cpp).  Stubs abort. */
+ * (sdpa_chordal.cpp, sdpa_newton.cpp), implemented in spooles_shim.cpp. */
 #include <stdio.h>
 #include <time.h>
 typedef struct _IV IV;

@@ -42,6 +42,12 @@ PHASES = ["noINFO", "pFEAS", "dFEAS", "pdFEAS", "pdINF", "pFEAS_dINF", "pINF_dFE
 _lib = None
 
 
+class SdddSchurInfo(ctypes.Structure):
+    """sddd_schur_info: the Schur form the reference's thresholds choose."""
+    _fields_ = [("sparse", ctypes.c_int), ("m", ctypes.c_int), ("aggregate", ctypes.c_long), ("extended", ctypes.c_long),
+                ("nnz", ctypes.c_long), ("ntiles", ctypes.c_long), ("reason", ctypes.c_char * 96)]
+
+
 def lib() -> ctypes.CDLL:
     """The loaded libsddd.so (raises when it has not been built)."""
     global _lib
@@ -125,6 +131,12 @@ def lib() -> ctypes.CDLL:
         "sddd_adjoint_grad_F": (ci, [vp, ci, vp]),
         "sddd_batch_set_core": (ci, [vp, ci]),
         "sddd_batch_tuning": (ctypes.c_char_p, [vp]),
+        "sddd_set_schur_mode": (ci, [vp, ci]),
+        "sddd_schur_form": (ci, [vp, ctypes.POINTER(SdddSchurInfo), vp, vp, vp]),
+        "sddd_plan_schur": (ci, [ctypes.c_char_p, ci, ci, ctypes.POINTER(SdddSchurInfo), vp, vp, vp]),
+        "sddd_sparse_factor_values": (ci, [vp, vp]),
+        "sddd_sparse_getCholesky": (ci, [vp, ci, vp, vp, vp]),
+        "sddd_sparse_solveSystems": (ci, [vp, ci, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -230,6 +242,28 @@ class Context:
         X, y, Z = (np.ascontiguousarray(a, dtype=DD) for a in (X, y, Z))
         return self._check(self.L.sddd_set_point(self.h, _ptr(X), _ptr(y), _ptr(Z)), "set_point")
 
+    def set_schur_mode(self, mode):
+        """0 the reference's thresholds, 1 always dense, 2 always sparse."""
+        self._check(self.L.sddd_set_schur_mode(self.h, mode), "sddd_set_schur_mode")
+
+    def schur_form(self):
+        """(info, order, diagonalIndex, column_index) of the attached problem."""
+        info = SdddSchurInfo()
+        self._check(self.L.sddd_schur_form(self.h, ctypes.byref(info), None, None, None), "sddd_schur_form")
+        if not info.sparse:
+            return info, None, None, None
+        order = np.zeros(info.m, np.int32)
+        di = np.zeros(info.m + 1, np.int32)
+        ci_ = np.zeros(max(1, info.nnz), np.int32)
+        self._check(self.L.sddd_schur_form(self.h, ctypes.byref(info), _ptr(order), _ptr(di), _ptr(ci_)), "sddd_schur_form")
+        return info, order, di, ci_[:info.nnz]
+
+    def sparse_factor_values(self, nnz):
+        """The sparse factor of the last Schur factorisation (reference layout)."""
+        out = np.zeros(nnz, DD)
+        self._check(self.L.sddd_sparse_factor_values(self.h, _ptr(out)), "sddd_sparse_factor_values")
+        return out
+
     def formula(self):
         out = np.zeros(self.m * self.nsdp, np.int32)
         self._check(self.L.sddd_formula(self.h, _ptr(out)), "formula")
@@ -319,6 +353,23 @@ class Batch:
         if rc != 0:
             raise SdddError(f"sddd_batch_grad_c failed ({rc})")
         return out
+
+
+def plan_schur(path, mode=0, sparse=True):
+    """The Schur form of a problem file (host only): (info, order,
+    diagonalIndex, column_index), the arrays None when B stays dense."""
+    L = lib()
+    info = SdddSchurInfo()
+    rc = L.sddd_plan_schur(str(path).encode(), 1 if sparse else 0, mode, ctypes.byref(info), None, None, None)
+    if rc != 0:
+        raise SdddError(L.sddd_last_error(None).decode())
+    if not info.sparse:
+        return info, None, None, None
+    order = np.zeros(info.m, np.int32)
+    di = np.zeros(info.m + 1, np.int32)
+    ci_ = np.zeros(max(1, info.nnz), np.int32)
+    L.sddd_plan_schur(str(path).encode(), 1 if sparse else 0, mode, ctypes.byref(info), _ptr(order), _ptr(di), _ptr(ci_))
+    return info, order, di, ci_[:info.nnz]
 
 
 def problem_info(path, sparse=True):

@@ -29,7 +29,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # dd arithmetic must round exactly as written: no contraction anywhere
 FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-ccbin", HOSTCXX,
                 "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-I", str(PKG.parent / "include")]
-LIB_SOURCES = ["prof.cu", "blas.cu", "schur.cu", "newton.cu", "eig.cu", "context.cu", "ddkern.cu", "noalloc.cu", "ozaki.cu", "ozaki_gemm.cu", "batched.cu", "trsv_blocked.cu", "adjoint.cu",
+LIB_SOURCES = ["prof.cu", "blas.cu", "schur.cu", "newton.cu", "eig.cu", "context.cu", "ddkern.cu", "noalloc.cu", "ozaki.cu", "ozaki_gemm.cu", "batched.cu", "trsv_blocked.cu", "adjoint.cu", "sparse_chol.cu", "sparse_schur.cpp",
                "problem.cpp", "solver.cpp", "capi.cpp", "cli.cpp", "batch.cpp"]
 
 

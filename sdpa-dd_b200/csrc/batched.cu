@@ -310,7 +310,7 @@ struct CoreEngine::Impl {
 };
 
 bool core_eligible(const Context &c) {
-    if (c.nSDP != 1 || c.tc_slices > 0 || c.m > CORE_MAX_M) return false;
+    if (c.nSDP != 1 || c.tc_slices > 0 || c.m > CORE_MAX_M || c.sparse_active()) return false;
     const BlockDev &bd = *c.blocks[0];
     return bd.n <= CORE_MAX_N && bd.nsparse == 0 && bd.nFG() == bd.nc && bd.fg_dense_contig && bd.nc == c.m;
 }

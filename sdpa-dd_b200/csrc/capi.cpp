@@ -15,6 +15,7 @@
 #include "newton.h"
 #include "prof.h"
 #include "solver.h"
+#include "sparse_chol.h"
 
 struct sddd_ctx {
     std::unique_ptr<sddd::Context> c;
@@ -810,6 +811,127 @@ int sddd_solve_stream(sddd_ctx *ctx, const sddd_param *param, FILE *disp, FILE *
         s.tm.total = total;
         s.print_last_info(disp, fo, total, "");
         if (mainLoop) *mainLoop = ml;
+        return SDDD_OK;
+    });
+}
+
+// ----------------------------------------------------- sparse Schur form
+namespace {
+void fill_form(const sddd::SparsePlan &pl, const sddd::TileSchedule *t, int m, sddd_schur_info *out, int *order, int *diagonalIndex, int *column_index) {
+    if (out) {
+        out->sparse = pl.sparse ? 1 : 0;
+        out->m = m;
+        out->aggregate = pl.aggregate;
+        out->extended = pl.extended;
+        out->nnz = pl.sparse ? pl.s.nnz() : 0;
+        out->ntiles = (pl.sparse && t) ? t->ntiles : 0;
+        std::snprintf(out->reason, sizeof(out->reason), "%s", pl.sparse ? "" : pl.dense_reason);
+    }
+    if (!pl.sparse) return;
+    if (order) std::copy(pl.order.begin(), pl.order.end(), order);
+    if (diagonalIndex) std::copy(pl.s.rowptr.begin(), pl.s.rowptr.end(), diagonalIndex);
+    if (column_index) std::copy(pl.s.col.begin(), pl.s.col.end(), column_index);
+}
+
+sddd::SparseStructure structure_from(int m, const int *diagonalIndex, const int *column_index) {
+    if (m < 0 || !diagonalIndex || (m > 0 && !column_index)) throw sddd::Error(SDDD_ERR_ARG, "sparse factor: m >= 0 and the structure arrays are required");
+    sddd::SparseStructure s;
+    s.m = m;
+    s.rowptr.assign(diagonalIndex, diagonalIndex + m + 1);
+    if (s.rowptr[m] < 0) throw sddd::Error(SDDD_ERR_ARG, "sparse factor: diagonalIndex[m] is negative");
+    s.col.assign(column_index, column_index + s.rowptr[m]);
+    return s;
+}
+
+// Sets the context's tiles up for a caller's structure, reusing the last one
+// when it is the same.
+void use_structure(sddd::Context &c, const sddd::SparseStructure &s) {
+    if (c.sp && c.sp->active && c.sp->plan.s.m == s.m && c.sp->plan.s.rowptr == s.rowptr && c.sp->plan.s.col == s.col && !c.have_problem) return;
+    if (c.have_problem) throw sddd::Error(SDDD_ERR_STATE, "sparse factor: the context holds a problem; use a context of its own");
+    sddd::sparse_setup_structure(c, s);
+}
+} // namespace
+
+int sddd_set_schur_mode(sddd_ctx *ctx, int mode) {
+    if (!ctx || !ctx->c || mode < 0 || mode > 2) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Context &c = *ctx->c;
+        c.schur_mode = mode;
+        if (c.have_problem) {
+            ctx->solver.reset();
+            sddd::sparse_setup(c);
+            c.chol_flops = c.sparse_active() ? 2.0 * (double)c.sp->sched.exact_terms : (double)c.m * c.m * c.m / 3.0;
+        }
+        return SDDD_OK;
+    });
+}
+
+int sddd_schur_form(const sddd_ctx *cctx, sddd_schur_info *out, int *order, int *diagonalIndex, int *column_index) {
+    sddd_ctx *ctx = const_cast<sddd_ctx *>(cctx);
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        if (!c.sp) throw sddd::Error(SDDD_ERR_STATE, "no Schur form planned");
+        fill_form(c.sp->plan, &c.sp->sched, c.m, out, order, diagonalIndex, column_index);
+        return SDDD_OK;
+    });
+}
+
+int sddd_plan_schur(const char *path, int sparse, int mode, sddd_schur_info *out, int *order, int *diagonalIndex, int *column_index) {
+    if (!path || mode < 0 || mode > 2) return SDDD_ERR_ARG;
+    return guarded(nullptr, [&] {
+        sddd::Problem p = sddd::read_problem(path, sparse != 0);
+        sddd::finalize_problem(p, 1.2);
+        const sddd::SparsePlan pl = sddd::plan_schur(p, mode);
+        if (pl.sparse) {
+            const sddd::TileSchedule t = sddd::make_tile_schedule(pl.s);
+            fill_form(pl, &t, p.m, out, order, diagonalIndex, column_index);
+        } else {
+            fill_form(pl, nullptr, p.m, out, order, diagonalIndex, column_index);
+        }
+        return SDDD_OK;
+    });
+}
+
+int sddd_sparse_factor_values(sddd_ctx *ctx, sddd_dd *sp_ele) {
+    if (!sp_ele) return SDDD_ERR_ARG;
+    return guarded(ctx, [&] {
+        sddd::Context &c = need_problem(ctx);
+        if (!c.sparse_active()) throw sddd::Error(SDDD_ERR_STATE, "the Schur matrix is dense");
+        const long nnz = c.sp->plan.s.nnz();
+        sddd::DBuf<dd_t> tmp;
+        tmp.alloc((size_t)std::max(1L, nnz));
+        sddd::sparse_values(c, tmp.p);
+        CK(cudaMemcpyAsync(sp_ele, tmp.p, sizeof(dd_t) * nnz, cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+        return SDDD_OK;
+    });
+}
+
+int sddd_sparse_getCholesky(sddd_ctx *ctx, int m, const int *diagonalIndex, const int *column_index, sddd_dd *sp_ele) {
+    return guarded(ctx, [&] {
+        if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
+        sddd::Context &c = *ctx->c;
+        const sddd::SparseStructure s = structure_from(m, diagonalIndex, column_index);
+        if (m == 0) return SDDD_OK;
+        if (!sp_ele) throw sddd::Error(SDDD_ERR_ARG, "sparse factor: sp_ele is required");
+        use_structure(c, s);
+        sddd::sparse_factor_values(c, reinterpret_cast<const dd_t *>(sp_ele));
+        sddd::sparse_values(c, reinterpret_cast<dd_t *>(sp_ele));
+        CK(cudaStreamSynchronize(c.stream));
+        return SDDD_OK;
+    });
+}
+
+int sddd_sparse_solveSystems(sddd_ctx *ctx, int m, const int *diagonalIndex, const int *column_index, const sddd_dd *sp_ele, sddd_dd *x) {
+    return guarded(ctx, [&] {
+        if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
+        sddd::Context &c = *ctx->c;
+        const sddd::SparseStructure s = structure_from(m, diagonalIndex, column_index);
+        if (m == 0) return SDDD_OK;
+        if (!sp_ele || !x) throw sddd::Error(SDDD_ERR_ARG, "sparse solve: sp_ele and x are required");
+        use_structure(c, s);
+        sddd::sparse_load_values(c, reinterpret_cast<const dd_t *>(sp_ele));
+        sddd::sparse_solve_raw(c, reinterpret_cast<dd_t *>(x));
         return SDDD_OK;
     });
 }

@@ -180,8 +180,15 @@ extern "C" int sddd_cli_main(int argc, char **argv) {
         std::fclose(fo);
         return 1;
     }
-    std::printf("DENSE computations\n");
-    std::fprintf(fo, "DENSE computation\n");
+    // Newton::initialize_bMat's report (sdpa_newton.cpp:345-391)
+    sddd_schur_info form{};
+    if (sddd_schur_form(ctx, &form, nullptr, nullptr, nullptr) == SDDD_OK && form.sparse) {
+        std::printf("SPARSE computation\n");
+        std::fprintf(fo, "SPARSE computation\n");
+    } else {
+        std::printf("DENSE computations\n");
+        std::fprintf(fo, "DENSE computation\n");
+    }
     const double fileRead = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     sddd_param p;
     p.maxIteration = param.maxIteration;

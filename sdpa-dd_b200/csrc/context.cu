@@ -1,6 +1,7 @@
 // Upload of the problem into its device layout and allocation of the
 // solver state (see context.h).
 #include "context.h"
+#include "sparse_chol.h"
 
 #include <algorithm>
 #include <cstring>
@@ -39,7 +40,10 @@ BlockView BlockDev::view() const {
     return v;
 }
 
+bool Context::sparse_active() const { return sp && sp->active; }
+
 Context::~Context() {
+    delete sp;
     if (tc.ev_pre) cudaEventDestroy(tc.ev_pre);
     if (tc.ev_diag) cudaEventDestroy(tc.ev_diag);
     if (tc.side) cudaStreamDestroy(tc.side);
@@ -407,6 +411,8 @@ void upload_problem(Context &c, Problem &&p) {
     c.cb_t.upload(tt, c.stream);
     c.b.upload(P.b, c.stream);
     alloc_state(c);
+    sparse_setup(c);
+    if (c.sparse_active()) c.chol_flops = 2.0 * (double)c.sp->sched.exact_terms;
     CK(cudaStreamSynchronize(c.stream));
     c.adj_valid = false;
     c.has_init = false;

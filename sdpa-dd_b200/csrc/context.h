@@ -119,6 +119,7 @@ struct Space {
 };
 
 class CoreEngine;
+struct SparseDev;
 
 struct Context {
     int device = 0;
@@ -220,6 +221,12 @@ struct Context {
     DBuf<double> lim_offr;
     // algorithmic dd-flop counts of one Make_bMat and one Cholesky of B
     double schur_flops = 0, chol_flops = 0;
+    // Schur form: SchurMode of sparse_schur.h (the reference's thresholds,
+    // always dense, always sparse) and, when B is sparse, its ordering,
+    // symbolic factor and tiles (sparse_chol.h)
+    int schur_mode = 0;
+    SparseDev *sp = nullptr;
+    bool sparse_active() const;
     ~Context();
 };
 

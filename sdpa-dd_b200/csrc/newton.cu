@@ -6,6 +6,7 @@
 
 #include "blas.h"
 #include "devops.cuh"
+#include "sparse_chol.h"
 
 namespace sddd {
 
@@ -162,6 +163,13 @@ void make_rhs(Context &c, bool corrector, dd_t beta_mu, bool dual_infeasible) {
 }
 
 int schur_factor(Context &c) {
+    if (c.sparse_active()) {
+        // Lal::getCholesky(SparseMatrix&, int*) reports no failure: a
+        // negative pivot becomes a zero row (sdpa_linear.cpp:366-372)
+        c.winv_valid = false;
+        sparse_factor_B(c);
+        return 0;
+    }
     CK(cudaMemsetAsync(c.info.p, 0, sizeof(int), c.stream));
     OzakiWork *tc = c.tc_slices > 0 ? &tc_work(c, c.m, c.tc_slices) : nullptr;
     c.winv_valid = false;
@@ -181,6 +189,10 @@ int schur_factor(Context &c) {
 }
 
 void solve_B(Context &c, dd_t *x) {
+    if (c.sparse_active()) {
+        sparse_solve(c, x);
+        return;
+    }
     TrsvSync &sync = trsv_sync(c, c.m);
     if (c.winv_valid) {
         trsv_blocked(c.stream, 'N', c.B.p, c.m, c.m, c.trsv_winv.p, x, sync);

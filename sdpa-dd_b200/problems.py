@@ -38,6 +38,7 @@ __all__ = [
     "control_like",
     "batch",
     "workload",
+    "chain_blocks",
     "write_param",
     "WORKLOADS",
 ]
@@ -173,6 +174,69 @@ def blocks_with_lp(sizes=(30,), q: int = 0, m: int = 40, seed: int = 8) -> str:
         if q > 0:
             nz = np.nonzero(a[k])[0]
             w.entries(k + 1, len(sizes) + 1, nz, nz, a[k, nz])
+    return w.text()
+
+
+def chain_blocks(nblocks: int = 40, n: int = 10, per: int = 4, overlap: int = 2, q: int = 0, seed: int = 9) -> str:
+    """SDP blocks in a chain: block b has `per` constraints of its own and
+    shares `overlap` constraints with block b+1 (dense N(0,1)/sqrt(n) data on
+    each block a constraint touches); with q > 0, q LP entries, entry t on
+    the constraints of block t % nblocks.  The constraints are numbered in a
+    random order, so the Schur matrix is a permuted band: more than 5 blocks,
+    m > 100 and a sparse aggregate pattern put it on the reference's sparse
+    Schur path.  Strictly feasible on both sides (x0 ~ N(0,1) primal, Y = I
+    and y_lp = 1 dual) as the other generators."""
+    rng = np.random.default_rng(seed)
+    touch: list[list[int]] = []  # blocks of each constraint, natural order
+    for b in range(nblocks):
+        touch += [[b] for _ in range(per)]
+        if b + 1 < nblocks:
+            touch += [[b, b + 1] for _ in range(overlap)]
+    m = len(touch)
+    perm = rng.permutation(m)  # natural constraint t gets index perm[t]
+    blocks_of = [None] * m
+    for t in range(m):
+        blocks_of[perm[t]] = touch[t]
+    x0 = rng.standard_normal(m)
+    c = np.zeros(m)
+    Fk = [dict() for _ in range(m)]  # per constraint: block -> matrix
+    F0 = []
+    s = 1.0 / np.sqrt(n)
+    for b in range(nblocks):
+        X0 = np.eye(n)
+        G = rng.standard_normal((n, n))
+        X0 = X0 + G @ G.T / n
+        acc = -X0
+        for k in range(m):
+            if b in blocks_of[k]:
+                A = rng.standard_normal((n, n)) * s
+                A = 0.5 * (A + A.T)
+                Fk[k][b] = A
+                acc = acc + x0[k] * A
+                c[k] += np.trace(A)
+        F0.append(acc)
+    lp = []
+    if q > 0:
+        for t in range(q):
+            b = t % nblocks
+            ks = [k for k in range(m) if b in blocks_of[k]]
+            a = {k: float(rng.standard_normal()) for k in ks if rng.random() < 0.5}
+            f0 = sum(x0[k] * v for k, v in a.items()) - (1.0 + rng.random())
+            for k, v in a.items():
+                c[k] += v
+            lp.append((a, f0))
+    blocks = [n] * nblocks + ([-q] if q > 0 else [])
+    w = _Writer(m, blocks, c, f"chain of {nblocks} SDP blocks n={n} per={per} overlap={overlap} LP {q} m={m} seed={seed}")
+    for b in range(nblocks):
+        w.dense_upper(0, b + 1, F0[b])
+    if q > 0:
+        w.entries(0, nblocks + 1, range(q), range(q), [f0 for _, f0 in lp])
+    for k in range(m):
+        for b in sorted(Fk[k]):
+            w.dense_upper(k + 1, b + 1, Fk[k][b])
+        if q > 0:
+            ts = [t for t in range(q) if k in lp[t][0]]
+            w.entries(k + 1, nblocks + 1, ts, ts, [lp[t][0][k] for t in ts])
     return w.text()
 
 
