@@ -50,6 +50,9 @@ SMALL_THETA = dict(name="theta", nv=120, p=0.5, seed=2)  # m = 3571
 # the other full-size shapes, solved to gap 1e-25 beside the headline
 MAXCUT = dict(name="maxcut", n=500, p=0.02, seed=1)  # n = m = 500, F3 Schur
 CONTROL = dict(name="control", sizes=(100, 50), m=1326, seed=3)  # F1 Schur
+# 200 SDP blocks of order 20 in a chain (m = 5990): the reference's sparse
+# Schur path (more than 5 blocks, a sparse aggregate pattern)
+CHAIN = dict(name="chain", nblocks=200, n=20, per=20, overlap=10, seed=31)
 EPS = 1e-25
 
 
@@ -75,6 +78,9 @@ def workload_label(w):
         return f"theta-shaped SDP nv={w['nv']} p={w['p']} seed={w['seed']}"
     if w["name"] == "maxcut":
         return f"max-cut-shaped SDP n={w['n']} p={w['p']} seed={w['seed']}"
+    if w["name"] == "chain":
+        return (f"chain of {w['nblocks']} SDP blocks of order {w['n']} ({w['per']} own and {w['overlap']} shared constraints per block, "
+                f"seed {w['seed']}; sparse Schur)")
     return f"control-shaped SDP blocks {w['sizes']} m={w['m']} seed={w['seed']}"
 
 
@@ -87,6 +93,8 @@ def write_workload(w, directory):
             text = P.theta(nv=w["nv"], p=w["p"], seed=w["seed"])
         elif w["name"] == "maxcut":
             text = P.maxcut(n=w["n"], p=w["p"], seed=w["seed"])
+        elif w["name"] == "chain":
+            text = P.chain_blocks(nblocks=w["nblocks"], n=w["n"], per=w["per"], overlap=w["overlap"], seed=w["seed"])
         else:
             text = P.control_like(sizes=w["sizes"], m=w["m"], seed=w["seed"])
         tmp = str(path) + f".tmp{os.getpid()}"
@@ -331,13 +339,18 @@ def _dd_dec(v):
     return Decimal(v.hi) + Decimal(v.lo)
 
 
+KERNELS_ALL = ("schur_build", "schur_pairs_tc", "potrf_diag", "potrf_diag_pre", "potrf_panel", "potrf_trailing_update",
+               "potrf_trailing_update_tc", "trsv", "trsv_diag_inverse", "sparse_factor", "sparse_solve", "min_eig")
+
+
 def other_solves(sddd, args, local, world):
-    """The max-cut (n = m = 500) and control-shaped (blocks 100 + 50, m =
-    1326) workloads solved to relative gap 1e-25 in both forms, each against
-    the reference build's own solve of the same file (one OpenMP thread,
-    tests/golden/large_solves.json: phase, iterations, dd objectives) and
-    its time to gap on the host cores (iterations x one timed pass of its
-    stock main loop)."""
+    """The max-cut (n = m = 500), control-shaped (blocks 100 + 50, m = 1326)
+    and chain (200 blocks, m = 5990, sparse Schur) workloads solved to
+    relative gap 1e-25 in each form, against the reference build's own
+    solve of the same file (one OpenMP thread, tests/golden/*.json: phase,
+    iterations, dd objectives) and its time to gap on the host cores
+    (iterations x one timed pass of its stock main loop); beside them, one
+    profiled solve's device time per iteration by phase."""
     import torch
     golden = {}
     gfile = ROOT / "tests" / "golden" / "large_solves.json"
@@ -346,19 +359,37 @@ def other_solves(sddd, args, local, world):
     out = {}
     workdir = pathlib.Path(tempfile.gettempdir()) / f"sddd_bench_{os.getuid()}_{local}"
     workdir.mkdir(exist_ok=True)
-    for key, w, gname in (("maxcut_n500", MAXCUT, "maxcut_n500"), ("control_100_50_m1326", CONTROL, "control_100_50_m1326")):
+    sfile = ROOT / "tests" / "golden" / "sparse_schur.json"
+    if sfile.exists():
+        for k, v in json.loads(sfile.read_text())["cases"].items():
+            d = v[0]
+            golden[k] = {"phase": d["phase"], "iterations": d["iterations"], "eps": 1e-20,
+                         "objValPrimal": [d["objValPrimal32"], "0"], "objValDual": [d["objValDual32"], "0"]}
+    forms = {"maxcut_n500": (("tc_split", args.tc, 0), ("plain", 0, 0)),
+             "control_100_50_m1326": (("tc_split", args.tc, 0), ("plain", 0, 0)),
+             "chain200_n20": (("sparse", 0, 0), ("dense_tc_split", args.tc, 1), ("dense_plain", 0, 1))}
+    for key, w, gname in (("maxcut_n500", MAXCUT, "maxcut_n500"), ("control_100_50_m1326", CONTROL, "control_100_50_m1326"),
+                          ("chain200_n20", CHAIN, "chain200_n20")):
         data, param_path = write_workload(w, workdir)
+        g = golden.get(gname)
+        if g and g.get("eps"):
+            param_path = problems().write_param(str(workdir / f"bench_{key}.param"), eps=g["eps"])
         par = sddd.param(param_path)
         ent = {"workload": workload_label(w)}
-        g = golden.get(gname)
+        if g and g.get("eps"):
+            ent["eps"] = g["eps"]
         with sddd.Context(local) as c:
             c.read_problem(data, sparse=True, kappa=1.2)
             ent["m"] = c.m
-            for label, slices in (("tc_split", args.tc), ("plain", 0)):
-                if label == "tc_split" and not args.tc:
+            for label, slices, mode in forms[key]:
+                if slices == 0 and label.endswith("tc_split"):
                     continue
                 if c.L.sddd_set_tc_split(c.h, slices) != 0:
                     raise RuntimeError(c.L.sddd_last_error(c.h).decode())
+                c.set_schur_mode(mode)
+                form = c.schur_form()[0]
+                if form.sparse:
+                    ent["schur_form"] = {"sparse": True, "nnz_factor": form.nnz, "tiles": form.ntiles, "aggregate": form.aggregate}
                 barrier(world)
                 torch.cuda.synchronize()
                 t1 = time.perf_counter()
@@ -372,8 +403,24 @@ def other_solves(sddd, args, local, world):
                         want = Decimal(g[nm][0]) + Decimal(g[nm][1])
                         e[f"{nm}_rel_diff_vs_reference"] = float(abs(_dd_dec(getattr(r, nm)) - want) / max(abs(want), Decimal(1)))
                 ent[label] = e
+            # one profiled solve of the first form: device ms per iteration by phase
+            label, slices, mode = forms[key][0]
+            c.L.sddd_set_tc_split(c.h, slices)
+            c.set_schur_mode(mode)
+            c.L.sddd_profile(c.h, 1)
+            c.L.sddd_profile_reset(c.h)
+            r = c.solve(par)
+            ph = {}
+            for name in KERNELS_ALL:
+                t, n = ctypes.c_double(), ctypes.c_long()
+                c.L.sddd_profile_read(c.h, name.encode(), ctypes.byref(t), ctypes.byref(n))
+                if n.value:
+                    ph[name] = round(t.value / max(1, r.iterations), 3)
+            c.L.sddd_profile(c.h, 0)
+            ent["phase_ms_per_iteration"] = {"form": label, **ph}
         if g:
-            ent["reference"] = {"phase": g["phase"], "iterations": g["iterations"], "source": "tests/golden/large_solves.json (one OpenMP thread)"}
+            src = "tests/golden/sparse_schur.json" if key.startswith("chain") else "tests/golden/large_solves.json"
+            ent["reference"] = {"phase": g["phase"], "iterations": g["iterations"], "source": f"{src} (one OpenMP thread)"}
         if local == 0 and not args.no_cpu_baseline and g:
             res, why = cpu_reference(w, 0, 1, os.cpu_count() or 1)
             if res is not None:

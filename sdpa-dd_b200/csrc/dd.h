@@ -256,6 +256,25 @@ DD_HD dd_t dd_sqrt(dd_t a) {
     return dd_add_dd_exact(ax, mul(d.hi, mul(x, 0.5)));
 }
 
+// 10^p as QD's npwr(10, p) forms it (src/dd_real.cpp): for |p| > 1 the
+// binary powers of 10 (QD's sqr) multiplied in ("*=" shape) where p has a
+// bit, for |p| == 1 ten itself; for p < 0 one division of 1 by the power.
+DD_HD dd_t dd_pow10(int p) {
+    if (p == 0) return dd_from(1.0);
+    const dd_t ten = dd_from(10.0);
+    unsigned bits = (unsigned)(p < 0 ? -p : p);
+    dd_t power = ten;
+    if (bits > 1) {
+        dd_t acc = dd_from(1.0), base = ten;
+        for (; bits != 0; bits >>= 1) {
+            if (bits & 1u) acc = dd_muleq(acc, base);
+            if (bits > 1) base = dd_sqr(base);
+        }
+        power = acc;
+    }
+    return p < 0 ? dd_div(dd_from(1.0), power) : power;
+}
+
 // ----------------------------------------------------------- comparisons
 DD_HD bool dd_lt(dd_t a, dd_t b) { return a.hi < b.hi || (a.hi == b.hi && a.lo < b.lo); }
 DD_HD bool dd_gt(dd_t a, dd_t b) { return a.hi > b.hi || (a.hi == b.hi && a.lo > b.lo); }

@@ -21,63 +21,53 @@ long Problem::nDim() const {
 }
 
 // ------------------------------------------------------------ decimal reader
-// QD's dd_real::read: digits accumulate as r = r*10 + d (operator*=(double),
-// operator+=(double)), then one multiplication by 10^e where the power is
-// QD's npwr (binary powering with operator*= and sqr, reciprocal for e < 0).
-static dd_t npwr(dd_t a, int n) {
-    if (n == 0) return dd_from(1.0);
-    dd_t r = a, s = dd_from(1.0);
-    int N = std::abs(n);
-    if (N > 1) {
-        while (N > 0) {
-            if (N % 2 == 1) s = dd_muleq(s, r);
-            N /= 2;
-            if (N > 0) r = dd_sqr(r);
-        }
-    } else {
-        s = r;
-    }
-    if (n < 0) return dd_div(dd_from(1.0), s);
-    return s;
-}
+// The value of a decimal string exactly as the reference's dd library reads
+// it (QD 2.3.23, dd_real::read and npwr in src/dd_real.cpp; QD is
+// Copyright (c) 2003-2009 The Regents of the University of California,
+// through Lawrence Berkeley National Laboratory, under a modified BSD
+// licence).  Bit-identical input needs its rounding steps: every mantissa
+// digit folds in as v*10 (dd times double) then + digit (dd plus double),
+// and the decimal exponent scales the result once, by 10^|e| built from
+// repeated squaring (multiplications of the "*=" shape, squares of QD's sqr)
+// and, for e < 0, one dd division of 1 by it.
 
-int dd_read(const char *s, dd_t *out) {
-    const char *p = s;
-    int sign = 0, point = -1, nd = 0, e = 0;
-    bool done = false;
-    dd_t r = dd_zero();
-    while (*p == ' ') p++;
-    while (!done && *p != '\0') {
-        char ch = *p;
-        if (ch >= '0' && ch <= '9') {
-            r = dd_mul_d(r, 10.0);
-            r = dd_add_d(r, (double)(ch - '0'));
-            nd++;
-        } else {
-            switch (ch) {
-            case '.':
-                if (point >= 0) return -1;
-                point = nd;
-                break;
-            case '-':
-            case '+':
-                if (sign != 0 || nd > 0) return -1;
-                sign = (ch == '-') ? -1 : 1;
-                break;
-            case 'E':
-            case 'e':
-                if (std::sscanf(p + 1, "%d", &e) != 1) return -1;
-                done = true;
-                break;
-            default:
-                return -1;
-            }
+// Grammar (QD's): leading blanks; then a sequence of digits, at most one
+// '.', one sign before the first digit, and optionally 'e'/'E' followed by
+// an integer as sscanf("%d") reads it, which ends the scan; anything else
+// is an error (-1).
+int dd_read(const char *text, dd_t *out) {
+    const char *c = text;
+    while (*c == ' ') ++c;
+    dd_t mant = dd_zero();
+    int ndigits = 0, point_at = -1, exp10 = 0;
+    bool negative = false, signed_ = false;
+    for (; *c != '\0'; ++c) {
+        const char ch = *c;
+        if (std::isdigit((unsigned char)ch)) {
+            mant = dd_add_d(dd_mul_d(mant, 10.0), (double)(ch - '0'));
+            ++ndigits;
+            continue;
         }
-        p++;
+        if (ch == '.') {
+            if (point_at >= 0) return -1;
+            point_at = ndigits;
+            continue;
+        }
+        if (ch == '+' || ch == '-') {
+            if (signed_ || ndigits > 0) return -1;
+            signed_ = true;
+            negative = ch == '-';
+            continue;
+        }
+        if (ch == 'e' || ch == 'E') {
+            if (std::sscanf(c + 1, "%d", &exp10) != 1) return -1;
+            break;
+        }
+        return -1;
     }
-    if (point >= 0) e -= (nd - point);
-    if (e != 0) r = dd_muleq(r, npwr(dd_from(10.0), e));
-    *out = (sign == -1) ? dd_neg(r) : r;
+    if (point_at >= 0) exp10 -= ndigits - point_at;
+    if (exp10 != 0) mant = dd_muleq(mant, dd_pow10(exp10));
+    *out = negative ? dd_neg(mant) : mant;
     return 0;
 }
 

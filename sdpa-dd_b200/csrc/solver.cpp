@@ -405,23 +405,13 @@ void Solver::print_one_iteration(FILE *fp) {
 }
 
 // -------------------------------------------------------- QD decimal output
-static dd_t npwr10(int e) {
-    // dd_real(10.0) ^ e (npwr)
-    dd_t r = dd_from(10.0), s = ONE;
-    int N = std::abs(e);
-    if (N == 0) return ONE;
-    if (N > 1) {
-        while (N > 0) {
-            if (N % 2 == 1) s = dd_muleq(s, r);
-            N /= 2;
-            if (N > 0) r = dd_sqr(r);
-        }
-    } else {
-        s = r;
-    }
-    if (e < 0) return dd_div(ONE, s);
-    return s;
-}
+// The reference prints dd values with QD 2.3.23's dd_real::to_digits /
+// to_string (src/dd_real.cpp; Copyright (c) 2003-2009 The Regents of the
+// University of California, through Lawrence Berkeley National Laboratory,
+// modified BSD licence).  Identical digits need its steps: scale by a power
+// of ten into [1, 10), peel precision + 1 digits by truncation and *10,
+// settle digits outside 0..9 by borrow and carry, round on the last digit.
+static dd_t npwr10(int e) { return dd_pow10(e); }
 
 static void to_digits(dd_t a, char *s, int &expn, int precision) {
     const int D = precision + 1;

@@ -35,6 +35,8 @@ CASES = {
     "chain40": lambda: P.chain_blocks(nblocks=40, n=10, per=4, overlap=2, q=0, seed=9),
     "chain40_lp30": lambda: P.chain_blocks(nblocks=40, n=10, per=4, overlap=2, q=30, seed=12),
     "chain150": lambda: P.chain_blocks(nblocks=150, n=8, per=6, overlap=3, q=0, seed=21),
+    # the bench's sparse-Schur workload (m = 5990)
+    "chain200_n20": lambda: P.chain_blocks(nblocks=200, n=20, per=20, overlap=10, q=0, seed=31),
 }
 
 
