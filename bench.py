@@ -689,6 +689,36 @@ def profile_case(args):
     return 0 if info == 0 else 1
 
 
+def profile_case_sparse(args):
+    """One sparse factorisation and solve (sddd_sparse_getCholesky /
+    sddd_sparse_solveSystems) of the chain workload's Schur structure with
+    random positive definite entries, for an ncu capture; prints its time."""
+    sddd = load_pkg()
+    L = sddd.lib()
+    import numpy as np
+    import torch
+    workdir = pathlib.Path(tempfile.gettempdir()) / f"sddd_bench_{os.getuid()}_sp"
+    workdir.mkdir(exist_ok=True)
+    data, _ = write_workload(CHAIN, workdir)
+    info, order, di, ci = sddd.plan_schur(data)
+    m, nnz = info.m, info.nnz
+    rng = np.random.default_rng(5)
+    v = rng.standard_normal((nnz, 2)) * np.array([0.1, 1e-18])
+    v[di[:-1], 0] = 4.0 + 10.0 * np.abs(rng.standard_normal(m))
+    v[di[:-1], 1] = 0.0
+    dv = torch.from_numpy(v.reshape(-1).copy()).cuda()
+    dx = torch.from_numpy(np.stack([rng.standard_normal(m), np.zeros(m)], 1).reshape(-1).copy()).cuda()
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    with sddd.Context(0) as ctx:
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        rc = L.sddd_sparse_getCholesky(ctx.h, m, p(di), p(ci), ctypes.c_void_p(dv.data_ptr()))
+        rc2 = L.sddd_sparse_solveSystems(ctx.h, m, p(di), p(ci), ctypes.c_void_p(dv.data_ptr()), ctypes.c_void_p(dx.data_ptr()))
+        torch.cuda.synchronize()
+        print(json.dumps({"case": "sparse", "m": m, "nnz": nnz, "tiles": info.ntiles, "rc": [rc, rc2], "s": time.perf_counter() - t}))
+    return 0 if rc == 0 and rc2 == 0 else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -696,7 +726,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-case", choices=["potrf"], help="run one kernel-level case for an ncu capture and exit")
+    ap.add_argument("--profile-case", choices=["potrf", "sparse"], help="run one kernel-level case for an ncu capture and exit")
     ap.add_argument("--m", type=int, default=4096)
     ap.add_argument("--tc", type=int, default=16, help="slices of the tensor-core split Cholesky (8..16; 0 = plain dd only)")
     ap.add_argument("--no-solve", action="store_true", help="skip the two solves to relative gap 1e-25")
@@ -704,6 +734,8 @@ def main():
     ap.add_argument("--batch-workers", type=int, default=0, help="host workers of the batched workload (0: the library's default)")
     ap.add_argument("--batch-only", action="store_true", help="run the batched workload alone and print its figures")
     args = ap.parse_args()
+    if args.profile_case == "sparse":
+        return profile_case_sparse(args)
     if args.profile_case:
         return profile_case(args)
     if args.warmup < 3:

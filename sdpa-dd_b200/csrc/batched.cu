@@ -331,22 +331,25 @@ CoreEngine::CoreEngine(int device) : p(new Impl) {
     for (auto &row : p->per_term)
         for (double &v : row) v = -1.0;
     // the graph: descriptor copy, zero, F, G, the pair products of each
-    // shape between event nodes, the factorisations
+    // shape between event-record nodes (recorded as external events, so
+    // that every launch of the graph records them and the autotuner can
+    // time the shapes; a plain record inside a capture only orders the
+    // graph), the factorisations
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
     cudaMemcpyAsync(p->db, p->hb, sizeof(CoreBatch), cudaMemcpyHostToDevice, p->stream);
     core_zero_kernel<<<dim3(8, CORE_CAP), 256, 0, p->stream>>>(p->db);
     core_fg_kernel<<<4 * p->sms, 256, 0, p->stream>>>(p->db, 0);
     core_fg_kernel<<<4 * p->sms, 256, 0, p->stream>>>(p->db, 1);
-    cudaEventRecord(p->ev_shape[0][0], p->stream);
+    cudaEventRecordWithFlags(p->ev_shape[0][0], p->stream, cudaEventRecordExternal);
     core_pairs_kernel<0, 16, 16, 32, 1, 1><<<8 * p->sms, 256, 0, p->stream>>>(p->db);
-    cudaEventRecord(p->ev_shape[0][1], p->stream);
-    cudaEventRecord(p->ev_shape[1][0], p->stream);
+    cudaEventRecordWithFlags(p->ev_shape[0][1], p->stream, cudaEventRecordExternal);
+    cudaEventRecordWithFlags(p->ev_shape[1][0], p->stream, cudaEventRecordExternal);
     core_pairs_kernel<1, 32, 32, 16, 2, 2><<<4 * p->sms, 256, 0, p->stream>>>(p->db);
-    cudaEventRecord(p->ev_shape[1][1], p->stream);
-    cudaEventRecord(p->ev_shape[2][0], p->stream);
+    cudaEventRecordWithFlags(p->ev_shape[1][1], p->stream, cudaEventRecordExternal);
+    cudaEventRecordWithFlags(p->ev_shape[2][0], p->stream, cudaEventRecordExternal);
     core_pairs_kernel<2, 64, 64, 16, 4, 4><<<2 * p->sms, 256, 0, p->stream>>>(p->db);
-    cudaEventRecord(p->ev_shape[2][1], p->stream);
+    cudaEventRecordWithFlags(p->ev_shape[2][1], p->stream, cudaEventRecordExternal);
     core_potrf_kernel<<<CORE_CAP, CORE_POTRF_THREADS, 0, p->stream>>>(p->db);
     cudaError_t cap = cudaStreamEndCapture(p->stream, &g);
     if (cap != cudaSuccess) throw Error(ERR_CUDA, std::string("batched core: graph capture failed: ") + cudaGetErrorString(cap));

@@ -167,6 +167,12 @@ void gemm(cudaStream_t st, char ta, char tb, int mode, int M, int N, int K, cons
           dd_t *C, long ldc, long sC, int batch, bool lower) {
     if (M <= 0 || N <= 0 || batch <= 0) return;
     if (K <= 0 && mode == GEMM_SUB) return;
+    if (batch > MAX_GRID_YZ) {
+        // grid.z holds at most 65535 matrices per launch
+        for (int b0 = 0; b0 < batch; b0 += MAX_GRID_YZ)
+            gemm(st, ta, tb, mode, M, N, K, A + b0 * sA, lda, sA, B + b0 * sB, ldb, sB, C + b0 * sC, ldc, sC, std::min(MAX_GRID_YZ, batch - b0), lower);
+        return;
+    }
 #define GL(TA_, TB_, MD_) gemm_launch<TA_, TB_, MD_>(st, M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, batch, lower)
     bool a = ta == 'T', b = tb == 'T';
     if (mode == GEMM_STORE) {
@@ -198,10 +204,11 @@ void gemm(cudaStream_t st, char ta, char tb, int mode, int M, int N, int K, cons
 // entry sees the same operations in the same order as the column-by-column
 // form: x(i,j) -= L(j,k) L(i,k) for k ascending, then the scaling.
 constexpr int DIAG_THREADS = 1024;
-__global__ void __launch_bounds__(DIAG_THREADS) potrf_diag_kernel(dd_t *A, long lda, int nb, int c0, int *info, dd_t *rdiag) {
+__global__ void __launch_bounds__(DIAG_THREADS) potrf_diag_kernel(dd_t *A, long lda, int nb, int c0, int *info, dd_t *rdiag, long sA) {
     extern __shared__ double2 sm[];
     double2 *S = sm; // nb x nb, column-major
     __shared__ int fail;
+    A += blockIdx.x * sA; // CTA b: matrix b of a batch of equal blocks (rdiag null then)
     if (*info != 0) return;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     for (int e = tid; e < nb * nb; e += nt) {
@@ -229,7 +236,7 @@ __global__ void __launch_bounds__(DIAG_THREADS) potrf_diag_kernel(dd_t *A, long 
                 const dd_t l = dd_sqrt(d);
                 put(col, col, l);
                 const dd_t r = dd_div(dd_from(1.0), l);
-                rdiag[col] = r;
+                if (rdiag) rdiag[col] = r;
                 rh = r.hi;
                 rl = r.lo;
             }
@@ -374,7 +381,7 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
         // block) runs; panel k+1 waits for both.
         {
             PROF_SCOPE("potrf_diag", st);
-            potrf_diag_kernel<<<1, DIAG_THREADS, sizeof(double2) * nbmax * nbmax, st>>>(A, lda, nbmax, 0, info_dev, rdiag_dev);
+            potrf_diag_kernel<<<1, DIAG_THREADS, sizeof(double2) * nbmax * nbmax, st>>>(A, lda, nbmax, 0, info_dev, rdiag_dev, 0);
             CK_LAUNCH();
         }
         for (int c0 = 0;; c0 += nbmax) {
@@ -397,7 +404,7 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
             CK(cudaStreamWaitEvent(tc->side, tc->ev_pre, 0));
             {
                 PROF_SCOPE("potrf_diag", tc->side);
-                potrf_diag_kernel<<<1, DIAG_THREADS, sizeof(double2) * nb1 * nb1, tc->side>>>(A, lda, nb1, c1, info_dev, rdiag_dev);
+                potrf_diag_kernel<<<1, DIAG_THREADS, sizeof(double2) * nb1 * nb1, tc->side>>>(A, lda, nb1, c1, info_dev, rdiag_dev, 0);
                 CK_LAUNCH();
             }
             CK(cudaEventRecord(tc->ev_diag, tc->side));
@@ -413,7 +420,7 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
         const int nb = std::min(nbmax, n - c0);
         {
             PROF_SCOPE("potrf_diag", st);
-            potrf_diag_kernel<<<1, DIAG_THREADS, sizeof(double2) * nb * nb, st>>>(A, lda, nb, c0, info_dev, rdiag_dev);
+            potrf_diag_kernel<<<1, DIAG_THREADS, sizeof(double2) * nb * nb, st>>>(A, lda, nb, c0, info_dev, rdiag_dev, 0);
             CK_LAUNCH();
         }
         const int below = n - c0 - nb;
@@ -436,15 +443,30 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
     }
 }
 
+void potrf_batched(cudaStream_t st, dd_t *A, long lda, int n, long sA, int batch, int *info_dev) {
+    if (n <= 0 || batch <= 0) return;
+    if (n > POTRF_NB) throw Error(ERR_ARG, "potrf_batched: order above one diagonal block");
+    const size_t smem = sizeof(double2) * n * n;
+    CK(cudaFuncSetAttribute(potrf_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(double2) * POTRF_NB * POTRF_NB)));
+    potrf_diag_kernel<<<batch, DIAG_THREADS, smem, st>>>(A, lda, n, 0, info_dev, nullptr, sA);
+    CK_LAUNCH();
+}
+
 // Zero the strict upper triangle (Lal::getCholesky, sdpa_linear.cpp:320-343).
-__global__ void zero_upper_kernel(dd_t *A, long lda, int n) {
+__global__ void zero_upper_kernel(dd_t *A, long lda, int n, long sA) {
     long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (e >= (long)n * n) return;
+    A += blockIdx.y * sA;
     int i = e % n, j = e / n;
     if (i < j) st_dd(A + i + lda * (long)j, dd_zero());
 }
-void zero_upper(cudaStream_t st, dd_t *A, long lda, int n) {
-    zero_upper_kernel<<<ceil_div((long)n * n, 256), 256, 0, st>>>(A, lda, n);
+void zero_upper(cudaStream_t st, dd_t *A, long lda, int n, int batch, long sA) {
+    if (n <= 0 || batch <= 0) return;
+    if (batch > MAX_GRID_YZ) {
+        for (int b0 = 0; b0 < batch; b0 += MAX_GRID_YZ) zero_upper(st, A + b0 * sA, lda, n, std::min(MAX_GRID_YZ, batch - b0), sA);
+        return;
+    }
+    zero_upper_kernel<<<dim3(ceil_div((long)n * n, 256), batch), 256, 0, st>>>(A, lda, n, sA);
     CK_LAUNCH();
 }
 
@@ -747,9 +769,11 @@ void trsv_check(cudaStream_t st, const TrsvSync &sync) {
 // ======================================================= triangular inverse
 // X = inv(L): one CTA per column j, right-looking over k = j..n-1
 // (Rtrsm "Left","Lower","N","N" on the identity).
-__global__ void inv_lower_kernel(const dd_t *L, long lda, int n, dd_t *X, long ldx) {
+__global__ void inv_lower_kernel(const dd_t *L, long lda, int n, dd_t *X, long ldx, long sL, long sX) {
     extern __shared__ double2 col[];
     const int j = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+    L += blockIdx.y * sL;
+    X += blockIdx.y * sX;
     for (int i = tid; i < n; i += nt) col[i] = make_double2(i == j ? 1.0 : 0.0, 0.0);
     __syncthreads();
     for (int k = j; k < n; ++k) {
@@ -771,36 +795,47 @@ __global__ void inv_lower_kernel(const dd_t *L, long lda, int n, dd_t *X, long l
     }
     for (int i = tid; i < n; i += nt) *reinterpret_cast<double2 *>(X + i + ldx * (long)j) = col[i];
 }
-void inv_lower(cudaStream_t st, const dd_t *L, long lda, int n, dd_t *X, long ldx) {
-    if (n <= 0) return;
+void inv_lower(cudaStream_t st, const dd_t *L, long lda, int n, dd_t *X, long ldx, int batch, long sL, long sX) {
+    if (n <= 0 || batch <= 0) return;
+    if (batch > MAX_GRID_YZ) {
+        for (int b0 = 0; b0 < batch; b0 += MAX_GRID_YZ) inv_lower(st, L + b0 * sL, lda, n, X + b0 * sX, ldx, std::min(MAX_GRID_YZ, batch - b0), sL, sX);
+        return;
+    }
     const size_t smem = sizeof(double2) * n;
     if (smem > 227 * 1024) throw Error(ERR_UNSUPPORTED, "inv_lower: block too large for one CTA");
     if (smem > 48 * 1024) CK(cudaFuncSetAttribute(inv_lower_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    inv_lower_kernel<<<n, 128, smem, st>>>(L, lda, n, X, ldx);
+    inv_lower_kernel<<<dim3(n, batch), 128, smem, st>>>(L, lda, n, X, ldx, sL, sX);
     CK_LAUNCH();
 }
 
 // B = M^T M for lower M, entry by entry as Rtrmm("L","L","T","N") does in
 // place: t = M(i,j) M(i,i); t += M(k,i) M(k,j), k = i+1..n-1 (terms with
 // M(k,j) = 0, k < j, add exact zeros and are skipped).
-__global__ void trmm_lt_kernel(const dd_t *M, long ldm, int n, dd_t *B, long ldb) {
+__global__ void trmm_lt_kernel(const dd_t *M, long ldm, int n, dd_t *B, long ldb, long sM, long sB) {
     long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (e >= (long)n * n) return;
+    M += blockIdx.y * sM;
+    B += blockIdx.y * sB;
     int i = e % n, j = e / n;
     dd_t t = dd_mul(ld_dd(M + i + ldm * (long)j), ld_dd(M + i + ldm * (long)i));
     for (int k = max(i + 1, j); k < n; ++k) t = dd_acc(t, dd_mul(ld_dd(M + k + ldm * (long)i), ld_dd(M + k + ldm * (long)j)));
     st_dd(B + i + ldb * (long)j, t);
 }
-void trmm_lt(cudaStream_t st, const dd_t *M, long ldm, int n, dd_t *B, long ldb) {
-    if (n <= 0) return;
-    trmm_lt_kernel<<<ceil_div((long)n * n, 128), 128, 0, st>>>(M, ldm, n, B, ldb);
+void trmm_lt(cudaStream_t st, const dd_t *M, long ldm, int n, dd_t *B, long ldb, int batch, long sM, long sB) {
+    if (n <= 0 || batch <= 0) return;
+    if (batch > MAX_GRID_YZ) {
+        for (int b0 = 0; b0 < batch; b0 += MAX_GRID_YZ) trmm_lt(st, M + b0 * sM, ldm, n, B + b0 * sB, ldb, std::min(MAX_GRID_YZ, batch - b0), sM, sB);
+        return;
+    }
+    trmm_lt_kernel<<<dim3(ceil_div((long)n * n, 128), batch), 128, 0, st>>>(M, ldm, n, B, ldb, sM, sB);
     CK_LAUNCH();
 }
 
 // =============================================================== symmetrize
-__global__ void symmetrize_kernel(dd_t *A, int n) {
+__global__ void symmetrize_kernel(dd_t *A, int n, long sA) {
     long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (e >= (long)n * n) return;
+    A += blockIdx.y * sA;
     int i = e % n, c = e / n;
     if (i <= c) return;
     dd_t v = dd_acc(ld_dd(A + i + (long)n * c), ld_dd(A + c + (long)n * i));
@@ -808,9 +843,13 @@ __global__ void symmetrize_kernel(dd_t *A, int n) {
     st_dd(A + i + (long)n * c, v);
     st_dd(A + c + (long)n * i, v);
 }
-void symmetrize(cudaStream_t st, dd_t *A, int n) {
-    if (n <= 1) return;
-    symmetrize_kernel<<<ceil_div((long)n * n, 256), 256, 0, st>>>(A, n);
+void symmetrize(cudaStream_t st, dd_t *A, int n, int batch, long sA) {
+    if (n <= 1 || batch <= 0) return;
+    if (batch > MAX_GRID_YZ) {
+        for (int b0 = 0; b0 < batch; b0 += MAX_GRID_YZ) symmetrize(st, A + b0 * sA, n, std::min(MAX_GRID_YZ, batch - b0), sA);
+        return;
+    }
+    symmetrize_kernel<<<dim3(ceil_div((long)n * n, 256), batch), 256, 0, st>>>(A, n, sA);
     CK_LAUNCH();
 }
 
@@ -876,6 +915,17 @@ __global__ void dot_seq_kernel(const dd_t *x, long incx, const dd_t *y, long inc
     st_dd(out, dd_acc(dd_zero(), t));
 }
 
+// Chains of a batch of equal-length dot products: CTA b, x + b sx, y + b
+// sy, result out[b].
+__global__ void dot_seq_batch_kernel(const dd_t *x, long sx, const dd_t *y, long sy, long n, dd_t *out) {
+    if (threadIdx.x != 0) return;
+    x += blockIdx.x * sx;
+    y += blockIdx.x * sy;
+    dd_t t = dd_zero();
+    for (long i = 0; i < n; ++i) t = dd_acc(t, dd_mul(ld_dd(x + i), ld_dd(y + i)));
+    st_dd(out + blockIdx.x, dd_acc(dd_zero(), t));
+}
+
 __device__ dd_t block_tree(dd_t v, double2 *sh) {
     const int tid = threadIdx.x;
     sh[tid] = make_double2(v.hi, v.lo);
@@ -920,6 +970,16 @@ void dot(cudaStream_t st, const dd_t *x, long incx, const dd_t *y, long incy, lo
     CK_LAUNCH();
     tree_final_kernel<<<1, DOT_THREADS, 0, st>>>(scratch, nb, out);
     CK_LAUNCH();
+}
+
+void dot_batched(cudaStream_t st, const dd_t *x, long sx, const dd_t *y, long sy, long n, int batch, dd_t *out, dd_t *scratch) {
+    if (batch <= 0) return;
+    if (n <= DOT_SEQ) {
+        dot_seq_batch_kernel<<<batch, 32, 0, st>>>(x, sx, y, sy, n, out);
+        CK_LAUNCH();
+        return;
+    }
+    for (int b = 0; b < batch; ++b) dot(st, x + b * sx, 1, y + b * sy, 1, n, out + b, scratch + 256 * (b % 8));
 }
 
 // max |x_i| (Residuals::computeMaxNorm) - exact in any order.

@@ -9,6 +9,7 @@ struct OzakiWork;
 
 enum GemmMode { GEMM_STORE = 0, GEMM_SUB = 1, GEMM_ACC = 2, GEMM_AB_PRE = 3, GEMM_AB_POST = 4 };
 constexpr int POTRF_NB = 64;
+constexpr int MAX_GRID_YZ = 65535; // largest grid.y / grid.z of one launch
 
 // C = op(A) op(B) (STORE: sum from zero; SUB: C - p_0 - p_1 - ...;
 // ACC: C + p_0 + ...), batched with strides, optionally the lower triangle
@@ -26,7 +27,11 @@ void gemm(cudaStream_t st, char ta, char tb, int mode, int M, int N, int K, cons
 void gemm_ab(cudaStream_t st, char ta, char tb, int M, int N, int K, dd_t alpha, const dd_t *A, long lda, const dd_t *B, long ldb, dd_t beta, dd_t *C,
              long ldc);
 void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag_dev, OzakiWork *tc = nullptr);
-void zero_upper(cudaStream_t st, dd_t *A, long lda, int n);
+void zero_upper(cudaStream_t st, dd_t *A, long lda, int n, int batch = 1, long sA = 0);
+// Rpotrf("Lower") of `batch` matrices of order n <= 64, matrix b at A + b sA,
+// one CTA each (the single diagonal block of potrf); any failure sets
+// *info_dev to a failing column.
+void potrf_batched(cudaStream_t st, dd_t *A, long lda, int n, long sA, int batch, int *info_dev);
 // Progress words of the one-launch triangular solve: one flag per 64-entry
 // block (the epoch of the solve that finished it), then an error word.
 // The owner zeroes them once; the epoch advances with every solve.
@@ -54,15 +59,18 @@ void trsv_diag_inverse(cudaStream_t st, const dd_t *L, long lda, int n, dd_t *W)
 // trsv_diag_inverse: one cooperative launch; the same progress words and
 // error reporting (trsv_check) as trsv_lower.  Not Rtrsv's operation order.
 void trsv_blocked(cudaStream_t st, char trans, const dd_t *L, long lda, int n, const dd_t *W, dd_t *x, TrsvSync &sync);
-void inv_lower(cudaStream_t st, const dd_t *L, long lda, int n, dd_t *X, long ldx);
-void trmm_lt(cudaStream_t st, const dd_t *M, long ldm, int n, dd_t *B, long ldb);
-void symmetrize(cudaStream_t st, dd_t *A, int n);
+void inv_lower(cudaStream_t st, const dd_t *L, long lda, int n, dd_t *X, long ldx, int batch = 1, long sL = 0, long sX = 0);
+void trmm_lt(cudaStream_t st, const dd_t *M, long ldm, int n, dd_t *B, long ldb, int batch = 1, long sM = 0, long sB = 0);
+void symmetrize(cudaStream_t st, dd_t *A, int n, int batch = 1, long sA = 0);
 void fill(cudaStream_t st, dd_t *x, long n, dd_t v);
 void scal(cudaStream_t st, dd_t *y, long n, dd_t a);
 void copy_scal(cudaStream_t st, const dd_t *x, dd_t *y, long n, dd_t a);
 void axpy(cudaStream_t st, const dd_t *x, const dd_t *y, dd_t *z, long n, dd_t a);
 // out = x.y (device scalar); scratch >= 256 dd
 void dot(cudaStream_t st, const dd_t *x, long incx, const dd_t *y, long incy, long n, dd_t *out, dd_t *scratch);
+// out[b] = dot(x + b sx, y + b sy) for b < batch (unit strides), each with
+// dot's own order.
+void dot_batched(cudaStream_t st, const dd_t *x, long sx, const dd_t *y, long sy, long n, int batch, dd_t *out, dd_t *scratch);
 void maxabs(cudaStream_t st, const dd_t *x, long n, dd_t *out, dd_t *scratch);
 
 } // namespace sddd

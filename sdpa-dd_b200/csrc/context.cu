@@ -384,6 +384,14 @@ void upload_problem(Context &c, Problem &&p) {
     c.off.assign(c.nSDP + 1, 0);
     for (int l = 0; l < c.nSDP; ++l) c.off[l + 1] = c.off[l] + (long)c.sizes[l] * c.sizes[l];
     c.space_len = c.off[c.nSDP];
+    c.c_slot_host.clear();
+    c.runs.clear();
+    for (int l = 0; l < c.nSDP; ++l) {
+        if (!c.runs.empty() && c.runs.back().n == c.sizes[l])
+            ++c.runs.back().count;
+        else
+            c.runs.push_back({l, 1, c.sizes[l]});
+    }
     // block objects (and their device buffers) are reused across uploads
     if ((int)c.blocks.size() > c.nSDP) c.blocks.resize(c.nSDP);
     while ((int)c.blocks.size() < c.nSDP) c.blocks.emplace_back(new BlockDev());

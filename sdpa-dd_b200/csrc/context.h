@@ -121,6 +121,13 @@ struct Space {
 class CoreEngine;
 struct SparseDev;
 
+// Consecutive SDP blocks of one order: they lie back to back in every
+// space (block first + t at off[first] + t n^2), so the per-block dense
+// kernels run once for the whole run with a batch stride of n^2.
+struct BlockRun {
+    int first, count, n;
+};
+
 struct Context {
     int device = 0;
     // a batch worker's batched Newton core (batched.h), or null; the event
@@ -145,6 +152,11 @@ struct Context {
     long nDim = 0;
     std::vector<int> sizes;
     std::vector<long> off; // block offsets within a space
+    std::vector<BlockRun> runs;
+    // result slot of each block with a C part (inner_C), built on first use
+    std::vector<int> c_slot_host;
+    DBuf<int> c_slot;
+    int c_nslots = 0;
     long space_len = 0;
     std::vector<std::unique_ptr<BlockDev>> blocks;
     DBuf<BlockView> views; // [l]

@@ -353,10 +353,12 @@ dd_t min_eig(Context &c, const Space &L, const Space &D) {
     }
     if (!small.empty()) {
         // DLS2 = D L^T (Rgemm "N","T"); DLS1 = L DLS2 (Rgemm "N","N")
-        for (int l : small) {
-            const int n = c.sizes[l];
-            gemm(st, 'N', 'T', GEMM_STORE, n, n, n, D.blk(c.off, l), n, 0, L.blk(c.off, l), n, 0, c.W2.blk(c.off, l), n, 0, 1, false);
-            gemm(st, 'N', 'N', GEMM_STORE, n, n, n, L.blk(c.off, l), n, 0, c.W2.blk(c.off, l), n, 0, c.W1.blk(c.off, l), n, 0, 1, false);
+        for (const BlockRun &r : c.runs) {
+            if (r.n > 20) continue;
+            const int n = r.n, l = r.first;
+            const long nn = (long)n * n;
+            gemm(st, 'N', 'T', GEMM_STORE, n, n, n, D.blk(c.off, l), n, nn, L.blk(c.off, l), n, nn, c.W2.blk(c.off, l), n, nn, r.count, false);
+            gemm(st, 'N', 'N', GEMM_STORE, n, n, n, L.blk(c.off, l), n, nn, c.W2.blk(c.off, l), n, nn, c.W1.blk(c.off, l), n, nn, r.count, false);
         }
         DBuf<int> &ids = c.eig_ids_small;
         ids.upload(small, st);

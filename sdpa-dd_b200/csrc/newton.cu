@@ -47,10 +47,15 @@ void constraint_inner(Context &c, const Space &M, const dd_t *addv, dd_t *out) {
 // InputData::multi_plusToA (sdpa_dataset.cpp:488-493), entry by entry, then
 // mode 0 (compute_DzMat, sdpa_newton.cpp:1318-1327): r = -r (+ D)
 // mode 1 (Residuals::compute, sdpa_dataset.cpp:632-636): r = -r + C - Z
-__global__ void sum_yA_kernel(BlockView v, const dd_t *y, dd_t *out, int mode, const dd_t *D, const dd_t *Z) {
+// One launch per run of equal blocks: CTA row t takes block first + t.
+__global__ void sum_yA_kernel(const BlockView *views, int first, long nn, const dd_t *y, dd_t *out, int mode, const dd_t *D, const dd_t *Z) {
+    const BlockView v = views[first + blockIdx.y];
     const long ne = (long)v.n * v.n;
     const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (e >= ne) return;
+    out += blockIdx.y * nn;
+    if (D) D += blockIdx.y * nn;
+    if (Z) Z += blockIdx.y * nn;
     dd_t acc = dd_zero();
     if (v.all_dense) {
         for (int t = 0; t < v.nc; ++t) acc = dd_acc(acc, dd_mul(ld_dd(v.dense + v.dense_off[t] + e), ld_dd(y + v.con[t])));
@@ -74,12 +79,14 @@ __global__ void sum_yA_kernel(BlockView v, const dd_t *y, dd_t *out, int mode, c
 }
 
 void sum_yA(Context &c, const dd_t *y, Space &out, int mode, const Space *D, const Space *Z) {
-    for (int l = 0; l < c.nSDP; ++l) {
-        const BlockDev &bd = *c.blocks[l];
-        const long ne = (long)bd.n * bd.n;
-        sum_yA_kernel<<<ceil_div(ne, 128), 128, 0, c.stream>>>(bd.view(), y, out.blk(c.off, l), mode, D ? D->blk(c.off, l) : nullptr,
-                                                               Z ? Z->blk(c.off, l) : nullptr);
-        CK_LAUNCH();
+    for (const BlockRun &r : c.runs) {
+        const long nn = (long)r.n * r.n;
+        for (int b0 = 0; b0 < r.count; b0 += MAX_GRID_YZ) {
+            const int l = r.first + b0;
+            sum_yA_kernel<<<dim3(ceil_div(nn, 128), std::min(MAX_GRID_YZ, r.count - b0)), 128, 0, c.stream>>>(
+                c.views.p, l, nn, y, out.blk(c.off, l), mode, D ? D->blk(c.off, l) : nullptr, Z ? Z->blk(c.off, l) : nullptr);
+            CK_LAUNCH();
+        }
     }
 }
 
@@ -114,18 +121,26 @@ void init_point(Context &c, dd_t lambda) {
 bool compute_inverse(Context &c) {
     cudaStream_t st = c.stream;
     CK(cudaMemsetAsync(c.info.p, 0, sizeof(int) * 2, st));
-    for (int l = 0; l < c.nSDP; ++l) {
-        const int n = c.sizes[l];
-        dd_t *w1 = c.W1.blk(c.off, l), *w2 = c.W2.blk(c.off, l);
-        CK(cudaMemcpyAsync(w1, c.X.blk(c.off, l), sizeof(dd_t) * n * n, cudaMemcpyDeviceToDevice, st));
-        potrf(st, w1, n, n, c.info.p, c.rdiag.p);
-        zero_upper(st, w1, n, n);
-        inv_lower(st, w1, n, n, c.invCholX.blk(c.off, l), n);
-        CK(cudaMemcpyAsync(w2, c.Z.blk(c.off, l), sizeof(dd_t) * n * n, cudaMemcpyDeviceToDevice, st));
-        potrf(st, w2, n, n, c.info.p + 1, c.rdiag.p + 128);
-        zero_upper(st, w2, n, n);
-        inv_lower(st, w2, n, n, c.invCholZ.blk(c.off, l), n);
-        trmm_lt(st, c.invCholZ.blk(c.off, l), n, n, c.invZ.blk(c.off, l), n);
+    CK(cudaMemcpyAsync(c.W1.buf.p, c.X.buf.p, sizeof(dd_t) * c.space_len, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(c.W2.buf.p, c.Z.buf.p, sizeof(dd_t) * c.space_len, cudaMemcpyDeviceToDevice, st));
+    for (const BlockRun &r : c.runs) {
+        const int n = r.n;
+        const long nn = (long)n * n;
+        dd_t *w1 = c.W1.blk(c.off, r.first), *w2 = c.W2.blk(c.off, r.first);
+        if (n <= POTRF_NB) {
+            potrf_batched(st, w1, n, n, nn, r.count, c.info.p);
+            potrf_batched(st, w2, n, n, nn, r.count, c.info.p + 1);
+        } else {
+            for (int t = 0; t < r.count; ++t) {
+                potrf(st, w1 + t * nn, n, n, c.info.p, c.rdiag.p);
+                potrf(st, w2 + t * nn, n, n, c.info.p + 1, c.rdiag.p + 128);
+            }
+        }
+        zero_upper(st, w1, n, n, r.count, nn);
+        inv_lower(st, w1, n, n, c.invCholX.blk(c.off, r.first), n, r.count, nn, nn);
+        zero_upper(st, w2, n, n, r.count, nn);
+        inv_lower(st, w2, n, n, c.invCholZ.blk(c.off, r.first), n, r.count, nn, nn);
+        trmm_lt(st, c.invCholZ.blk(c.off, r.first), n, n, c.invZ.blk(c.off, r.first), n, r.count, nn, nn);
     }
     int info[2];
     d2h(c, info, c.info.p, sizeof(info));
@@ -135,10 +150,11 @@ bool compute_inverse(Context &c) {
 // ------------------------------------------------------------ Newton step
 void triple(Context &c, const Space &A, const Space &B, const Space &C, Space &out) {
     // Jal::ns_jordan_triple_product: work = A B; out = work C (two Rgemm)
-    for (int l = 0; l < c.nSDP; ++l) {
-        const int n = c.sizes[l];
-        gemm(c.stream, 'N', 'N', GEMM_STORE, n, n, n, A.blk(c.off, l), n, 0, B.blk(c.off, l), n, 0, c.W2.blk(c.off, l), n, 0, 1, false);
-        gemm(c.stream, 'N', 'N', GEMM_STORE, n, n, n, c.W2.blk(c.off, l), n, 0, C.blk(c.off, l), n, 0, out.blk(c.off, l), n, 0, 1, false);
+    for (const BlockRun &r : c.runs) {
+        const int n = r.n, l = r.first;
+        const long nn = (long)n * n;
+        gemm(c.stream, 'N', 'N', GEMM_STORE, n, n, n, A.blk(c.off, l), n, nn, B.blk(c.off, l), n, nn, c.W2.blk(c.off, l), n, nn, r.count, false);
+        gemm(c.stream, 'N', 'N', GEMM_STORE, n, n, n, c.W2.blk(c.off, l), n, nn, C.blk(c.off, l), n, nn, out.blk(c.off, l), n, nn, r.count, false);
     }
 }
 
@@ -213,7 +229,7 @@ void make_dz_dx(Context &c, bool dual_infeasible) {
     sum_yA(c, c.Dy.p, c.Dz, 0, dual_infeasible ? &c.dualMat : nullptr, nullptr);
     triple(c, c.X, c.Dz, c.invZ, c.W1);
     axpy(c.stream, c.rzinv.buf.p, c.W1.buf.p, c.Dx.buf.p, c.space_len, MONE);
-    for (int l = 0; l < c.nSDP; ++l) symmetrize(c.stream, c.Dx.blk(c.off, l), c.sizes[l]);
+    for (const BlockRun &r : c.runs) symmetrize(c.stream, c.Dx.blk(c.off, r.first), r.n, r.count, (long)r.n * r.n);
 }
 
 // ------------------------------------------------------------ inner products
@@ -228,9 +244,9 @@ static dd_t fetch_sum(Context &c, int nslots) {
 // Lal::getInnerProduct(DenseLinearSpace, DenseLinearSpace)
 // (sdpa_linear.cpp:1571-1611): Rdot per block, summed with "+=".
 dd_t inner_space(Context &c, const Space &a, const Space &b) {
-    for (int l = 0; l < c.nSDP; ++l) {
-        const long nn = (long)c.sizes[l] * c.sizes[l];
-        dot(c.stream, a.blk(c.off, l), 1, b.blk(c.off, l), 1, nn, c.scal.p + l, c.red.p + 256 * (l % 8));
+    for (const BlockRun &r : c.runs) {
+        const long nn = (long)r.n * r.n;
+        dot_batched(c.stream, a.blk(c.off, r.first), nn, b.blk(c.off, r.first), nn, nn, r.count, c.scal.p + r.first, c.red.p);
     }
     return fetch_sum(c, c.nSDP);
 }
@@ -239,24 +255,48 @@ __global__ void sparse_inner_kernel(int n, int nnz, const int *row, const int *c
     if (threadIdx.x == 0) st_dd(out, sparse_dot_dense(n, nnz, row, col, val, D));
 }
 
+// The blocks whose product with C is one chain (sparse C, or dense C of at
+// most DOT_SEQ_TERMS entries) in one launch: CTA l, result to its slot.
+constexpr long DOT_SEQ_TERMS = 1024; // the longest dot that dot() runs as one chain
+__global__ void inner_C_small_kernel(const BlockView *views, const int *slot, const long *off, const dd_t *x, dd_t *out) {
+    if (threadIdx.x != 0) return;
+    const int l = blockIdx.x;
+    const BlockView v = views[l];
+    const int s = slot[l];
+    if (s < 0 || !v.c_present) return;
+    const dd_t *D = x + off[l];
+    if (!v.c_dense) {
+        st_dd(out + s, sparse_dot_dense(v.n, v.c_nnz, v.c_row, v.c_col, v.c_val, D));
+        return;
+    }
+    const long nn = (long)v.n * v.n;
+    if (nn > DOT_SEQ_TERMS) return;
+    dd_t t = dd_zero();
+    for (long i = 0; i < nn; ++i) t = dd_acc(t, dd_mul(ld_dd(v.c_dense_val + i), ld_dd(D + i)));
+    st_dd(out + s, dd_acc(dd_zero(), t));
+}
+
 // Lal::getInnerProduct(SparseLinearSpace C, DenseLinearSpace X)
-// (sdpa_linear.cpp:1616-1650) over C's nonzero SDP blocks.
+// (sdpa_linear.cpp:1616-1650) over C's nonzero SDP blocks: one result slot
+// per such block, summed in block order on the host.
 dd_t inner_C(Context &c, const Space &x) {
-    int slots = 0;
+    if (c.c_slot_host.size() != (size_t)c.nSDP) {
+        c.c_slot_host.assign(c.nSDP, -1);
+        c.c_nslots = 0;
+        for (int l = 0; l < c.nSDP; ++l)
+            if (c.blocks[l]->c_present) c.c_slot_host[l] = c.c_nslots++;
+        c.c_slot.upload(c.c_slot_host, c.stream);
+    }
+    if (c.c_nslots == 0) return dd_zero();
+    inner_C_small_kernel<<<c.nSDP, 32, 0, c.stream>>>(c.views.p, c.c_slot.p, c.d_off.p, x.buf.p, c.scal.p);
+    CK_LAUNCH();
     for (int l = 0; l < c.nSDP; ++l) {
         const BlockDev &bd = *c.blocks[l];
-        if (!bd.c_present) continue;
         const long nn = (long)bd.n * bd.n;
-        if (bd.c_dense) {
-            dot(c.stream, bd.c_dense_val.p, 1, x.blk(c.off, l), 1, nn, c.scal.p + slots, c.red.p + 256 * (slots % 8));
-        } else {
-            sparse_inner_kernel<<<1, 32, 0, c.stream>>>(bd.n, (int)bd.c_row.n, bd.c_row.p, bd.c_col.p, bd.c_val.p, x.blk(c.off, l), c.scal.p + slots);
-            CK_LAUNCH();
-        }
-        ++slots;
+        if (bd.c_present && bd.c_dense && nn > DOT_SEQ_TERMS)
+            dot(c.stream, bd.c_dense_val.p, 1, x.blk(c.off, l), 1, nn, c.scal.p + c.c_slot_host[l], c.red.p + 256 * (c.c_slot_host[l] % 8));
     }
-    if (slots == 0) return dd_zero();
-    return fetch_sum(c, slots);
+    return fetch_sum(c, c.c_nslots);
 }
 
 // Lal::getInnerProduct(Vector, Vector): Rdot over m.
