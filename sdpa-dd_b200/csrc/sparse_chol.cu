@@ -107,8 +107,12 @@ __global__ void sp_gather_kernel(const dd_t *tiles, const int *ent_b, const int 
 
 // ------------------------------------------------------------ panel
 // CTA 0: the diagonal tile of panel J; CTA k > 0: the diagonal tile again
-// (identical arithmetic) and below-diagonal tile col_tiles[k - 1].
-__global__ void __launch_bounds__(SP_THREADS) sp_panel_kernel(dd_t *tiles, const unsigned long long *mask, int m, int J, int diag_t, const int *col_tiles) {
+// (identical arithmetic) and below-diagonal tile col_tiles[k - 1].  Every
+// CTA reads the unfactored diagonal tile at its start, so the factored one
+// is written back by the CTA that finishes last (counted in done[J], which
+// it resets for the next factorisation).
+__global__ void __launch_bounds__(SP_THREADS) sp_panel_kernel(dd_t *tiles, const unsigned long long *mask, int m, int J, int diag_t, const int *col_tiles,
+                                                              int *done) {
     extern __shared__ double2 sp_sm[];
     double2 *D = sp_sm;
     double2 *U = sp_sm + SP_T * SPL;
@@ -148,10 +152,14 @@ __global__ void __launch_bounds__(SP_THREADS) sp_panel_kernel(dd_t *tiles, const
         }
         __syncthreads();
     }
-    if (ut < 0)
+    if (ut >= 0) sp_store_tile(tiles + (long)ut * SP_T * SP_T, U, tid, blockDim.x);
+    __shared__ int last;
+    if (tid == 0) last = atomicAdd(done + J, 1) == (int)gridDim.x - 1;
+    __syncthreads();
+    if (last) {
         sp_store_tile(tiles + (long)diag_t * SP_T * SP_T, D, tid, blockDim.x);
-    else
-        sp_store_tile(tiles + (long)ut * SP_T * SP_T, U, tid, blockDim.x);
+        if (tid == 0) done[J] = 0;
+    }
 }
 
 // ------------------------------------------------------------ update
@@ -427,6 +435,9 @@ static void upload_schedule(Context &c, SparseDev &s) {
     s.upd.upload(t.upd.empty() ? std::vector<int>{0} : t.upd, st);
     s.tiles.alloc((size_t)t.ntiles * SP_T * SP_T);
     s.xp.alloc(std::max(1, t.m));
+    s.panel_done.alloc(std::max(1, t.nblk));
+    CK(cudaMemsetAsync(s.panel_done.p, 0, sizeof(int) * std::max(1, t.nblk), st));
+    s.drop_graph();
     // per entry of the reference layout: its column b and row a
     const SparseStructure &ss = s.plan.s;
     std::vector<int> eb(ss.nnz()), ea(ss.nnz());
@@ -468,25 +479,93 @@ void sparse_setup_structure(Context &c, const SparseStructure &ss) {
     upload_schedule(c, s);
 }
 
-static void sparse_panels(Context &c) {
+// The launches of one factorisation.  Panel J waits for every update that
+// writes into its column block; the update of panel J waits for panel J and
+// for the previous update of each tile it writes (updates of one tile stay
+// in pivot order).  Panels of independent subtrees of the elimination run
+// side by side.
+static void sparse_launches(Context &c, cudaGraph_t g) {
     SparseDev &s = *c.sp;
     const TileSchedule &t = s.sched;
-    cudaStream_t st = c.stream;
     CK(cudaFuncSetAttribute(sp_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SP_TWO_TILES));
     CK(cudaFuncSetAttribute(sp_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SP_TWO_TILES));
+    std::vector<cudaGraphNode_t> last_writer(t.ntiles, nullptr);
+    std::vector<std::vector<cudaGraphNode_t>> into(t.nblk);
+    auto uniq = [](std::vector<cudaGraphNode_t> v) {
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+        return v;
+    };
+    dd_t *tiles = s.tiles.p;
+    const unsigned long long *mask = s.mask.p;
+    int m = t.m;
+    int *done = s.panel_done.p;
     for (int J = 0; J < t.nblk; ++J) {
         const int ncol = t.col_ptr[J + 1] - t.col_ptr[J];
-        const int diag = t.tile_of[J + (size_t)t.nblk * J];
+        int diag = t.tile_of[J + (size_t)t.nblk * J];
         const size_t smem = ncol > 0 ? SP_TWO_TILES : SP_TILE_SMEM;
-        sp_panel_kernel<<<1 + ncol, SP_THREADS, smem, st>>>(s.tiles.p, s.mask.p, t.m, J, diag, s.col_tiles.p + t.col_ptr[J]);
-        CK_LAUNCH();
-        const int nt = t.upd_ptr[J + 1] - t.upd_ptr[J];
-        if (nt > 0) {
-            const int nbJ = std::min(SP_T, t.m - J * SP_T);
-            sp_update_kernel<<<nt * SP_UPD_SPLIT, SP_THREADS, SP_TWO_TILES, st>>>(s.tiles.p, s.mask.p, s.upd.p + 3 * (size_t)t.upd_ptr[J], nbJ);
-            CK_LAUNCH();
+        const int *col = s.col_tiles.p + t.col_ptr[J];
+        int Jv = J;
+        cudaGraphNode_t pnode = nullptr;
+        {
+            void *args[] = {&tiles, &mask, &m, &Jv, &diag, &col, &done};
+            cudaKernelNodeParams kp{};
+            kp.func = (void *)sp_panel_kernel;
+            kp.gridDim = dim3(1 + ncol);
+            kp.blockDim = dim3(SP_THREADS);
+            kp.sharedMemBytes = (unsigned)smem;
+            kp.kernelParams = args;
+            const std::vector<cudaGraphNode_t> deps = uniq(into[J]);
+            CK(cudaGraphAddKernelNode(&pnode, g, deps.data(), deps.size(), &kp));
+        }
+        // the update of panel J in two nodes: the targets in column block
+        // J + 1 (listed first: the schedule sorts targets by column block),
+        // which panel J + 1 waits for, and the rest, which run beside it
+        int nbJ = std::min(SP_T, t.m - J * SP_T);
+        const int q0 = t.upd_ptr[J], q1 = t.upd_ptr[J + 1];
+        int qs = q0;
+        while (qs < q1 && t.tJ[t.upd[3 * qs]] == J + 1) ++qs;
+        for (int part = 0; part < 2; ++part) {
+            const int a = part == 0 ? q0 : qs, b = part == 0 ? qs : q1;
+            if (a == b) continue;
+            const int *upd = s.upd.p + 3 * (size_t)a;
+            void *args[] = {&tiles, &mask, &upd, &nbJ};
+            cudaKernelNodeParams kp{};
+            kp.func = (void *)sp_update_kernel;
+            kp.gridDim = dim3((b - a) * SP_UPD_SPLIT);
+            kp.blockDim = dim3(SP_THREADS);
+            kp.sharedMemBytes = (unsigned)SP_TWO_TILES;
+            kp.kernelParams = args;
+            std::vector<cudaGraphNode_t> deps{pnode};
+            for (int q = a; q < b; ++q)
+                if (last_writer[t.upd[3 * q]]) deps.push_back(last_writer[t.upd[3 * q]]);
+            deps = uniq(deps);
+            cudaGraphNode_t unode;
+            CK(cudaGraphAddKernelNode(&unode, g, deps.data(), deps.size(), &kp));
+            for (int q = a; q < b; ++q) {
+                const int target = t.upd[3 * q];
+                last_writer[target] = unode;
+                into[t.tJ[target]].push_back(unode);
+            }
         }
     }
+}
+
+static void sparse_panels(Context &c) {
+    SparseDev &s = *c.sp;
+    if (!s.graph) {
+        cudaGraph_t g;
+        CK(cudaGraphCreate(&g, 0));
+        try {
+            sparse_launches(c, g);
+            CK(cudaGraphInstantiate(&s.graph, g, 0));
+        } catch (...) {
+            cudaGraphDestroy(g);
+            throw;
+        }
+        CK(cudaGraphDestroy(g));
+    }
+    CK(cudaGraphLaunch(s.graph, c.stream));
 }
 
 void sparse_factor_B(Context &c) {

@@ -24,6 +24,15 @@ struct SparseDev {
     DBuf<int> order;     // new -> old
     DBuf<int> ent_b, ent_a; // per entry of the reference layout: column b, row a >= b
     DBuf<dd_t> xp;       // the permuted right-hand side
+    DBuf<int> panel_done; // per panel: its CTAs that finished (sp_panel_kernel)
+    // the factorisation's panel and update launches as one graph whose
+    // edges are the tiles' data dependencies, built once per structure
+    cudaGraphExec_t graph = nullptr;
+    void drop_graph() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+    }
+    ~SparseDev() { drop_graph(); }
 };
 
 // Plans the Schur form of the attached problem for c.schur_mode and, when
