@@ -17,8 +17,10 @@
 // pivot.  Here, per panel J of 64 pivots:
 //   sp_panel_kernel   one CTA per tile of column block J (the diagonal
 //                     tile first): every CTA factors the diagonal tile in
-//                     shared memory (pivots in order), and CTA k > 0 carries
-//                     its own tile below along with the same pivots;
+//                     shared memory (pivots in order, the next column's
+//                     pivot chain beside the other columns' updates), and
+//                     CTA k > 0 carries its own tile below with the same
+//                     pivots;
 //   sp_update_kernel  every tile (I, K), K > J, that some column of J
 //                     reaches in both I and K: entry (a, r) -= L(r,b) L(a,b)
 //                     for the columns b of J ascending, where both are in
@@ -111,13 +113,19 @@ __global__ void sp_gather_kernel(const dd_t *tiles, const int *ent_b, const int 
 // CTA reads the unfactored diagonal tile at its start, so the factored one
 // is written back by the CTA that finishes last (counted in done[J], which
 // it resets for the next factorisation).
-__global__ void __launch_bounds__(SP_THREADS) sp_panel_kernel(dd_t *tiles, const unsigned long long *mask, int m, int J, int diag_t, const int *col_tiles,
-                                                              int *done) {
+// Step k (one barrier): warp 0 takes column k+1 through pivot k's update,
+// its own pivot (1/sqrt) and its scaling, while warps 1.. apply pivot k's
+// update to columns k+2.. (one column per warp at a time, rows over the
+// lanes); so the chain of pivots runs beside the bulk of the updates and
+// every entry still sees pivot k's update before pivot k+1's.
+constexpr int SP_PANEL_THREADS = 512;
+__global__ void __launch_bounds__(SP_PANEL_THREADS) sp_panel_kernel(dd_t *tiles, const unsigned long long *mask, int m, int J, int diag_t,
+                                                                    const int *col_tiles, int *done) {
     extern __shared__ double2 sp_sm[];
     double2 *D = sp_sm;
-    double2 *U = sp_sm + SP_T * SPL;
+    double2 *U = sp_sm + SP_T * SPL; // used only when the CTA has a tile below (ut >= 0, mu != 0)
     __shared__ unsigned long long md[SP_T], mu[SP_T];
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
     const int nb = min(SP_T, m - J * SP_T);
     const int ut = blockIdx.x > 0 ? col_tiles[blockIdx.x - 1] : -1;
     sp_load_tile(D, tiles + (long)diag_t * SP_T * SP_T, tid, blockDim.x);
@@ -127,28 +135,44 @@ __global__ void __launch_bounds__(SP_THREADS) sp_panel_kernel(dd_t *tiles, const
         mu[tid] = ut >= 0 ? mask[(long)ut * SP_T + tid] : 0ull;
     }
     __syncthreads();
-    for (int b = 0; b < nb; ++b) {
-        const unsigned long long cb = md[b], ub = mu[b];
-        if (tid == 0) {
-            const dd_t d = sm_dd(D, b, b);
-            sm_st(D, b, b, dd_lt_d(d, 0.0) ? dd_zero() : dd_div(dd_from(1.0), dd_sqrt(d)));
+    // warp 0: column c's pivot d_c = 1/sqrt(B(c,c)) (0 for a negative
+    // pivot) and the scaling of column c by it
+    auto pivot = [&](int c) {
+        double ih = 0.0, il = 0.0;
+        if (lane == 0) {
+            const dd_t d = sm_dd(D, c, c);
+            const dd_t inv = dd_lt_d(d, 0.0) ? dd_zero() : dd_div(dd_from(1.0), dd_sqrt(d));
+            sm_st(D, c, c, inv);
+            ih = inv.hi;
+            il = inv.lo;
         }
-        __syncthreads();
-        const dd_t inv = sm_dd(D, b, b);
-        if (tid < SP_T) {
-            if (tid > b && bit64(cb, tid)) sm_st(D, tid, b, dd_muleq(sm_dd(D, tid, b), inv));
-        } else if (tid < 2 * SP_T) {
-            const int i = tid - SP_T;
-            if (bit64(ub, i)) sm_st(U, i, b, dd_muleq(sm_dd(U, i, b), inv));
+        const dd_t inv = dd_make(__shfl_sync(0xffffffffu, ih, 0), __shfl_sync(0xffffffffu, il, 0));
+        const unsigned long long cc = md[c], uc = mu[c];
+        for (int i = lane; i < SP_T; i += 32) {
+            if (i > c && bit64(cc, i)) sm_st(D, i, c, dd_muleq(sm_dd(D, i, c), inv));
+            if (bit64(uc, i)) sm_st(U, i, c, dd_muleq(sm_dd(U, i, c), inv));
         }
-        __syncthreads();
-        // entry (i, r), r in struct(b) within the panel: -= L(r,b) L(i,b)
-        for (int e = tid; e < SP_T * SP_T; e += blockDim.x) {
-            const int i = e & (SP_T - 1), r = e >> 6;
-            if (r <= b || r >= nb || !bit64(cb, r)) continue;
-            const dd_t lrb = sm_dd(D, r, b);
-            if (i >= r && bit64(cb, i)) sm_st(D, i, r, dd_sub(sm_dd(D, i, r), dd_mul(lrb, sm_dd(D, i, b))));
-            if (bit64(ub, i)) sm_st(U, i, r, dd_sub(sm_dd(U, i, r), dd_mul(lrb, sm_dd(U, i, b))));
+        __syncwarp();
+    };
+    // pivot k's update of column r (r in struct(k)): entry (i, r) -= L(r,k) L(i,k)
+    auto apply = [&](int k, int r, unsigned long long ck, unsigned long long uk) {
+        const dd_t lrk = sm_dd(D, r, k);
+        for (int i = lane; i < SP_T; i += 32) {
+            if (i >= r && bit64(ck, i)) sm_st(D, i, r, dd_sub(sm_dd(D, i, r), dd_mul(lrk, sm_dd(D, i, k))));
+            if (bit64(uk, i)) sm_st(U, i, r, dd_sub(sm_dd(U, i, r), dd_mul(lrk, sm_dd(U, i, k))));
+        }
+    };
+    if (warp == 0 && nb > 0) pivot(0);
+    __syncthreads();
+    for (int k = 0; k + 1 < nb; ++k) {
+        const unsigned long long ck = md[k], uk = mu[k];
+        if (warp == 0) {
+            if (bit64(ck, k + 1)) apply(k, k + 1, ck, uk);
+            __syncwarp();
+            pivot(k + 1);
+        } else {
+            for (int r = k + 1 + warp; r < nb; r += nw - 1)
+                if (bit64(ck, r)) apply(k, r, ck, uk);
         }
         __syncthreads();
     }
@@ -512,7 +536,7 @@ static void sparse_launches(Context &c, cudaGraph_t g) {
             cudaKernelNodeParams kp{};
             kp.func = (void *)sp_panel_kernel;
             kp.gridDim = dim3(1 + ncol);
-            kp.blockDim = dim3(SP_THREADS);
+            kp.blockDim = dim3(SP_PANEL_THREADS);
             kp.sharedMemBytes = (unsigned)smem;
             kp.kernelParams = args;
             const std::vector<cudaGraphNode_t> deps = uniq(into[J]);
