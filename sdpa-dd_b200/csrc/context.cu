@@ -42,7 +42,16 @@ BlockView BlockDev::view() const {
 
 bool Context::sparse_active() const { return sp && sp->active; }
 
+SchurGraph::~SchurGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    for (cudaStream_t s : branch) cudaStreamDestroy(s);
+    for (cudaEvent_t e : joined) cudaEventDestroy(e);
+    if (forked) cudaEventDestroy(forked);
+}
+
 Context::~Context() {
+    if (stream) cudaStreamSynchronize(stream);
+    delete sg;
     delete sp;
     if (tc.ev_pre) cudaEventDestroy(tc.ev_pre);
     if (tc.ev_diag) cudaEventDestroy(tc.ev_diag);
@@ -384,6 +393,7 @@ void upload_problem(Context &c, Problem &&p) {
     c.off.assign(c.nSDP + 1, 0);
     for (int l = 0; l < c.nSDP; ++l) c.off[l + 1] = c.off[l] + (long)c.sizes[l] * c.sizes[l];
     c.space_len = c.off[c.nSDP];
+    ++c.upload_gen;
     c.c_slot_host.clear();
     c.runs.clear();
     for (int l = 0; l < c.nSDP; ++l) {

@@ -121,6 +121,25 @@ struct Space {
 class CoreEngine;
 struct SparseDev;
 
+// The Schur build of a problem with many blocks as one CUDA graph (schur.cu):
+// every block's pairs on one of a few parallel branches, each with its own
+// F/G scratch, the pair values into per-block staging squares, then one
+// kernel that adds each entry's block values to B in block order.
+struct SchurGraph {
+    unsigned long gen = 0;     // upload generation the graph was built for (0: none)
+    bool eligible = false;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaStream_t> branch;
+    std::vector<cudaEvent_t> joined;
+    cudaEvent_t forked = nullptr;
+    DBuf<dd_t> stage, F, G;
+    DBuf<int> ent;             // per B entry (i >= j): i, j
+    DBuf<int> ptr;             // per entry: its contributions [ptr[e], ptr[e+1])
+    DBuf<long> src;            // contributions: staging offsets, blocks in order
+    int nent = 0;
+    ~SchurGraph();
+};
+
 // Consecutive SDP blocks of one order: they lie back to back in every
 // space (block first + t at off[first] + t n^2), so the per-block dense
 // kernels run once for the whole run with a batch stride of n^2.
@@ -238,6 +257,9 @@ struct Context {
     // symbolic factor and tiles (sparse_chol.h)
     int schur_mode = 0;
     SparseDev *sp = nullptr;
+    // problem uploads so far (cached graphs and plans are per upload)
+    unsigned long upload_gen = 0;
+    SchurGraph *sg = nullptr;
     bool sparse_active() const;
     ~Context();
 };

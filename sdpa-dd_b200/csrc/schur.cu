@@ -25,6 +25,9 @@
 #include "devops.cuh"
 #include "prof.h"
 
+#include <algorithm>
+#include <unordered_map>
+
 namespace sddd {
 
 static BlockView view(const BlockDev &b) { return b.view(); }
@@ -37,6 +40,17 @@ __device__ __forceinline__ void b_add(dd_t *B, int m, int i, int j, dd_t v) {
         dd_t *q = B + j + (long)m * i;
         st_dd(q, dd_acc(ld_dd(q), v));
     }
+}
+
+// Where a block's pair value goes: into B directly (blocks one after the
+// other), or, with stage != null, into the block's own staging square at
+// (owner position, partner position), from which schur_accumulate_kernel
+// adds the blocks' values to B in block order (blocks side by side).
+__device__ __forceinline__ void pair_out(dd_t *B, int m, dd_t *stage, int nc, int s_own, int s_par, int i, int j, dd_t v) {
+    if (stage)
+        st_dd(stage + (long)s_own * nc + s_par, v);
+    else
+        b_add(B, m, i, j, v);
 }
 
 // ------------------------------------------------- F = A Z^-1, sparse A
@@ -60,7 +74,8 @@ __global__ void f_sparse_kernel(int n, const int *ownFG, const int *rl_off, cons
 // branch), for dense partner d with sorted position nsparse + d <= s(owner r).
 template <int BM, int BN, int BK, int TM, int TN>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN))
-    schur_dense_pairs_kernel(BlockView bv, const int *ownFG, int nfg, int ndense, const dd_t *__restrict__ W, const dd_t *__restrict__ V, dd_t *B, int m) {
+    schur_dense_pairs_kernel(BlockView bv, const int *ownFG, int nfg, int ndense, const dd_t *__restrict__ W, const dd_t *__restrict__ V, dd_t *B, int m,
+                             dd_t *stage) {
     constexpr int TX = BN / TN, TY = BM / TM, NT = TX * TY;
     __shared__ double2 As[BK][BM + 1];
     __shared__ double2 Bs[BK][BN + 1];
@@ -126,13 +141,13 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
             if (s_par > s_own) continue;
             int i = bv.con[bv.perm[s_own]], j = bv.con[bv.perm[s_par]];
             // acc holds the Rdot partial (templ); Rdot returns 0 + templ
-            b_add(B, m, i, j, dd_acc(dd_zero(), acc[r][c]));
+            pair_out(B, m, stage, bv.nc, s_own, s_par, i, j, dd_acc(dd_zero(), acc[r][c]));
         }
 }
 
 // ------------------------------------------ sparse partners of F1 owners
 // value = A_j . G (calF1 with a sparse A_j)
-__global__ void schur_f1_sparse_kernel(BlockView bv, const int *ownFG, int nfg, const dd_t *G, dd_t *B, int m) {
+__global__ void schur_f1_sparse_kernel(BlockView bv, const int *ownFG, int nfg, const dd_t *G, dd_t *B, int m, dd_t *stage) {
     const int r = blockIdx.y;
     const int s_own = ownFG[r];
     const int t_own = bv.perm[s_own];
@@ -142,7 +157,7 @@ __global__ void schur_f1_sparse_kernel(BlockView bv, const int *ownFG, int nfg, 
     const int tj = bv.perm[sp];
     const int off = bv.coo_off[tj];
     dd_t v = sparse_dot_dense(bv.n, bv.nnz[tj], bv.row + off, bv.col + off, bv.val + off, G + (long)r * bv.n * bv.n);
-    b_add(B, m, bv.con[t_own], bv.con[tj], v);
+    pair_out(B, m, stage, bv.nc, s_own, sp, bv.con[t_own], bv.con[tj], v);
 }
 
 // ------------------------------------------ sparse partners of F2 owners
@@ -150,7 +165,7 @@ __global__ void schur_f1_sparse_kernel(BlockView bv, const int *ownFG, int nfg, 
 // of v * Rdot(n, X(alpha, :), F(:, beta)) (+ the swapped term).  One warp per
 // pair: lanes compute the dots, lane 0 accumulates in order.
 constexpr int F2_WARPS = 4;
-__global__ void schur_f2_sparse_kernel(BlockView bv, const int *ownFG, int nfg, const dd_t *X, const dd_t *F, dd_t *B, int m) {
+__global__ void schur_f2_sparse_kernel(BlockView bv, const int *ownFG, int nfg, const dd_t *X, const dd_t *F, dd_t *B, int m, dd_t *stage) {
     __shared__ double2 dots[F2_WARPS][64];
     const int r = blockIdx.y;
     const int s_own = ownFG[r];
@@ -190,7 +205,7 @@ __global__ void schur_f2_sparse_kernel(BlockView bv, const int *ownFG, int nfg, 
             }
             __syncwarp();
         }
-        if (lane == 0) b_add(B, m, bv.con[t_own], bv.con[tj], ret);
+        if (lane == 0) pair_out(B, m, stage, bv.nc, s_own, sp, bv.con[t_own], bv.con[tj], ret);
     }
 }
 
@@ -208,7 +223,7 @@ __global__ void schur_scatter_pairs_kernel(BlockView bv, int nfg, const dd_t *pa
 
 // ----------------------------------------------------------- F3 owners
 // calF3 (sdpa_newton.cpp:937-977), one thread per pair.
-__global__ void schur_f3_kernel(BlockView bv, const int *ownF3, int nf3, const dd_t *X, const dd_t *invZ, dd_t *B, int m) {
+__global__ void schur_f3_kernel(BlockView bv, const int *ownF3, int nf3, const dd_t *X, const dd_t *invZ, dd_t *B, int m, dd_t *stage) {
     const int r = blockIdx.y;
     const int s_own = ownF3[r];
     const int sp = blockIdx.x * blockDim.x + threadIdx.x;
@@ -240,90 +255,221 @@ __global__ void schur_f3_kernel(BlockView bv, const int *ownF3, int nf3, const d
         }
         ret = dd_acc(ret, dd_mul(v1, sum));
     }
-    b_add(B, m, bv.con[ti], bv.con[tj], ret);
+    pair_out(B, m, stage, bv.nc, s_own, sp, bv.con[ti], bv.con[tj], ret);
+}
+
+// One block's pairs, all on stream st, with F and G scratch of its own and
+// its pair values into B (stage null) or into its staging square.
+static void schur_block(Context &c, int l, cudaStream_t st, dd_t *Fb, dd_t *Gb, dd_t *stage) {
+    const int m = c.m;
+    BlockDev &bd = *c.blocks[l];
+    const BlockView bv = view(bd);
+    const int n = bd.n;
+    const long nn = (long)n * n;
+    const dd_t *X = c.X.blk(c.off, l), *Zi = c.invZ.blk(c.off, l);
+    const int nfg = bd.nFG();
+    if (nfg > 0) {
+        // F_r = A_r Z^-1
+        bool any_sparse = false;
+        for (int v : bd.h_rl_off) any_sparse |= v >= 0;
+        if (any_sparse) {
+            dim3 grid(ceil_div(nn, 128), nfg);
+            f_sparse_kernel<<<grid, 128, 0, st>>>(n, bd.ownFG.p, bd.rl_off.p, bd.rl_ptr.p, bd.rl_src.p, bd.rl_val.p, Zi, Fb, nfg);
+            CK_LAUNCH();
+        }
+        if (bd.fg_dense_contig) {
+            // the FG owners' dense matrices are consecutive in bd.dense
+            const long o0 = bd.h_dense_off[bd.h_perm[bd.h_ownFG[0]]];
+            gemm(st, 'N', 'N', GEMM_STORE, n, n, n, bd.dense.p + o0, n, nn, Zi, n, 0, Fb, n, nn, nfg, false);
+        } else {
+            for (int r = 0; r < nfg; ++r) {
+                long o = bd.h_dense_off[bd.h_perm[bd.h_ownFG[r]]];
+                if (o >= 0) gemm(st, 'N', 'N', GEMM_STORE, n, n, n, bd.dense.p + o, n, 0, Zi, n, 0, Fb + r * nn, n, 0, 1, false);
+            }
+        }
+        // G_r = X F_r
+        gemm(st, 'N', 'N', GEMM_STORE, n, n, n, X, n, 0, Fb, n, nn, Gb, n, nn, nfg, false);
+        // dense partners
+        const int ndense = bd.nc - bd.nsparse;
+        if (!stage && c.tc_slices > 0 && bd.nsparse == 0 && nfg == bd.nc && bd.fg_dense_contig && nn <= OG_MAX_K) {
+            // every pair of the block is one n^2-term product G_r . A_d:
+            // the INT8 tensor-core split of W^T V, W = [vec G_r],
+            // V = [vec A_d], then the pairs into B
+            OzakiGemmWork &w = tcg_work(c, nfg, nn, c.tc_slices);
+            c.tcg_pairs.alloc((size_t)nfg * nfg);
+            const long o0 = bd.h_dense_off[bd.h_perm[0]];
+            ozaki_gemm_lower(st, Gb, nn, bd.dense.p + o0, nn, nfg, nn, c.tcg_pairs.p, nfg, w);
+            dim3 grid(ceil_div(nfg, 128), nfg);
+            schur_scatter_pairs_kernel<<<grid, 128, 0, st>>>(bv, nfg, c.tcg_pairs.p, c.B.p, m);
+            CK_LAUNCH();
+        } else if (ndense > 0) {
+            // Every pair is one sequential dot over the n^2 entries.  With
+            // few pairs (small m) 64 x 64 tiles of 16 pairs per thread
+            // leave the GPU nearly idle on long chains; one pair per
+            // thread in 16 x 16 tiles spreads them over many more CTAs.
+            if ((long)ceil_div(ndense, 64) * ceil_div(nfg, 64) >= 2L * 148) {
+                constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4;
+                dim3 grid(ceil_div(ndense, BN), ceil_div(nfg, BM));
+                schur_dense_pairs_kernel<BM, BN, BK, TM, TN>
+                    <<<grid, (BM / TM) * (BN / TN), 0, st>>>(bv, bd.ownFG.p, nfg, ndense, Gb, bd.dense.p, c.B.p, m, stage);
+            } else {
+                constexpr int BM = 16, BN = 16, BK = 32, TM = 1, TN = 1;
+                dim3 grid(ceil_div(ndense, BN), ceil_div(nfg, BM));
+                schur_dense_pairs_kernel<BM, BN, BK, TM, TN>
+                    <<<grid, (BM / TM) * (BN / TN), 0, st>>>(bv, bd.ownFG.p, nfg, ndense, Gb, bd.dense.p, c.B.p, m, stage);
+            }
+            CK_LAUNCH();
+        }
+        // sparse partners
+        if (bd.nsparse > 0) {
+            dim3 g1(ceil_div(bd.nsparse, 128), nfg);
+            schur_f1_sparse_kernel<<<g1, 128, 0, st>>>(bv, bd.ownFG.p, nfg, Gb, c.B.p, m, stage);
+            CK_LAUNCH();
+            dim3 g2(ceil_div(bd.nsparse, F2_WARPS), nfg);
+            schur_f2_sparse_kernel<<<g2, 32 * F2_WARPS, 0, st>>>(bv, bd.ownFG.p, nfg, X, Fb, c.B.p, m, stage);
+            CK_LAUNCH();
+        }
+    }
+    const int nf3 = bd.nF3();
+    if (nf3 > 0) {
+        dim3 grid(ceil_div(bd.nsparse, 128), nf3);
+        schur_f3_kernel<<<grid, 128, 0, st>>>(bv, bd.ownF3.p, nf3, X, Zi, c.B.p, m, stage);
+        CK_LAUNCH();
+    }
+}
+
+// ------------------------------------------------ many blocks: one graph
+// B(i,j) = 0 + v_l1 + v_l2 + ... over the blocks holding both constraints,
+// in block order (bMat.setZero, then each block's "+="), from the blocks'
+// staging squares; both triangles.
+__global__ void schur_accumulate_kernel(const int *ent, const int *ptr, const long *src, int nent, const dd_t *stage, dd_t *B, int m) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nent) return;
+    const int i = ent[2 * e], j = ent[2 * e + 1];
+    dd_t acc = dd_zero();
+    for (int q = ptr[e]; q < ptr[e + 1]; ++q) acc = dd_acc(acc, ld_dd(stage + src[q]));
+    st_dd(B + i + (long)m * j, acc);
+    if (i != j) st_dd(B + j + (long)m * i, acc);
+}
+
+constexpr int SG_MIN_BLOCKS = 4;         // fewer blocks: the blocks one after the other
+constexpr int SG_BRANCHES = 8;           // parallel branches of the graph
+constexpr long SG_MAX_STAGE = 1L << 24;  // staging entries (256 MB)
+constexpr long SG_MAX_FG = 1L << 22;     // F (and G) scratch entries per branch
+
+static void schur_block(Context &c, int l, cudaStream_t st, dd_t *Fb, dd_t *Gb, dd_t *stage);
+
+// Builds (once per upload) and launches the many-block graph; false when the
+// problem takes the sequential path (few blocks, the tensor-core split of
+// the pair products, or scratch above the caps).
+static bool schur_graph_launch(Context &c) {
+    if (c.nSDP < SG_MIN_BLOCKS || c.tc_slices > 0) return false;
+    if (!c.sg) c.sg = new SchurGraph();
+    SchurGraph &g = *c.sg;
+    if (g.gen != c.upload_gen) {
+        g.gen = c.upload_gen;
+        g.eligible = false;
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+        std::vector<long> soff(c.nSDP + 1, 0);
+        long maxfg = 1;
+        for (int l = 0; l < c.nSDP; ++l) {
+            const BlockDev &bd = *c.blocks[l];
+            soff[l + 1] = soff[l] + (long)bd.nc * bd.nc;
+            maxfg = std::max(maxfg, (long)bd.nFG() * bd.n * bd.n);
+        }
+        if (soff[c.nSDP] > SG_MAX_STAGE || maxfg > SG_MAX_FG) return false;
+        // the B entries and their contributions, blocks in order
+        std::unordered_map<long, int> index;
+        std::vector<std::pair<long, std::vector<long>>> entries;
+        for (int l = 0; l < c.nSDP; ++l) {
+            const BlockDev &bd = *c.blocks[l];
+            const std::vector<int> &con = c.prob.cons[l];
+            for (int so = 0; so < bd.nc; ++so)
+                for (int sp = 0; sp <= so; ++sp) {
+                    const int a = con[bd.h_perm[so]], b = con[bd.h_perm[sp]];
+                    const long key = (long)std::max(a, b) * c.m + std::min(a, b);
+                    auto it = index.find(key);
+                    int e;
+                    if (it == index.end()) {
+                        e = (int)entries.size();
+                        index.emplace(key, e);
+                        entries.push_back({key, {}});
+                    } else {
+                        e = it->second;
+                    }
+                    entries[e].second.push_back(soff[l] + (long)so * bd.nc + sp);
+                }
+        }
+        std::sort(entries.begin(), entries.end(), [](const auto &x, const auto &y) { return x.first < y.first; });
+        std::vector<int> ent, ptr(1, 0);
+        std::vector<long> src;
+        for (const auto &e : entries) {
+            ent.push_back((int)(e.first / c.m));
+            ent.push_back((int)(e.first % c.m));
+            src.insert(src.end(), e.second.begin(), e.second.end());
+            ptr.push_back((int)src.size());
+        }
+        g.nent = (int)entries.size();
+        g.ent.upload(ent, c.stream);
+        g.ptr.upload(ptr, c.stream);
+        g.src.upload(src, c.stream);
+        g.stage.alloc((size_t)std::max(1L, soff[c.nSDP]));
+        g.F.alloc((size_t)SG_BRANCHES * maxfg);
+        g.G.alloc((size_t)SG_BRANCHES * maxfg);
+        if (g.branch.empty()) {
+            g.branch.resize(SG_BRANCHES);
+            g.joined.resize(SG_BRANCHES);
+            for (int k = 0; k < SG_BRANCHES; ++k) {
+                CK(cudaStreamCreateWithFlags(&g.branch[k], cudaStreamNonBlocking));
+                CK(cudaEventCreateWithFlags(&g.joined[k], cudaEventDisableTiming));
+            }
+            CK(cudaEventCreateWithFlags(&g.forked, cudaEventDisableTiming));
+        }
+        CK(cudaStreamSynchronize(c.stream));
+        cudaStream_t st = c.stream;
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        try {
+            CK(cudaMemsetAsync(c.B.p, 0, sizeof(dd_t) * (size_t)c.m * c.m, st)); // bMat.setZero()
+            CK(cudaEventRecord(g.forked, st));
+            const int nbr = std::min(SG_BRANCHES, c.nSDP);
+            for (int k = 0; k < nbr; ++k) CK(cudaStreamWaitEvent(g.branch[k], g.forked, 0));
+            for (int l = 0; l < c.nSDP; ++l) {
+                const int k = l % nbr;
+                schur_block(c, l, g.branch[k], g.F.p + k * maxfg, g.G.p + k * maxfg, g.stage.p + soff[l]);
+            }
+            for (int k = 0; k < nbr; ++k) {
+                CK(cudaEventRecord(g.joined[k], g.branch[k]));
+                CK(cudaStreamWaitEvent(st, g.joined[k], 0));
+            }
+            if (g.nent > 0) {
+                schur_accumulate_kernel<<<ceil_div(g.nent, 128), 128, 0, st>>>(g.ent.p, g.ptr.p, g.src.p, g.nent, g.stage.p, c.B.p, c.m);
+                CK_LAUNCH();
+            }
+        } catch (...) {
+            cudaGraph_t dropped;
+            cudaStreamEndCapture(st, &dropped);
+            if (dropped) cudaGraphDestroy(dropped);
+            throw;
+        }
+        CK(cudaStreamEndCapture(st, &graph));
+        CK(cudaGraphInstantiate(&g.exec, graph, 0));
+        CK(cudaGraphDestroy(graph));
+        g.eligible = true;
+    }
+    if (!g.eligible) return false;
+    CK(cudaGraphLaunch(g.exec, c.stream));
+    return true;
 }
 
 void schur_build(Context &c) {
     cudaStream_t st = c.stream;
     PROF_SCOPE("schur_build", st);
+    if (schur_graph_launch(c)) return;
     const int m = c.m;
     CK(cudaMemsetAsync(c.B.p, 0, sizeof(dd_t) * (size_t)m * m, st)); // bMat.setZero()
-    for (int l = 0; l < c.nSDP; ++l) {
-        BlockDev &bd = *c.blocks[l];
-        const BlockView bv = view(bd);
-        const int n = bd.n;
-        const long nn = (long)n * n;
-        const dd_t *X = c.X.blk(c.off, l), *Zi = c.invZ.blk(c.off, l);
-        const int nfg = bd.nFG();
-        if (nfg > 0) {
-            // F_r = A_r Z^-1
-            bool any_sparse = false;
-            for (int v : bd.h_rl_off) any_sparse |= v >= 0;
-            if (any_sparse) {
-                dim3 grid(ceil_div(nn, 128), nfg);
-                f_sparse_kernel<<<grid, 128, 0, st>>>(n, bd.ownFG.p, bd.rl_off.p, bd.rl_ptr.p, bd.rl_src.p, bd.rl_val.p, Zi, c.Fbuf.p, nfg);
-                CK_LAUNCH();
-            }
-            if (bd.fg_dense_contig) {
-                // the FG owners' dense matrices are consecutive in bd.dense
-                const long o0 = bd.h_dense_off[bd.h_perm[bd.h_ownFG[0]]];
-                gemm(st, 'N', 'N', GEMM_STORE, n, n, n, bd.dense.p + o0, n, nn, Zi, n, 0, c.Fbuf.p, n, nn, nfg, false);
-            } else {
-                for (int r = 0; r < nfg; ++r) {
-                    long o = bd.h_dense_off[bd.h_perm[bd.h_ownFG[r]]];
-                    if (o >= 0) gemm(st, 'N', 'N', GEMM_STORE, n, n, n, bd.dense.p + o, n, 0, Zi, n, 0, c.Fbuf.p + r * nn, n, 0, 1, false);
-                }
-            }
-            // G_r = X F_r
-            gemm(st, 'N', 'N', GEMM_STORE, n, n, n, X, n, 0, c.Fbuf.p, n, nn, c.Gbuf.p, n, nn, nfg, false);
-            // dense partners
-            const int ndense = bd.nc - bd.nsparse;
-            if (c.tc_slices > 0 && bd.nsparse == 0 && nfg == bd.nc && bd.fg_dense_contig && nn <= OG_MAX_K) {
-                // every pair of the block is one n^2-term product G_r . A_d:
-                // the INT8 tensor-core split of W^T V, W = [vec G_r],
-                // V = [vec A_d], then the pairs into B
-                OzakiGemmWork &w = tcg_work(c, nfg, nn, c.tc_slices);
-                c.tcg_pairs.alloc((size_t)nfg * nfg);
-                const long o0 = bd.h_dense_off[bd.h_perm[0]];
-                ozaki_gemm_lower(st, c.Gbuf.p, nn, bd.dense.p + o0, nn, nfg, nn, c.tcg_pairs.p, nfg, w);
-                dim3 grid(ceil_div(nfg, 128), nfg);
-                schur_scatter_pairs_kernel<<<grid, 128, 0, st>>>(bv, nfg, c.tcg_pairs.p, c.B.p, m);
-                CK_LAUNCH();
-            } else if (ndense > 0) {
-                // Every pair is one sequential dot over the n^2 entries.  With
-                // few pairs (small m) 64 x 64 tiles of 16 pairs per thread
-                // leave the GPU nearly idle on long chains; one pair per
-                // thread in 16 x 16 tiles spreads them over many more CTAs.
-                if ((long)ceil_div(ndense, 64) * ceil_div(nfg, 64) >= 2L * 148) {
-                    constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4;
-                    dim3 grid(ceil_div(ndense, BN), ceil_div(nfg, BM));
-                    schur_dense_pairs_kernel<BM, BN, BK, TM, TN>
-                        <<<grid, (BM / TM) * (BN / TN), 0, st>>>(bv, bd.ownFG.p, nfg, ndense, c.Gbuf.p, bd.dense.p, c.B.p, m);
-                } else {
-                    constexpr int BM = 16, BN = 16, BK = 32, TM = 1, TN = 1;
-                    dim3 grid(ceil_div(ndense, BN), ceil_div(nfg, BM));
-                    schur_dense_pairs_kernel<BM, BN, BK, TM, TN>
-                        <<<grid, (BM / TM) * (BN / TN), 0, st>>>(bv, bd.ownFG.p, nfg, ndense, c.Gbuf.p, bd.dense.p, c.B.p, m);
-                }
-                CK_LAUNCH();
-            }
-            // sparse partners
-            if (bd.nsparse > 0) {
-                dim3 g1(ceil_div(bd.nsparse, 128), nfg);
-                schur_f1_sparse_kernel<<<g1, 128, 0, st>>>(bv, bd.ownFG.p, nfg, c.Gbuf.p, c.B.p, m);
-                CK_LAUNCH();
-                dim3 g2(ceil_div(bd.nsparse, F2_WARPS), nfg);
-                schur_f2_sparse_kernel<<<g2, 32 * F2_WARPS, 0, st>>>(bv, bd.ownFG.p, nfg, X, c.Fbuf.p, c.B.p, m);
-                CK_LAUNCH();
-            }
-        }
-        const int nf3 = bd.nF3();
-        if (nf3 > 0) {
-            dim3 grid(ceil_div(bd.nsparse, 128), nf3);
-            schur_f3_kernel<<<grid, 128, 0, st>>>(bv, bd.ownF3.p, nf3, X, Zi, c.B.p, m);
-            CK_LAUNCH();
-        }
-    }
+    for (int l = 0; l < c.nSDP; ++l) schur_block(c, l, st, c.Fbuf.p, c.Gbuf.p, nullptr);
     if (c.tcg.err) ozaki_gemm_check(st, c.tcg);
 }
 
