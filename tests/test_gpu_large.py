@@ -73,8 +73,13 @@ def test_large_solve_matches_reference(name, form, workdir):
             mus.append(Decimal(res.mu.hi) + Decimal(res.mu.lo))
         r = c.solve(par)
     spread = g["mu_spread"]
+    # the passes before the reference's own runs part by more than 1e-20:
+    # all 47 but the last ~25 for theta_nv120, only pass 0 for the control
+    # shape (its 2-thread run leaves the 1-thread trajectory by 5.7e-20 at
+    # pass 1: dense F1 products whose OpenMP partial sums round by thread
+    # count), whose parity then rests on phase, iterations and objectives
     chaos = next((q for q, s_ in enumerate(spread) if s_ > 1e-20), len(spread))
-    assert chaos >= 3, chaos
+    assert chaos >= 1, chaos
     for q in range(min(chaos, len(mus))):
         want = _dec(g["mu_trajectory"][q])
         tol = max(Decimal("1e-25"), 10 * Decimal(spread[q]))
