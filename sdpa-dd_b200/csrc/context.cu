@@ -449,10 +449,11 @@ void alloc_state(Context &c) {
     for (auto &bd : c.blocks) fg = std::max(fg, (size_t)bd->nFG() * bd->n * bd->n);
     c.Fbuf.alloc(std::max<size_t>(fg, 1));
     c.Gbuf.alloc(std::max<size_t>(fg, 1));
-    // one result slot per block: the per-block inner products
-    // (inner_space, inner_C) and the step-length eigenvalues (min_eig, big
-    // blocks first, then the small ones) each use at most nSDP slots
-    c.scal.alloc(std::max<size_t>(64, (size_t)c.nSDP + 8));
+    // result slots: the per-block inner products (inner_space, inner_C) use
+    // at most nSDP; the step-length eigenvalues of up to two spaces use 2
+    // nSDP (per space: big blocks first, then the small ones) plus 2 nSDP
+    // for the Lanczos launch's own outputs
+    c.scal.alloc(std::max<size_t>(64, 4 * (size_t)c.nSDP + 8));
     c.red.alloc(4096);
     c.info.alloc(4);
     c.rdiag.alloc(256);

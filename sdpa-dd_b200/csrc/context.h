@@ -199,7 +199,7 @@ struct Context {
     // Schur work: F_i and G_i of FG owners (largest block)
     DBuf<dd_t> Fbuf, Gbuf;
     // small scratch
-    DBuf<dd_t> scal;   // device scalars: max(64, nSDP + 8) result slots
+    DBuf<dd_t> scal;   // device scalars: max(64, 4 nSDP + 8) result slots
     DBuf<dd_t> red;    // reduction scratch
     DBuf<int> info;
     DBuf<dd_t> rdiag;
@@ -207,6 +207,7 @@ struct Context {
     // step-length eigenvalue work: block lists and Lanczos vectors (kept, so
     // that no call allocates or frees)
     DBuf<int> eig_ids_big, eig_ids_small;
+    unsigned long eig_ids_gen = 0;
     DBuf<dd_t> eig_work;
     TrsvSync trsv;
     // budget of every bounded device wait of this context's kernels (the

@@ -152,11 +152,18 @@ struct LanczosShared {
     int go, check;
 };
 
-// One CTA per block: work holds 5 n-vectors (q, qold, r, w, tmp).
-__global__ void __launch_bounds__(LZ_THREADS) lanczos_kernel(const int *blk_ids, const int *sizes, const long *off, const dd_t *Lsp, const dd_t *Dsp,
-                                                             dd_t *work, long work_stride, dd_t *out) {
+// One CTA per block: work holds 5 n-vectors (q, qold, r, w, tmp).  With a
+// second space (Lsp2, Dsp2), CTAs nb.. take the same blocks of that space,
+// so the two step-length eigenvalues run side by side.
+__global__ void __launch_bounds__(LZ_THREADS) lanczos_kernel(const int *blk_ids, int nb, const int *sizes, const long *off, const dd_t *Lsp,
+                                                             const dd_t *Dsp, const dd_t *Lsp2, const dd_t *Dsp2, dd_t *work, long work_stride, dd_t *out) {
     __shared__ LanczosShared S;
-    const int b = blk_ids[blockIdx.x];
+    const bool second = (int)blockIdx.x >= nb;
+    const int b = blk_ids[second ? blockIdx.x - nb : blockIdx.x];
+    if (second) {
+        Lsp = Lsp2;
+        Dsp = Dsp2;
+    }
     const int n = sizes[b];
     const dd_t *L = Lsp + off[b], *X = Dsp + off[b];
     dd_t *q = work + blockIdx.x * work_stride, *qold = q + n, *r = qold + n, *w = r + n, *tmp = w + n;
@@ -331,54 +338,81 @@ __global__ void small_min_eig_kernel(const int *blk_ids, const int *sizes, const
     out[blockIdx.x] = dd_mul_d(dd_add(lo, hi), 0.5);
 }
 
-dd_t min_eig(Context &c, const Space &L, const Space &D) {
+// The small blocks (n <= 20) of one space: DLS2 = D L^T (Rgemm "N","T"),
+// DLS1 = L DLS2 (Rgemm "N","N"), then each block's smallest eigenvalue to
+// res[0 ..) in block order.
+static void small_blocks(Context &c, const Space &L, const Space &D, const std::vector<int> &small, dd_t *res) {
+    cudaStream_t st = c.stream;
+    for (const BlockRun &r : c.runs) {
+        if (r.n > 20) continue;
+        const int n = r.n, l = r.first;
+        const long nn = (long)n * n;
+        gemm(st, 'N', 'T', GEMM_STORE, n, n, n, D.blk(c.off, l), n, nn, L.blk(c.off, l), n, nn, c.W2.blk(c.off, l), n, nn, r.count, false);
+        gemm(st, 'N', 'N', GEMM_STORE, n, n, n, L.blk(c.off, l), n, nn, c.W2.blk(c.off, l), n, nn, c.W1.blk(c.off, l), n, nn, r.count, false);
+    }
+    small_min_eig_kernel<<<(unsigned)small.size(), 32, 0, st>>>(c.eig_ids_small.p, c.d_sizes.p, c.d_off.p, c.W1.buf.p, res);
+    CK_LAUNCH();
+}
+
+// min over the blocks of lambda_min(L D L^T) for nsp spaces (1 or 2): the
+// big blocks' Lanczos of all spaces in one launch; results per space in
+// block order, then the minimum as the reference takes it.
+static void min_eig_spaces(Context &c, int nsp, const Space *L[2], const Space *D[2], dd_t out[2]) {
     cudaStream_t st = c.stream;
     PROF_SCOPE("min_eig", st);
     std::vector<int> big, small;
     for (int l = 0; l < c.nSDP; ++l) (c.sizes[l] > 20 ? big : small).push_back(l);
     static_assert(LZ_KMAX >= 64, "Lanczos step bound");
-    std::vector<dd_t> vals;
-    if (!big.empty()) {
-        DBuf<int> &ids = c.eig_ids_big;
-        ids.upload(big, st);
+    if (c.eig_ids_big.n != big.size() || c.eig_ids_small.n != small.size() || c.eig_ids_gen != c.upload_gen) {
+        c.eig_ids_big.upload(big, st);
+        c.eig_ids_small.upload(small, st);
+        c.eig_ids_gen = c.upload_gen;
+    }
+    const size_t nb = big.size(), ns = small.size();
+    // result slots: space s at s * nSDP: big blocks first, then the small
+    dd_t *res = c.scal.p;
+    if (nb > 0) {
         long maxn = 0;
         for (int l : big) maxn = std::max<long>(maxn, c.sizes[l]);
-        DBuf<dd_t> &work = c.eig_work;
-        work.alloc(5 * maxn * big.size());
-        lanczos_kernel<<<(unsigned)big.size(), LZ_THREADS, 0, st>>>(ids.p, c.d_sizes.p, c.d_off.p, L.buf.p, D.buf.p, work.p, 5 * maxn, c.scal.p);
+        c.eig_work.alloc(5 * maxn * nb * nsp);
+        // the two spaces' CTAs write slots 0 .. 2 nb - 1; spread below
+        lanczos_kernel<<<(unsigned)(nb * nsp), LZ_THREADS, 0, st>>>(c.eig_ids_big.p, (int)nb, c.d_sizes.p, c.d_off.p, L[0]->buf.p, D[0]->buf.p,
+                                                                   L[nsp - 1]->buf.p, D[nsp - 1]->buf.p, c.eig_work.p, 5 * maxn, res + 2 * c.nSDP);
         CK_LAUNCH();
-        std::vector<dd_t> h(big.size());
-        d2h(c, h.data(), c.scal.p, sizeof(dd_t) * big.size());
-        vals.insert(vals.end(), h.begin(), h.end());
     }
-    if (!small.empty()) {
-        // DLS2 = D L^T (Rgemm "N","T"); DLS1 = L DLS2 (Rgemm "N","N")
-        for (const BlockRun &r : c.runs) {
-            if (r.n > 20) continue;
-            const int n = r.n, l = r.first;
-            const long nn = (long)n * n;
-            gemm(st, 'N', 'T', GEMM_STORE, n, n, n, D.blk(c.off, l), n, nn, L.blk(c.off, l), n, nn, c.W2.blk(c.off, l), n, nn, r.count, false);
-            gemm(st, 'N', 'N', GEMM_STORE, n, n, n, L.blk(c.off, l), n, nn, c.W2.blk(c.off, l), n, nn, c.W1.blk(c.off, l), n, nn, r.count, false);
+    for (int sp = 0; sp < nsp && ns > 0; ++sp) small_blocks(c, *L[sp], *D[sp], small, res + (size_t)sp * c.nSDP + nb);
+    if (nb > 0) {
+        for (int sp = 0; sp < nsp; ++sp)
+            CK(cudaMemcpyAsync(res + (size_t)sp * c.nSDP, res + 2 * c.nSDP + sp * nb, sizeof(dd_t) * nb, cudaMemcpyDeviceToDevice, st));
+    }
+    std::vector<dd_t> h((size_t)nsp * c.nSDP);
+    d2h(c, h.data(), res, sizeof(dd_t) * h.size());
+    for (int sp = 0; sp < nsp; ++sp) {
+        // blocks in order: big blocks' values first in the slots, then the small
+        const dd_t *v = h.data() + (size_t)sp * c.nSDP;
+        size_t bi = 0, si = 0;
+        dd_t mn = dd_from(1.0e50);
+        for (int l = 0; l < c.nSDP; ++l) {
+            const dd_t x = (c.sizes[l] > 20) ? v[bi++] : v[nb + si++];
+            if (dd_lt(x, mn)) mn = x;
         }
-        DBuf<int> &ids = c.eig_ids_small;
-        ids.upload(small, st);
-        // results after the big blocks' slots: big.size() + small.size()
-        // = nSDP slots, which c.scal always holds
-        dd_t *res = c.scal.p + big.size();
-        small_min_eig_kernel<<<(unsigned)small.size(), 32, 0, st>>>(ids.p, c.d_sizes.p, c.d_off.p, c.W1.buf.p, res);
-        CK_LAUNCH();
-        std::vector<dd_t> h(small.size());
-        d2h(c, h.data(), res, sizeof(dd_t) * small.size());
-        vals.insert(vals.end(), h.begin(), h.end());
+        out[sp] = mn;
     }
-    // blocks in order: re-sort the values by block index
-    std::vector<dd_t> byblock(c.nSDP);
-    size_t bi = 0, si = 0;
-    for (int l = 0; l < c.nSDP; ++l) byblock[l] = (c.sizes[l] > 20) ? vals[bi++] : vals[big.size() + si++];
-    dd_t mn = dd_from(1.0e50);
-    for (int l = 0; l < c.nSDP; ++l)
-        if (dd_lt(byblock[l], mn)) mn = byblock[l];
-    return mn;
+}
+
+dd_t min_eig(Context &c, const Space &L, const Space &D) {
+    const Space *Ls[2] = {&L, &L}, *Ds[2] = {&D, &D};
+    dd_t out[2];
+    min_eig_spaces(c, 1, Ls, Ds, out);
+    return out[0];
+}
+
+void min_eig_pair(Context &c, const Space &L1, const Space &D1, const Space &L2, const Space &D2, dd_t &out1, dd_t &out2) {
+    const Space *Ls[2] = {&L1, &L2}, *Ds[2] = {&D1, &D2};
+    dd_t out[2];
+    min_eig_spaces(c, 2, Ls, Ds, out);
+    out1 = out[0];
+    out2 = out[1];
 }
 
 } // namespace sddd

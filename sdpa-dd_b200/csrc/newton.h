@@ -38,6 +38,8 @@ void residuals(Context &c, dd_t &normPrimal, dd_t &normDual);
 dd_t lambda_trace(Context &c, const Space &s, double lambda);
 // Jal::getMinEigen(L, D) over the SDP blocks (sdpa_jordan.cpp:55-88).
 dd_t min_eig(Context &c, const Space &L, const Space &D);
+// The same for two spaces at once (their Lanczos side by side).
+void min_eig_pair(Context &c, const Space &L1, const Space &D1, const Space &L2, const Space &D2, dd_t &out1, dd_t &out2);
 
 // Building blocks shared with the adjoint (adjoint.cu):
 // out_k = -(A_k . M) + addv_k (InputData::multi_InnerProductToA, then the

@@ -117,7 +117,7 @@ extern "C" int sddd_min_eig_noalloc(void *stream, long n, const sddd_dd *L, cons
         noalloc_header_kernel<<<1, 1, 0, st>>>(ids, sizes, off, (int)n);
         CK_LAUNCH();
         if (n > SMALL_N) {
-            lanczos_kernel<<<1, LZ_THREADS, 0, st>>>(ids, sizes, off, Ld, Dd, work, 5 * n, o);
+            lanczos_kernel<<<1, LZ_THREADS, 0, st>>>(ids, 1, sizes, off, Ld, Dd, Ld, Dd, work, 5 * n, o);
             CK_LAUNCH();
         } else {
             // W2 = D L^T (Rgemm "N","T"), W1 = L W2 (Rgemm "N","N")

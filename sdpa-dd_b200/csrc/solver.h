@@ -17,7 +17,7 @@ enum PhaseType { noINFO = 0, pFEAS, dFEAS, pdFEAS, pdINF, pFEAS_dINF, pINF_dFEAS
 // ComputeTime rows the device path measures (seconds).
 struct Timers {
     double predictor = 0, corrector = 0, makebMat = 0, choleskybMat = 0, solve = 0, makedXdZ = 0, makegVec = 0, stepPred = 0, stepCorr = 0,
-           eigX = 0, eigZ = 0, xMatTime = 0, zMatTime = 0, updateRes = 0, mainLoop = 0, fileRead = 0, total = 0;
+           eigX = 0, eigZ = 0, eigBoth = 0, xMatTime = 0, zMatTime = 0, updateRes = 0, mainLoop = 0, fileRead = 0, total = 0;
 };
 
 class Solver {
