@@ -58,6 +58,9 @@ Context::~Context() {
     if (tc.side) cudaStreamDestroy(tc.side);
     if (sync_ev) cudaEventDestroy(sync_ev);
     if (core_ready) cudaEventDestroy(core_ready);
+    if (aux_fork) cudaEventDestroy(aux_fork);
+    if (aux_join) cudaEventDestroy(aux_join);
+    if (aux) cudaStreamDestroy(aux);
     if (stream) cudaStreamDestroy(stream);
     if (h_pin) cudaFreeHost(h_pin);
 }

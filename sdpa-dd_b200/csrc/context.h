@@ -154,6 +154,10 @@ struct Context {
     CoreEngine *core = nullptr;
     cudaEvent_t core_ready = nullptr;
     cudaStream_t stream = nullptr;
+    // a second stream for work independent of the main stream's (the
+    // inverses of Z beside those of X), joined back through events
+    cudaStream_t aux = nullptr;
+    cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
     bool shared_gpu = false; // a batch worker: other contexts' streams share the GPU
     // pinned host staging for the small device-to-host reads of the solver
     // (scalars, status words): a copy into pageable memory goes through the

@@ -120,28 +120,39 @@ void init_point(Context &c, dd_t lambda) {
 // Z^-1 = L_Z^-T L_Z^-1 by Rtrmm.
 bool compute_inverse(Context &c) {
     cudaStream_t st = c.stream;
+    if (!c.aux) {
+        CK(cudaStreamCreateWithFlags(&c.aux, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c.aux_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c.aux_join, cudaEventDisableTiming));
+    }
     CK(cudaMemsetAsync(c.info.p, 0, sizeof(int) * 2, st));
     CK(cudaMemcpyAsync(c.W1.buf.p, c.X.buf.p, sizeof(dd_t) * c.space_len, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(c.W2.buf.p, c.Z.buf.p, sizeof(dd_t) * c.space_len, cudaMemcpyDeviceToDevice, st));
-    for (const BlockRun &r : c.runs) {
-        const int n = r.n;
-        const long nn = (long)n * n;
-        dd_t *w1 = c.W1.blk(c.off, r.first), *w2 = c.W2.blk(c.off, r.first);
-        if (n <= POTRF_NB) {
-            potrf_batched(st, w1, n, n, nn, r.count, c.info.p);
-            potrf_batched(st, w2, n, n, nn, r.count, c.info.p + 1);
-        } else {
-            for (int t = 0; t < r.count; ++t) {
-                potrf(st, w1 + t * nn, n, n, c.info.p, c.rdiag.p);
-                potrf(st, w2 + t * nn, n, n, c.info.p + 1, c.rdiag.p + 128);
+    // X's factors on the main stream, Z's (and Z^-1) on the second one
+    CK(cudaEventRecord(c.aux_fork, st));
+    CK(cudaStreamWaitEvent(c.aux, c.aux_fork, 0));
+    for (int side = 0; side < 2; ++side) {
+        cudaStream_t s = side == 0 ? st : c.aux;
+        const Space &W = side == 0 ? c.W1 : c.W2;
+        Space &inv = side == 0 ? c.invCholX : c.invCholZ;
+        int *info = c.info.p + side;
+        dd_t *rdiag = c.rdiag.p + 128 * side;
+        for (const BlockRun &r : c.runs) {
+            const int n = r.n;
+            const long nn = (long)n * n;
+            dd_t *w = W.blk(c.off, r.first);
+            if (n <= POTRF_NB) {
+                potrf_batched(s, w, n, n, nn, r.count, info);
+            } else {
+                for (int t = 0; t < r.count; ++t) potrf(s, w + t * nn, n, n, info, rdiag);
             }
+            zero_upper(s, w, n, n, r.count, nn);
+            inv_lower(s, w, n, n, inv.blk(c.off, r.first), n, r.count, nn, nn);
+            if (side == 1) trmm_lt(s, c.invCholZ.blk(c.off, r.first), n, n, c.invZ.blk(c.off, r.first), n, r.count, nn, nn);
         }
-        zero_upper(st, w1, n, n, r.count, nn);
-        inv_lower(st, w1, n, n, c.invCholX.blk(c.off, r.first), n, r.count, nn, nn);
-        zero_upper(st, w2, n, n, r.count, nn);
-        inv_lower(st, w2, n, n, c.invCholZ.blk(c.off, r.first), n, r.count, nn, nn);
-        trmm_lt(st, c.invCholZ.blk(c.off, r.first), n, n, c.invZ.blk(c.off, r.first), n, r.count, nn, nn);
     }
+    CK(cudaEventRecord(c.aux_join, c.aux));
+    CK(cudaStreamWaitEvent(st, c.aux_join, 0));
     int info[2];
     d2h(c, info, c.info.p, sizeof(info));
     return info[0] == 0 && info[1] == 0;
