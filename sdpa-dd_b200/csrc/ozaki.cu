@@ -25,11 +25,10 @@
 // then writes diagonals s+1 .. S+1 in one instruction: S x 2 K steps = 32
 // MMAs per tile for 16 slices.
 //
-// Epilogue: four consecutive diagonals combine exactly in int64 (2^21 A_d +
-// 2^14 A_d+1 + 2^7 A_d+2 + A_d+3 < 2^44).  The two smallest groups fold into
-// an int64 carry in units of 2^-104, the third joins it as a dd, the
-// largest (an exact double) is added, and the dd is scaled by 2^(e_i+e_j)
-// and subtracted from C.
+// Epilogue: four consecutive diagonals combine exactly into a double
+// (2^21 A_d + 2^14 A_d+1 + 2^7 A_d+2 + A_d+3 < 2^44: two int32 pairs and one
+// FMA), the four groups (2^-28 apart) sum to a dd through two TwoSums, and
+// the dd is scaled by 2^(e_i+e_j-35) and subtracted from C.
 //
 // Kernel layout: one persistent CTA per SM over the tiles of the lower
 // triangle (row-block major, so a CTA keeps its 128-row A slices in shared
@@ -294,7 +293,8 @@ __device__ __forceinline__ void tc_ld2(uint32_t taddr, int32_t *r) {
 // P_2j+1 are exact doubles (|G| < 2^44, one FMA each), so value = 2^-35
 // (G0 + G1 2^-28 + G2 2^-56 + G3 2^-84).  Two TwoSums leave only the
 // rounding of the two smallest parts' sum and of the final low part:
-// within 2^-106 of the value plus 2^-140 absolute.
+// within 2^-106 of the value plus 2^-140 absolute.  The result comes back
+// without its factor 2^-35, which the caller folds into the entry's scale.
 __device__ __forceinline__ void oz_entry_dd(const int32_t (*v)[2], int c, double &hi, double &lo) {
     double G[4];
 #pragma unroll
@@ -307,8 +307,8 @@ __device__ __forceinline__ void oz_entry_dd(const int32_t (*v)[2], int c, double
     double e2, s2 = ddm::two_sum(e1, cc, e2);
     double l, h = ddm::two_sum(s1, s2, l);
     h = ddm::fast_two_sum(h, l + (e2 + d), l);
-    hi = h * 0x1p-35;
-    lo = l * 0x1p-35;
+    hi = h;
+    lo = l;
 }
 
 // Epilogue warps 1-16: warp w reads tensor-memory lanes 32 (w mod 4) .. +31
@@ -375,7 +375,7 @@ __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_e
                 double phi, plo;
                 oz_entry_dd(v, c, phi, plo);
                 if (cc < ncol) {
-                    const int sc = ei + ej[cc];
+                    const int sc = ei + ej[cc] - 35;
                     dd_t p;
                     if (sc >= -1022 && sc <= 1023) {
                         const double pw = oz_pow2(sc);
