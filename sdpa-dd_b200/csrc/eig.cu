@@ -9,7 +9,7 @@
 //            eigenvector component to dd rounding).
 //   n <= 20  M = L (D L^T) by two Rgemm, then the smallest eigenvalue of the
 //            lower triangle of M (the reference's Rsyev "N","L") by
-//            Householder tridiagonalisation and bisection.
+//            Householder tridiagonalisation (one warp) and Sturm multisection.
 // The whole Lanczos loop runs in one CTA per block: no host round trip per
 // step.
 #include "newton.h"
@@ -273,69 +273,80 @@ __global__ void __launch_bounds__(LZ_THREADS) lanczos_kernel(const int *blk_ids,
 }
 
 // Smallest eigenvalue of the lower triangle of an n x n symmetric M
-// (n <= 32): Householder tridiagonalisation then bisection.  One thread.
-__global__ void small_min_eig_kernel(const int *blk_ids, const int *sizes, const long *off, const dd_t *Msp, dd_t *out) {
-    if (threadIdx.x != 0) return;
+// (n <= 32): Householder tridiagonalisation, then the warp multisection of
+// tri_min_eigenvalue.  One warp per block: the scalar sums of a reflector
+// on lane 0 in sequence, the products with A and the rank-2 update row by
+// row over the lanes, A in shared memory.
+__global__ void __launch_bounds__(32) small_min_eig_kernel(const int *blk_ids, const int *sizes, const long *off, const dd_t *Msp, dd_t *out) {
+    __shared__ dd_t A[32][33];
+    __shared__ dd_t v[32], p[32], d[32], e[32], e2[32];
+    __shared__ dd_t tau_s, K_s;
+    __shared__ int skip;
+    const int lane = threadIdx.x;
     const int b = blk_ids[blockIdx.x];
     const int n = sizes[b];
     const dd_t *M = Msp + off[b];
-    dd_t A[32][32], d[32], e[32], e2[32], v[32], p[32];
     for (int j = 0; j < n; ++j)
-        for (int i = j; i < n; ++i) {
-            A[i][j] = ld_dd(M + i + (long)n * j);
-            A[j][i] = A[i][j];
+        if (lane >= j && lane < n) {
+            const dd_t x = ld_dd(M + lane + (long)n * j);
+            A[lane][j] = x;
+            A[j][lane] = x;
         }
+    __syncwarp();
     for (int k = 0; k + 2 < n; ++k) {
-        dd_t s = dd_zero();
-        for (int i = k + 1; i < n; ++i) s = dd_acc(s, dd_mul(A[i][k], A[i][k]));
-        dd_t nrm = dd_sqrt(s);
-        if (dd_is_zero(nrm)) continue;
-        dd_t alpha = A[k + 1][k].hi < 0.0 ? nrm : dd_neg(nrm);
-        for (int i = 0; i < n; ++i) v[i] = dd_zero();
-        v[k + 1] = dd_sub(A[k + 1][k], alpha);
-        for (int i = k + 2; i < n; ++i) v[i] = A[i][k];
-        dd_t vv = dd_zero();
-        for (int i = k + 1; i < n; ++i) vv = dd_acc(vv, dd_mul(v[i], v[i]));
-        if (dd_is_zero(vv)) continue;
-        dd_t tau = dd_div(dd_from(2.0), vv);
-        // p = tau A v ; K = tau/2 v^T p ; w = p - K v ; A -= v w^T + w v^T
-        for (int i = 0; i < n; ++i) {
-            dd_t t = dd_zero();
-            for (int j = k + 1; j < n; ++j) t = dd_acc(t, dd_mul(A[i][j], v[j]));
-            p[i] = dd_mul(tau, t);
+        if (lane == 0) {
+            skip = 0;
+            dd_t s = dd_zero();
+            for (int i = k + 1; i < n; ++i) s = dd_acc(s, dd_mul(A[i][k], A[i][k]));
+            const dd_t nrm = dd_sqrt(s);
+            if (dd_is_zero(nrm)) {
+                skip = 1;
+            } else {
+                const dd_t alpha = A[k + 1][k].hi < 0.0 ? nrm : dd_neg(nrm);
+                for (int i = 0; i < n; ++i) v[i] = dd_zero();
+                v[k + 1] = dd_sub(A[k + 1][k], alpha);
+                for (int i = k + 2; i < n; ++i) v[i] = A[i][k];
+                dd_t vv = dd_zero();
+                for (int i = k + 1; i < n; ++i) vv = dd_acc(vv, dd_mul(v[i], v[i]));
+                if (dd_is_zero(vv))
+                    skip = 1;
+                else
+                    tau_s = dd_div(dd_from(2.0), vv);
+            }
         }
-        dd_t vp = dd_zero();
-        for (int i = k + 1; i < n; ++i) vp = dd_acc(vp, dd_mul(v[i], p[i]));
-        dd_t K = dd_mul(dd_mul_d(tau, 0.5), vp);
-        for (int i = 0; i < n; ++i) p[i] = dd_sub(p[i], dd_mul(K, v[i]));
-        for (int i = 0; i < n; ++i)
-            for (int j = 0; j < n; ++j) A[i][j] = dd_sub(dd_sub(A[i][j], dd_mul(v[i], p[j])), dd_mul(p[i], v[j]));
+        __syncwarp();
+        if (skip) continue;
+        const dd_t tau = tau_s;
+        // p = tau A v (row i on lane i)
+        if (lane < n) {
+            dd_t t = dd_zero();
+            for (int j = k + 1; j < n; ++j) t = dd_acc(t, dd_mul(A[lane][j], v[j]));
+            p[lane] = dd_mul(tau, t);
+        }
+        __syncwarp();
+        // K = tau/2 v^T p ; w = p - K v
+        if (lane == 0) {
+            dd_t vp = dd_zero();
+            for (int i = k + 1; i < n; ++i) vp = dd_acc(vp, dd_mul(v[i], p[i]));
+            K_s = dd_mul(dd_mul_d(tau, 0.5), vp);
+        }
+        __syncwarp();
+        if (lane < n) p[lane] = dd_sub(p[lane], dd_mul(K_s, v[lane]));
+        __syncwarp();
+        // A -= v w^T + w v^T (row i on lane i)
+        if (lane < n) {
+            const dd_t vi = v[lane], pi = p[lane];
+            for (int j = 0; j < n; ++j) A[lane][j] = dd_sub(dd_sub(A[lane][j], dd_mul(vi, p[j])), dd_mul(pi, v[j]));
+        }
+        __syncwarp();
     }
-    for (int i = 0; i < n; ++i) d[i] = A[i][i];
-    for (int i = 0; i + 1 < n; ++i) {
-        e[i] = A[i + 1][i];
-        e2[i] = dd_mul(e[i], e[i]);
+    if (lane < n) {
+        d[lane] = A[lane][lane];
+        if (lane + 1 < n) e[lane] = A[lane + 1][lane];
     }
-    dd_t lo = d[0], hi = d[0];
-    for (int i = 0; i < n; ++i) {
-        dd_t r = dd_zero();
-        if (i > 0) r = dd_add(r, dd_abs(e[i - 1]));
-        if (i + 1 < n) r = dd_add(r, dd_abs(e[i]));
-        lo = dd_min(lo, dd_sub(d[i], r));
-        hi = dd_max(hi, dd_add(d[i], r));
-    }
-    dd_t w = dd_sub(hi, lo);
-    lo = dd_sub(lo, dd_mul_d(w, 1e-10));
-    hi = dd_add(hi, dd_mul_d(w, 1e-10));
-    for (int it = 0; it < 400; ++it) {
-        dd_t mid = dd_mul_d(dd_add(lo, hi), 0.5);
-        if (!(dd_lt(lo, mid) && dd_lt(mid, hi))) break;
-        if (sturm_count(n, d, e2, mid) >= 1)
-            hi = mid;
-        else
-            lo = mid;
-    }
-    out[blockIdx.x] = dd_mul_d(dd_add(lo, hi), 0.5);
+    __syncwarp();
+    const dd_t lam = tri_min_eigenvalue(n, d, e, e2);
+    if (lane == 0) out[blockIdx.x] = lam;
 }
 
 // The small blocks (n <= 20) of one space: DLS2 = D L^T (Rgemm "N","T"),

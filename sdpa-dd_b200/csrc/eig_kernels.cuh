@@ -18,6 +18,6 @@ __global__ void __launch_bounds__(LZ_THREADS) lanczos_kernel(const int *blk_ids,
 
 // One warp per block id: smallest eigenvalue of the lower triangle of the
 // symmetric M (order <= 32) at Msp + off[b]; the result goes to out[blockIdx.x].
-__global__ void small_min_eig_kernel(const int *blk_ids, const int *sizes, const long *off, const dd_t *Msp, dd_t *out);
+__global__ void __launch_bounds__(32) small_min_eig_kernel(const int *blk_ids, const int *sizes, const long *off, const dd_t *Msp, dd_t *out);
 
 } // namespace sddd
