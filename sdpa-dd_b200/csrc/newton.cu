@@ -3,6 +3,7 @@
 #include "newton.h"
 
 #include <algorithm>
+#include <cstring>
 
 #include "blas.h"
 #include "devops.cuh"
@@ -118,7 +119,7 @@ void init_point(Context &c, dd_t lambda) {
 // Jal::getInvChol / getInvCholAndInv (sdpa_jordan.cpp:123-170): copy,
 // Rpotrf, zero the upper triangle, Rtrsm on the identity; for Z also
 // Z^-1 = L_Z^-T L_Z^-1 by Rtrmm.
-bool compute_inverse(Context &c) {
+void compute_inverse_async(Context &c) {
     cudaStream_t st = c.stream;
     if (!c.aux) {
         CK(cudaStreamCreateWithFlags(&c.aux, cudaStreamNonBlocking));
@@ -153,8 +154,25 @@ bool compute_inverse(Context &c) {
     }
     CK(cudaEventRecord(c.aux_join, c.aux));
     CK(cudaStreamWaitEvent(st, c.aux_join, 0));
+}
+
+bool compute_inverse(Context &c) {
+    compute_inverse_async(c);
+    ScalarBatch sb(c);
+    const int g = sb.inverse_info();
+    sb.fetch();
+    return sb.inverse_ok(g);
+}
+
+int ScalarBatch::inverse_info() {
+    const int g = group(1);
+    CK(cudaMemcpyAsync(c.scal.p + groups[g].first, c.info.p, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
+    return g;
+}
+
+bool ScalarBatch::inverse_ok(int g) const {
     int info[2];
-    d2h(c, info, c.info.p, sizeof(info));
+    std::memcpy(info, &host[groups[g].first], sizeof(info));
     return info[0] == 0 && info[1] == 0;
 }
 
@@ -244,22 +262,41 @@ void make_dz_dx(Context &c, bool dual_infeasible) {
 }
 
 // ------------------------------------------------------------ inner products
-static dd_t fetch_sum(Context &c, int nslots) {
-    std::vector<dd_t> h(nslots);
-    d2h(c, h.data(), c.scal.p, sizeof(dd_t) * nslots);
+// Each reduction writes its partial results (one per block, or one) to
+// slots of c.scal; a ScalarBatch lays several reductions side by side and
+// reads them all back with one copy, so that independent scalars of one
+// step cost one host round trip.  The host sums a group's slots in order
+// from zero with "+=", as the reference sums its per-block results.
+int ScalarBatch::group(int count) {
+    groups.push_back({used, count});
+    used += count;
+    if ((size_t)used > c.scal.n) throw Error(ERR_STATE, "scalar batch: more result slots than the context holds");
+    return (int)groups.size() - 1;
+}
+
+void ScalarBatch::fetch() {
+    host.resize(used);
+    if (used > 0) d2h(c, host.data(), c.scal.p, sizeof(dd_t) * used);
+}
+
+dd_t ScalarBatch::sum(int g) const {
     dd_t r = dd_zero();
-    for (int s = 0; s < nslots; ++s) r = dd_acc(r, h[s]);
+    for (int s = 0; s < groups[g].second; ++s) r = dd_acc(r, host[groups[g].first + s]);
     return r;
 }
 
+dd_t ScalarBatch::value(int g) const { return host[groups[g].first]; }
+
 // Lal::getInnerProduct(DenseLinearSpace, DenseLinearSpace)
 // (sdpa_linear.cpp:1571-1611): Rdot per block, summed with "+=".
-dd_t inner_space(Context &c, const Space &a, const Space &b) {
+int ScalarBatch::inner_space(const Space &a, const Space &b) {
+    const int g = group(c.nSDP);
+    dd_t *out = c.scal.p + groups[g].first;
     for (const BlockRun &r : c.runs) {
         const long nn = (long)r.n * r.n;
-        dot_batched(c.stream, a.blk(c.off, r.first), nn, b.blk(c.off, r.first), nn, nn, r.count, c.scal.p + r.first, c.red.p);
+        dot_batched(c.stream, a.blk(c.off, r.first), nn, b.blk(c.off, r.first), nn, nn, r.count, out + r.first, c.red.p);
     }
-    return fetch_sum(c, c.nSDP);
+    return g;
 }
 
 __global__ void sparse_inner_kernel(int n, int nnz, const int *row, const int *col, const dd_t *val, const dd_t *D, dd_t *out) {
@@ -290,7 +327,7 @@ __global__ void inner_C_small_kernel(const BlockView *views, const int *slot, co
 // Lal::getInnerProduct(SparseLinearSpace C, DenseLinearSpace X)
 // (sdpa_linear.cpp:1616-1650) over C's nonzero SDP blocks: one result slot
 // per such block, summed in block order on the host.
-dd_t inner_C(Context &c, const Space &x) {
+int ScalarBatch::inner_C(const Space &x) {
     if (c.c_slot_host.size() != (size_t)c.nSDP) {
         c.c_slot_host.assign(c.nSDP, -1);
         c.c_nslots = 0;
@@ -298,22 +335,53 @@ dd_t inner_C(Context &c, const Space &x) {
             if (c.blocks[l]->c_present) c.c_slot_host[l] = c.c_nslots++;
         c.c_slot.upload(c.c_slot_host, c.stream);
     }
-    if (c.c_nslots == 0) return dd_zero();
-    inner_C_small_kernel<<<c.nSDP, 32, 0, c.stream>>>(c.views.p, c.c_slot.p, c.d_off.p, x.buf.p, c.scal.p);
+    const int g = group(c.c_nslots);
+    if (c.c_nslots == 0) return g;
+    dd_t *out = c.scal.p + groups[g].first;
+    inner_C_small_kernel<<<c.nSDP, 32, 0, c.stream>>>(c.views.p, c.c_slot.p, c.d_off.p, x.buf.p, out);
     CK_LAUNCH();
     for (int l = 0; l < c.nSDP; ++l) {
         const BlockDev &bd = *c.blocks[l];
         const long nn = (long)bd.n * bd.n;
         if (bd.c_present && bd.c_dense && nn > DOT_SEQ_TERMS)
-            dot(c.stream, bd.c_dense_val.p, 1, x.blk(c.off, l), 1, nn, c.scal.p + c.c_slot_host[l], c.red.p + 256 * (c.c_slot_host[l] % 8));
+            dot(c.stream, bd.c_dense_val.p, 1, x.blk(c.off, l), 1, nn, out + c.c_slot_host[l], c.red.p + 256 * (c.c_slot_host[l] % 8));
     }
-    return fetch_sum(c, c.c_nslots);
+    return g;
 }
 
 // Lal::getInnerProduct(Vector, Vector): Rdot over m.
+int ScalarBatch::inner_b(const dd_t *v) {
+    const int g = group(1);
+    dot(c.stream, c.b.p, 1, v, 1, c.m, c.scal.p + groups[g].first, c.red.p);
+    return g;
+}
+
+// max |x_i| (Residuals::computeMaxNorm): one slot, taken as is.
+int ScalarBatch::maxabs_of(const dd_t *x, long n, int scratch) {
+    const int g = group(1);
+    maxabs(c.stream, x, n, c.scal.p + groups[g].first, c.red.p + 512 * scratch);
+    return g;
+}
+
+dd_t inner_space(Context &c, const Space &a, const Space &b) {
+    ScalarBatch sb(c);
+    const int g = sb.inner_space(a, b);
+    sb.fetch();
+    return sb.sum(g);
+}
+
+dd_t inner_C(Context &c, const Space &x) {
+    ScalarBatch sb(c);
+    const int g = sb.inner_C(x);
+    sb.fetch();
+    return sb.sum(g);
+}
+
 dd_t inner_b(Context &c, const dd_t *v) {
-    dot(c.stream, c.b.p, 1, v, 1, c.m, c.scal.p, c.red.p);
-    return fetch_sum(c, 1);
+    ScalarBatch sb(c);
+    const int g = sb.inner_b(v);
+    sb.fetch();
+    return sb.sum(g);
 }
 
 // ----------------------------------------------------------------- update
@@ -324,15 +392,22 @@ void update_point(Context &c, dd_t alphaP, dd_t alphaD) {
 }
 
 // -------------------------------------------------------------- residuals
-void residuals(Context &c, dd_t &normPrimal, dd_t &normDual) {
+// Residuals::compute (sdpa_dataset.cpp:625-645): the primal residual vector
+// and the dual residual matrix, then their max-abs norms into the batch.
+void ScalarBatch::residuals(int &gPrimal, int &gDual) {
     constraint_inner(c, c.X, c.b.p, c.primalVec.p);
     sum_yA(c, c.y.p, c.dualMat, 1, nullptr, &c.Z);
-    maxabs(c.stream, c.primalVec.p, c.m, c.scal.p, c.red.p);
-    maxabs(c.stream, c.dualMat.buf.p, c.space_len, c.scal.p + 1, c.red.p + 512);
-    dd_t h[2];
-    d2h(c, h, c.scal.p, sizeof(h));
-    normPrimal = h[0];
-    normDual = h[1];
+    gPrimal = maxabs_of(c.primalVec.p, c.m, 0);
+    gDual = maxabs_of(c.dualMat.buf.p, c.space_len, 1);
+}
+
+void residuals(Context &c, dd_t &normPrimal, dd_t &normDual) {
+    ScalarBatch sb(c);
+    int gp, gd;
+    sb.residuals(gp, gd);
+    sb.fetch();
+    normPrimal = sb.value(gp);
+    normDual = sb.value(gd);
 }
 
 __global__ void lambda_trace_kernel(const dd_t *S, const long *off, const int *sizes, int nb, double lambda, dd_t *out) {
@@ -345,10 +420,18 @@ __global__ void lambda_trace_kernel(const dd_t *S, const long *off, const int *s
     st_dd(out, r);
 }
 
-dd_t lambda_trace(Context &c, const Space &s, double lambda) {
-    lambda_trace_kernel<<<1, 32, 0, c.stream>>>(s.buf.p, c.d_off.p, c.d_sizes.p, c.nSDP, lambda, c.scal.p);
+int ScalarBatch::lambda_trace(const Space &s, double lambda) {
+    const int g = group(1);
+    lambda_trace_kernel<<<1, 32, 0, c.stream>>>(s.buf.p, c.d_off.p, c.d_sizes.p, c.nSDP, lambda, c.scal.p + groups[g].first);
     CK_LAUNCH();
-    return fetch_sum(c, 1);
+    return g;
+}
+
+dd_t lambda_trace(Context &c, const Space &s, double lambda) {
+    ScalarBatch sb(c);
+    const int g = sb.lambda_trace(s, lambda);
+    sb.fetch();
+    return sb.sum(g);
 }
 
 } // namespace sddd

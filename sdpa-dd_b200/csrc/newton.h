@@ -9,8 +9,36 @@ namespace sddd {
 // L_X^-1 = L_Z^-1 = I / sqrt(lambda), Z^-1 = I / lambda.
 void init_point(Context &c, dd_t lambda);
 // Solutions::computeInverse (sdpa_dataset.cpp:96-118); false when a
-// Cholesky factorisation of X or Z fails.
+// Cholesky factorisation of X or Z fails.  The _async form enqueues the
+// same work and leaves the two failure words in c.info.
 bool compute_inverse(Context &c);
+void compute_inverse_async(Context &c);
+
+// Several reductions' results side by side in c.scal, read back with one
+// copy (one host round trip): each call enqueues its kernels and returns a
+// group; after fetch(), sum(g) is the group's slots summed in order from
+// zero with "+=" (the reference's per-block sums) and value(g) a one-slot
+// group's value as it is.
+struct ScalarBatch {
+    Context &c;
+    int used = 0;
+    std::vector<std::pair<int, int>> groups; // (first slot, count)
+    std::vector<dd_t> host;
+    explicit ScalarBatch(Context &cc) : c(cc) {}
+    int group(int count);
+    int inner_space(const Space &a, const Space &b);
+    int inner_C(const Space &x);
+    int inner_b(const dd_t *v);
+    int lambda_trace(const Space &s, double lambda);
+    int maxabs_of(const dd_t *x, long n, int scratch);
+    void residuals(int &gPrimal, int &gDual);
+    // the failure words of compute_inverse_async (two ints in one slot)
+    int inverse_info();
+    void fetch();
+    dd_t sum(int g) const;
+    dd_t value(int g) const;
+    bool inverse_ok(int g) const;
+};
 // Newton::compute_rMat + Newton::Make_gVec (sdpa_newton.cpp:821-893).
 // dual_infeasible: phase is pFEAS or noINFO.
 void make_rhs(Context &c, bool corrector, dd_t beta_mu, bool dual_infeasible);

@@ -250,7 +250,10 @@ int Solver::step(FILE *display, FILE *out) {
     last_alphaPredD = alpha_dual;
     // DirectionParameter::MehrotraCorrector (sdpa_parts.cpp:498-529)
     {
-        dd_t xv = inner_space(c, c.X, c.Dz), uz = inner_space(c, c.Dx, c.Z), uv = inner_space(c, c.Dx, c.Dz);
+        ScalarBatch sb(c);
+        const int gxv = sb.inner_space(c.X, c.Dz), guz = sb.inner_space(c.Dx, c.Z), guv = sb.inner_space(c.Dx, c.Dz);
+        sb.fetch();
+        dd_t xv = sb.sum(gxv), uz = sb.sum(guz), uv = sb.sum(guv);
         dd_t muTarget = mu_after(mu_current, alpha_primal, alpha_dual, uz, xv, uv, c.nDim);
         dd_t v = dd_div(muTarget, mu_current);
         if (dd_lt_d(v, 1.0)) v = dd_mul(v, v);
@@ -298,7 +301,10 @@ int Solver::step(FILE *display, FILE *out) {
         clamp_steps(*this, primal, dual);
         if (reduction_on && (phase == noINFO || phase == pFEAS || phase == dFEAS)) {
             const dd_t xi = dd_from(3.0);
-            dd_t xv = inner_space(c, c.X, c.Dz), uz = inner_space(c, c.Dx, c.Z), uv = inner_space(c, c.Dx, c.Dz);
+            ScalarBatch sb(c);
+            const int gxv = sb.inner_space(c.X, c.Dz), guz = sb.inner_space(c.Dx, c.Z), guv = sb.inner_space(c.Dx, c.Dz);
+            sb.fetch();
+            dd_t xv = sb.sum(gxv), uz = sb.sum(guz), uv = sb.sum(guv);
             dd_t thetaMax = smax(dd_mul(d_sub_dd(1.0, primal), theta_primal), dd_mul(d_sub_dd(1.0, dual), theta_dual));
             dd_t muNew = mu_after(mu_current, primal, dual, uz, xv, uv, c.nDim);
             while (dd_gt(dd_mul(dd_mul(thetaMax, thetaMax), mu_initial), dd_mul(xi, muNew))) {
@@ -311,9 +317,12 @@ int Solver::step(FILE *display, FILE *out) {
             }
         }
         if (phase == pdFEAS) {
-            dd_t oD = inner_b(c, c.y.p), oP = inner_C(c, c.X);
-            dd_t incD = dd_muleq(inner_b(c, c.Dy.p), dual);
-            dd_t incP = dd_muleq(inner_C(c, c.Dx), primal);
+            ScalarBatch sb(c);
+            const int goD = sb.inner_b(c.y.p), goP = sb.inner_C(c.X), giD = sb.inner_b(c.Dy.p), giP = sb.inner_C(c.Dx);
+            sb.fetch();
+            dd_t oD = sb.sum(goD), oP = sb.sum(goP);
+            dd_t incD = dd_muleq(sb.sum(giD), dual);
+            dd_t incP = dd_muleq(sb.sum(giP), primal);
             dd_t maxRatio = dd_div(dd_sub(oD, oP), dd_sub(incP, incD));
             if (dd_gt_d(maxRatio, 0.0) && dd_lt_d(maxRatio, 1.0)) {
                 primal = dd_muleq(primal, maxRatio);
@@ -333,11 +342,26 @@ int Solver::step(FILE *display, FILE *out) {
         clk.collect();
         return 4;
     }
+    // Solutions::computeInverse, then everything the loop tail reads from
+    // the new point (mu, the residual norms, the objectives and the
+    // SolveInfo traces), read back together
     cudaEvent_t u0 = clk.mark();
-    bool ok = compute_inverse(c);
+    compute_inverse_async(c);
     cudaEvent_t u1 = clk.mark();
     clk.span(u0, u1, &tm.zMatTime);
-    if (!ok) {
+    ScalarBatch tail(c);
+    const int g_inv = tail.inverse_info();
+    const int g_mu = tail.inner_space(c.X, c.Z);
+    cudaEvent_t r0 = clk.mark();
+    int g_np, g_nd;
+    tail.residuals(g_np, g_nd);
+    cudaEvent_t r1 = clk.mark();
+    clk.span(r0, r1, &tm.updateRes);
+    const int g_oP = tail.inner_C(c.X), g_oD = tail.inner_b(c.y.p);
+    const int g_x0z = c.has_init ? tail.inner_space(c.init_X, c.Z) : tail.lambda_trace(c.Z, param.lambdaStar);
+    const int g_xz0 = c.has_init ? tail.inner_space(c.X, c.init_Z) : tail.lambda_trace(c.X, param.lambdaStar);
+    tail.fetch();
+    if (!tail.inverse_ok(g_inv)) {
         if (display) std::fprintf(display, "cannot cholesky decomposition\nCould you try with smaller gammaStar?\ncannot move\n");
         clk.collect();
         return 4;
@@ -348,26 +372,24 @@ int Solver::step(FILE *display, FILE *out) {
         theta_dual = dd_abs(dd_mul(d_sub_dd(1.0, alpha_dual), theta_dual));
     }
     // AverageComplementarity::update (sdpa_parts.cpp:585-589)
-    mu_current = dd_div_d(inner_space(c, c.X, c.Z), (double)c.nDim);
+    mu_current = dd_div_d(tail.sum(g_mu), (double)c.nDim);
     // Residuals::update
-    cudaEvent_t r0 = clk.mark();
-    residuals(c, normPrimalVec, normDualMat);
-    cudaEvent_t r1 = clk.mark();
-    clk.span(r0, r1, &tm.updateRes);
+    normPrimalVec = tail.value(g_np);
+    normDualMat = tail.value(g_nd);
     // RatioInitResCurrentRes::update_exact (sdpa_parts.cpp:644-655)
     theta_primal = dd_gt_d(initNormPrimalVec, 1.0e-10) ? dd_div(normPrimalVec, initNormPrimalVec) : ZERO;
     theta_dual = dd_gt_d(initNormDualMat, 1.0e-10) ? dd_div(normDualMat, initNormDualMat) : ZERO;
     // SolveInfo::update (sdpa_parts.cpp:690-739 with an initial point file,
     // :741-770 with lambda I)
     {
-        objValPrimal = inner_C(c, c.X);
-        objValDual = inner_b(c, c.y.p);
+        objValPrimal = tail.sum(g_oP);
+        objValDual = tail.sum(g_oD);
         const dd_t primal = theta_primal, dual = theta_dual, omega = dd_from(param.omegaStar);
         rho = ZERO;
         const dd_t x0z0 = dd_mul_d(mu_initial, (double)c.nDim);
         const dd_t xMatzMat = dd_mul_d(mu_current, (double)c.nDim);
-        const dd_t x0zMat = c.has_init ? inner_space(c, c.init_X, c.Z) : lambda_trace(c, c.Z, param.lambdaStar);
-        const dd_t xMatz0 = c.has_init ? inner_space(c, c.X, c.init_Z) : lambda_trace(c, c.X, param.lambdaStar);
+        const dd_t x0zMat = tail.sum(g_x0z);
+        const dd_t xMatz0 = tail.sum(g_xz0);
         const dd_t accuracy = dd_from(param.epsilonDash);
         if (dd_le(normPrimalVec, accuracy))
             if (dd_lt(xMatz0, etaPrimal)) etaPrimal = xMatz0;
