@@ -41,7 +41,10 @@ CASES = {
     "theta_nv120": (lambda: P.theta(nv=120, p=0.5, seed=2), 1e-25),
 }
 # (threads) of the runs beside the one-thread run
-VARIANTS = {"maxcut_n500": (2, 4, 3), "control_100_50_m1326": (2,), "theta_nv120": (2, 4)}
+# theta_nv120 ends where its mu stalls near 1.2e-25: the runs part in phase
+# (pFEAS after a too-small step, or pdOPT) and iteration count, so it has
+# more of them
+VARIANTS = {"maxcut_n500": (2, 4, 3), "control_100_50_m1326": (2,), "theta_nv120": (2, 4, 3, 6, 8)}
 
 PHASES = ["noINFO", "pFEAS", "dFEAS", "pdFEAS", "pdINF", "pFEAS_dINF", "pINF_dFEAS", "pdOPT", "pUNBD", "dUNBD"]
 # Phase::reverse (sdpa_parts.cpp:956-990), applied before printing
