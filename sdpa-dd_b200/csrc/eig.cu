@@ -38,8 +38,25 @@ __device__ int sturm_count(int k, const dd_t *d, const dd_t *e2, dd_t x) {
     return c;
 }
 
+// The same count on the high parts in double: a quick estimate only.
+__device__ int sturm_count_d(int k, const dd_t *d, const dd_t *e2, double x) {
+    int c = 0;
+    double q = d[0].hi - x;
+    if (q < 0.0) c++;
+    for (int i = 1; i < k; ++i) {
+        if (q == 0.0) q = 1e-300;
+        q = (d[i].hi - x) - e2[i - 1].hi / q;
+        if (q < 0.0) c++;
+    }
+    return c;
+}
+
 // Smallest eigenvalue of the k x k tridiagonal (d, e) by multisection over
-// the 32 lanes of one warp; every lane returns the same value.
+// the 32 lanes of one warp; every lane returns the same value.  A first
+// multisection in double on the high parts narrows the Gershgorin bracket
+// to ~2^-40 of the spectrum's scale; that bracket is kept only when dd
+// Sturm counts confirm it (no eigenvalue below its lower end, one below
+// its upper end), and the dd multisection then runs from it.
 __device__ dd_t tri_min_eigenvalue(int k, const dd_t *d, const dd_t *e, dd_t *e2) {
     const int lane = threadIdx.x & 31;
     dd_t lo = d[0], hi = d[0];
@@ -57,6 +74,36 @@ __device__ dd_t tri_min_eigenvalue(int k, const dd_t *d, const dd_t *e, dd_t *e2
     dd_t w = dd_sub(hi, lo);
     lo = dd_sub(lo, dd_mul_d(w, 1e-10));
     hi = dd_add(hi, dd_mul_d(w, 1e-10));
+    {
+        double dlo = lo.hi, dhi = hi.hi;
+        for (int round = 0; round < 12; ++round) {
+            const double width = dhi - dlo;
+            const double x = dlo + width * (double)(lane + 1) / 33.0;
+            const bool below = !(x > dlo) ? false : !(x < dhi) ? true : sturm_count_d(k, d, e2, x) >= 1;
+            const unsigned ball = __ballot_sync(0xffffffffu, below);
+            double nlo, nhi;
+            if (ball == 0) {
+                nlo = dlo + width * 32.0 / 33.0;
+                nhi = dhi;
+            } else {
+                const int first = __ffs(ball) - 1;
+                nhi = dlo + width * (double)(first + 1) / 33.0;
+                nlo = first == 0 ? dlo : dlo + width * (double)first / 33.0;
+            }
+            if (!(nlo < nhi) || (nlo == dlo && nhi == dhi)) break;
+            dlo = nlo;
+            dhi = nhi;
+        }
+        const double rad = (fabs(lo.hi) + fabs(hi.hi) + (hi.hi - lo.hi)) * 0x1p-40;
+        const dd_t blo = dd_max(lo, dd_from(dlo - rad)), bhi = dd_min(hi, dd_from(dhi + rad));
+        int okv = 1;
+        if (lane == 0) okv = sturm_count(k, d, e2, blo) == 0;
+        if (lane == 1) okv = dd_lt(blo, bhi) && sturm_count(k, d, e2, bhi) >= 1;
+        if (__all_sync(0xffffffffu, okv)) {
+            lo = blo;
+            hi = bhi;
+        }
+    }
     for (int round = 0; round < 40; ++round) {
         const dd_t width = dd_sub(hi, lo);
         // 32 interior points x_lane = lo + width (lane+1)/33; the smallest
