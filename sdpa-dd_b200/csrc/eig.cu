@@ -306,7 +306,8 @@ __global__ void __launch_bounds__(LZ_THREADS) lanczos_kernel(const int *blk_ids,
                 }
             }
         }
-        if (tid == 0) S.rr = seq_dot(n, r, r);
+        // r.r on warp 1, beside warp 0's checkpoint
+        if (tid == 32) S.rr = seq_dot(n, r, r);
         __syncthreads();
         if (tid == 0) {
             S.beta = dd_sqrt(S.rr);
