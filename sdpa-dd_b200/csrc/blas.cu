@@ -281,11 +281,14 @@ __global__ void __launch_bounds__(DIAG_THREADS) potrf_diag_kernel(dd_t *A, long 
 constexpr int PANEL_ROWS = 32;
 static_assert(PANEL_ROWS == 32, "potrf_panel_kernel maps one row to each lane");
 constexpr int PANEL_THREADS = 512;
+// L11's lower triangle packed by rows: entry (j, k), k <= j, at j (j+1)/2 + k
+// (half the shared memory of the square, so three CTAs fit an SM).
+__device__ __forceinline__ int tri_at(int j, int k) { return j * (j + 1) / 2 + k; }
 __global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, long lda, int n, int nb, int c0, const int *info, const dd_t *rdiag) {
     extern __shared__ double2 sm[];
-    double2 *L11 = sm;                 // nb x nb
-    double2 *P = sm + nb * nb;         // PANEL_ROWS x nb, column-major ld PANEL_ROWS
-    double2 *R = P + PANEL_ROWS * nb;  // nb reciprocals
+    double2 *L11 = sm;                         // lower triangle of nb x nb, packed
+    double2 *P = sm + nb * (nb + 1) / 2;       // PANEL_ROWS x nb, column-major ld PANEL_ROWS
+    double2 *R = P + PANEL_ROWS * nb;          // nb reciprocals
     if (*info != 0) return;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int r0 = c0 + nb + blockIdx.x * PANEL_ROWS;
@@ -293,7 +296,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, lon
     if (rows <= 0) return;
     for (int e = tid; e < nb * nb; e += nt) {
         int i = e % nb, j = e / nb;
-        L11[e] = (i >= j) ? *reinterpret_cast<const double2 *>(A + (c0 + i) + lda * (long)(c0 + j)) : make_double2(0.0, 0.0);
+        if (i >= j) L11[tri_at(i, j)] = *reinterpret_cast<const double2 *>(A + (c0 + i) + lda * (long)(c0 + j));
     }
     for (int e = tid; e < PANEL_ROWS * nb; e += nt) {
         int i = e % PANEL_ROWS, j = e / PANEL_ROWS;
@@ -318,7 +321,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, lon
             const double2 xik = P[lane + PANEL_ROWS * k];
             const dd_t x_ik = dd_make(xik.x, xik.y);
             for (int j = k + 1 + warp; j < nb; j += nw) {
-                const double2 ljk = L11[j + nb * k], v = P[lane + PANEL_ROWS * j];
+                const double2 ljk = L11[tri_at(j, k)], v = P[lane + PANEL_ROWS * j];
                 dd_t y = dd_sub(dd_make(v.x, v.y), dd_mul(dd_make(ljk.x, ljk.y), x_ik));
                 if (j == k + 1) y = dd_mul(rk(k + 1), y);
                 P[lane + PANEL_ROWS * j] = make_double2(y.hi, y.lo);
@@ -364,7 +367,7 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
     static thread_local bool attr[64] = {};
     const int nbmax = POTRF_NB;
     const size_t smem_diag = sizeof(double2) * nbmax * nbmax;
-    const size_t smem_panel = sizeof(double2) * (nbmax * nbmax + PANEL_ROWS * nbmax + nbmax);
+    const size_t smem_panel = sizeof(double2) * (nbmax * (nbmax + 1) / 2 + PANEL_ROWS * nbmax + nbmax);
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (!attr[dev & 63]) {
@@ -390,7 +393,7 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
             if (below <= 0) break;
             {
                 PROF_SCOPE("potrf_panel", st);
-                potrf_panel_kernel<<<ceil_div(below, PANEL_ROWS), PANEL_THREADS, sizeof(double2) * (nb * nb + PANEL_ROWS * nb + nb), st>>>(
+                potrf_panel_kernel<<<ceil_div(below, PANEL_ROWS), PANEL_THREADS, sizeof(double2) * (nb * (nb + 1) / 2 + PANEL_ROWS * nb + nb), st>>>(
                     A, lda, n, nb, c0, info_dev, rdiag_dev);
                 CK_LAUNCH();
             }
@@ -427,7 +430,7 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
         if (below <= 0) break;
         {
             PROF_SCOPE("potrf_panel", st);
-            potrf_panel_kernel<<<ceil_div(below, PANEL_ROWS), PANEL_THREADS, sizeof(double2) * (nb * nb + PANEL_ROWS * nb + nb), st>>>(A, lda, n, nb, c0, info_dev,
+            potrf_panel_kernel<<<ceil_div(below, PANEL_ROWS), PANEL_THREADS, sizeof(double2) * (nb * (nb + 1) / 2 + PANEL_ROWS * nb + nb), st>>>(A, lda, n, nb, c0, info_dev,
                                                                                                                           rdiag_dev);
             CK_LAUNCH();
         }
