@@ -211,6 +211,8 @@ def batch_measure(sddd, device, rank, world, args):
     # independent problems shard over ranks by work, no data-path exchange
     mine = shard.partition_by_work([shard.work_estimate(m, [n]) for _, n, m in paths], world)[rank]
     with sddd.Batch(device, args.batch_workers) as bt:
+        if args.batch_core >= 0 and bt.L.sddd_batch_set_core(bt.h, args.batch_core) != 0:
+            raise RuntimeError("sddd_batch_set_core failed")
         for q in mine:
             path, n, m = paths[q]
             bt.add_file(path, m, n * n)
@@ -227,6 +229,7 @@ def batch_measure(sddd, device, rank, world, args):
            "solves_per_s": len(paths) / dt,
            "solves_per_s_basis": "every problem run to the end of its main loop, whatever its final phase (phases below)",
            "pdopt_solves_per_s": n_opt / dt, "pdOPT": n_opt, "seconds": dt, "ranks": world, "workers": args.batch_workers or "default",
+           "batched_core": {-1: "default (on)", 0: "off", 1: "on"}[args.batch_core],
            "phases_rank0": counts, "problems_rank0": len(mine),
            "mean_iterations_rank0": (sum(r.iterations for r in res) / len(res)) if res else None}
     exe = ROOT / "oracle" / "_ref" / "sdpa_dd"
@@ -732,6 +735,7 @@ def main():
     ap.add_argument("--no-solve", action="store_true", help="skip the two solves to relative gap 1e-25")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched workload (256 small SDPs)")
     ap.add_argument("--batch-workers", type=int, default=0, help="host workers of the batched workload (0: the library's default)")
+    ap.add_argument("--batch-core", type=int, default=-1, choices=[-1, 0, 1], help="batched Newton core off (0) or on (1); -1: the library's default")
     ap.add_argument("--batch-only", action="store_true", help="run the batched workload alone and print its figures")
     args = ap.parse_args()
     if args.profile_case == "sparse":
