@@ -360,7 +360,7 @@ int adjoint_limit(Context &c, const dd_t *g_x, const dd_t *g_Y, const dd_t *g_X,
     }
     int info = 0;
     d2h(c, &info, c.info.p, sizeof(int));
-    if (info != 0) throw Error(ERR_STATE, "adjoint: Z is not positive definite on the null space of X");
+    if (potrf_info_check(info) != 0) throw Error(ERR_STATE, "adjoint: Z is not positive definite on the null space of X");
     // the originals, restored at the end
     CK(cudaMemcpyAsync(c.lim_Xs.buf.p, c.X.buf.p, sizeof(dd_t) * L, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(c.lim_Zs.buf.p, c.invZ.buf.p, sizeof(dd_t) * L, cudaMemcpyDeviceToDevice, st));

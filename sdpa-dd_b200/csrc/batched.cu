@@ -501,7 +501,7 @@ int CoreEngine::schur_factor(Context &c) {
     }
     int info = 0;
     d2h(c, &info, c.info.p, sizeof(int));
-    return info;
+    return potrf_info_check(info);
 }
 
 std::string CoreEngine::tuning() const {

@@ -18,6 +18,7 @@
 // The blocking below (tiles, panels) is the B200 schedule; it never
 // reorders the operations that land on one entry.
 #include "blas.h"
+#include "bulk.cuh"
 #include "ozaki.h"
 #include "prof.h"
 
@@ -193,145 +194,216 @@ void gemm(cudaStream_t st, char ta, char tb, int mode, int M, int N, int K, cons
 }
 
 // ==================================================================== POTRF
-// Diagonal block: right-looking dd Cholesky of an nb x nb block held in
-// shared memory (lower triangle).  On a non-positive or NaN pivot the
-// 1-based global column goes to *info and the block stops (Rpotrf2's n=1
-// test, mplapack/Rpotrf2.cpp).  1/L(j,j) for the panel goes to rdiag.
-// Step k: warp 0 takes column k+1 through its step-k update, its pivot
-// (sqrt, reciprocal) and its scaling, while the other warps apply the
-// step-k update to columns k+2 and beyond (one column per warp at a time,
-// one row per lane); one barrier per step.  Every
-// entry sees the same operations in the same order as the column-by-column
-// form: x(i,j) -= L(j,k) L(i,k) for k ascending, then the scaling.
+// Diagonal block: right-looking dd Cholesky of an nb x nb block, nb <= 64.
+// On a non-positive or NaN pivot the 1-based global column goes to *info
+// and the block is left as it was (Rpotrf2's n = 1 test,
+// mplapack/Rpotrf2.cpp).  1/L(j,j) for the panel goes to rdiag.
+// Dataflow form, with no CTA-wide barrier between columns: warp w owns
+// columns w and w + 32 in registers (lane l holds rows j + l and j + l + 32
+// of column j).  When column k is final (pivot, scaling) its owner copies
+// it to shared memory and its 32 lanes arrive on column k's mbarrier;
+// every warp waits for that barrier, then subtracts column k's term from
+// its own columns right of k, the owner of column k + 1 taking that column
+// first and finishing it at once, so that one pivot follows the next
+// through a single warp.  Every entry sees the same operations in the same
+// order as the column-by-column form: x(i,j) -= L(j,k) L(i,k) for k
+// ascending, then the sqrt (diagonal) or the scaling by 1/L(j,j).
 constexpr int DIAG_THREADS = 1024;
+constexpr unsigned long long DIAG_WAIT_NS = 2000000000ull; // one column's wait, at most
+static_assert(POTRF_NB <= 64 && DIAG_THREADS == 1024, "two columns a warp, two rows a lane");
+__device__ __forceinline__ bool diag_wait(uint64_t *b) {
+    if (mbar_try_wait(b, 0)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    while (!mbar_try_wait(b, 0))
+        if (globaltimer_ns() - t0 > DIAG_WAIT_NS) return false;
+    return true;
+}
 __global__ void __launch_bounds__(DIAG_THREADS) potrf_diag_kernel(dd_t *A, long lda, int nb, int c0, int *info, dd_t *rdiag, long sA) {
     extern __shared__ double2 sm[];
-    double2 *S = sm; // nb x nb, column-major
+    double2 *S = sm; // nb x nb, column-major: the final columns
+    __shared__ uint64_t bar[POTRF_NB];
     __shared__ int fail;
     A += blockIdx.x * sA; // CTA b: matrix b of a batch of equal blocks (rdiag null then)
     if (*info != 0) return;
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
-    for (int e = tid; e < nb * nb; e += nt) {
-        int i = e % nb, j = e / nb;
-        S[e] = (i >= j) ? *reinterpret_cast<const double2 *>(A + (c0 + i) + lda * (long)(c0 + j)) : make_double2(0.0, 0.0);
-    }
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid < nb) mbar_init(&bar[tid], 32);
     if (tid == 0) fail = 0;
     __syncthreads();
-    auto at = [&](int i, int j) -> dd_t {
-        const double2 v = S[i + nb * j];
-        return dd_make(v.x, v.y);
-    };
-    auto put = [&](int i, int j, dd_t x) { S[i + nb * j] = make_double2(x.hi, x.lo); };
-    // warp 0: pivot of column col (sqrt, 1/L) and the scaling below it
-    auto finish_column = [&](int col) {
+    volatile int *vfail = &fail;
+    dd_t x[2][2];
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int j = warp + 32 * c, i = j + lane + 32 * r;
+            x[c][r] = (j < nb && i < nb) ? ld_dd(A + (c0 + i) + lda * (long)(c0 + j)) : dd_from(0.0);
+        }
+    // Column warp + 32 c: pivot (lane 0 holds the diagonal), scaling, copy
+    // to shared memory, arrival.  False when the pivot fails.
+    auto finish = [&](const int c) -> bool {
+        const int j = warp + 32 * c;
         int bad = 0;
         double rh = 0.0, rl = 0.0;
         if (lane == 0) {
-            const dd_t d = at(col, col);
+            const dd_t d = x[c][0];
             if (dd_le_d(d, 0.0) || dd_isnan(d)) {
                 bad = 1;
-                fail = 1;
-                *info = c0 + col + 1;
+                *vfail = 1;
+                *info = c0 + j + 1;
             } else {
                 const dd_t l = dd_sqrt(d);
-                put(col, col, l);
+                x[c][0] = l;
                 const dd_t r = dd_div(dd_from(1.0), l);
-                if (rdiag) rdiag[col] = r;
+                if (rdiag) rdiag[j] = r;
                 rh = r.hi;
                 rl = r.lo;
             }
         }
-        if (__shfl_sync(0xffffffffu, bad, 0)) return;
-        const dd_t r = dd_make(__shfl_sync(0xffffffffu, rh, 0), __shfl_sync(0xffffffffu, rl, 0));
-        for (int i = col + 1 + lane; i < nb; i += 32) put(i, col, dd_mul(r, at(i, col)));
-        __syncwarp();
-    };
-    if (warp == 0) finish_column(0);
-    __syncthreads();
-    if (fail) return;
-    for (int k = 0; k + 1 < nb; ++k) {
-        if (warp == 0) {
-            const dd_t l = at(k + 1, k);
-            for (int i = k + 1 + lane; i < nb; i += 32) put(i, k + 1, dd_sub(at(i, k + 1), dd_mul(l, at(i, k))));
-            __syncwarp();
-            finish_column(k + 1);
-        } else {
-            // warps 1.. take the columns k+2.. round-robin, lanes the rows
-            // of the column's lower part
-            for (int j = k + 2 + warp - 1; j < nb; j += nt / 32 - 1) {
-                const dd_t ljk = at(j, k);
-                for (int i = j + lane; i < nb; i += 32) put(i, j, dd_sub(at(i, j), dd_mul(ljk, at(i, k))));
+        bad = __shfl_sync(0xffffffffu, bad, 0);
+        if (!bad) {
+            const dd_t r = dd_make(__shfl_sync(0xffffffffu, rh, 0), __shfl_sync(0xffffffffu, rl, 0));
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int i = j + lane + 32 * q;
+                if (i < nb) {
+                    if (i > j) x[c][q] = dd_mul(r, x[c][q]);
+                    S[i + nb * j] = make_double2(x[c][q].hi, x[c][q].lo);
+                }
             }
         }
-        __syncthreads();
-        if (fail) return;
+        mbar_arrive(&bar[j]);
+        return !bad;
+    };
+    // column warp + 32 c takes column k's term
+    auto update = [&](const int c, const int k) {
+        const int j = warp + 32 * c;
+        const double2 l = S[j + nb * k];
+        const dd_t ljk = dd_make(l.x, l.y);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int i = j + lane + 32 * q;
+            if (i < nb) {
+                const double2 v = S[i + nb * k];
+                x[c][q] = dd_sub(x[c][q], dd_mul(ljk, dd_make(v.x, v.y)));
+            }
+        }
+    };
+    const bool two = warp + 32 < nb;
+    const int last = two ? warp + 32 : (warp < nb ? warp : -1); // the warp's last column
+    bool ok = true;
+    if (warp == 0 && nb > 0) ok = finish(0);
+    for (int k = 0; ok && k < last; ++k) {
+        // warp-uniform outcomes: the lanes go on together or stop together
+        if (!__all_sync(0xffffffffu, diag_wait(&bar[k]))) {
+            if (lane == 0) {
+                *vfail = 2;
+                atomicCAS(info, 0, -1);
+            }
+            break;
+        }
+        if (__any_sync(0xffffffffu, *vfail != 0)) break;
+        if (((k + 1) & 31) == warp) {
+            // this warp owns column k + 1
+            if (k + 1 < 32) {
+                update(0, k);
+                ok = finish(0);
+                if (ok && two) update(1, k);
+            } else {
+                update(1, k);
+                ok = finish(1);
+            }
+        } else {
+            if (warp > k) update(0, k);
+            if (two) update(1, k);
+        }
     }
-    for (int e = tid; e < nb * nb; e += nt) {
-        int i = e % nb, j = e / nb;
-        if (i >= j) *reinterpret_cast<double2 *>(A + (c0 + i) + lda * (long)(c0 + j)) = S[e];
-    }
+    __syncthreads();
+    if (*vfail) return;
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int j = warp + 32 * c, i = j + lane + 32 * r;
+            if (j < nb && i < nb) st_dd(A + (c0 + i) + lda * (long)(c0 + j), x[c][r]);
+        }
 }
 
-// Panel rows below the diagonal block: each CTA takes PANEL_ROWS rows and
-// solves them against L11 in shared memory (Rtrsm "Right", "Lower",
-// "Transpose": x(i,j) -= L(j,k) x(i,k) for k < j, then x(i,j) *= 1/L(j,j)).
-// Each thread owns fixed entries; at step k it subtracts column k's term
-// from its entries right of k and, for column k+1, applies the scaling at
-// once (the entry is final then): one barrier per step.
-constexpr int PANEL_ROWS = 32;
-static_assert(PANEL_ROWS == 32, "potrf_panel_kernel maps one row to each lane");
-constexpr int PANEL_THREADS = 512;
-// L11's lower triangle packed by rows: entry (j, k), k <= j, at j (j+1)/2 + k
-// (half the shared memory of the square, so three CTAs fit an SM).
+// Panel rows below the diagonal block (Rtrsm "Right", "Lower", "Transpose":
+// x(i,j) -= L(j,k) x(i,k) for k < j ascending, then x(i,j) *= 1/L(j,j)).
+// Rows are independent, so a warp solves PANEL_WROWS rows by itself, with
+// no barrier: lane = (column class c, row r), c = lane / PANEL_WROWS, and
+// the lane holds the row's columns c, c + PANEL_CLASSES, ... in registers.
+// At step k the holder of x(r,k) passes it to the row's other lanes by
+// shuffle; every lane subtracts the step's term from its columns right of
+// k, and the holder of column k + 1 then scales it (the entry is final).
+// Rounds of PANEL_CLASSES steps: in round q, slot s holds column
+// c + PANEL_CLASSES (q + s) (the slots rotate by one between rounds, and the
+// column leaving slot 0 is final and goes back to memory); the rounds are
+// unrolled so that each one updates exactly its live slots, without
+// branches between the slots' independent chains.  L11 (lower triangle,
+// packed by rows) and the reciprocals are shared by the CTA's warps.  The
+// panel is POTRF_NB columns wide.
+constexpr int PANEL_CLASSES = 16;                           // lanes a row
+constexpr int PANEL_WROWS = 32 / PANEL_CLASSES;             // rows a warp
+constexpr int PANEL_SLOTS = POTRF_NB / PANEL_CLASSES;       // columns a lane
+constexpr int PANEL_THREADS = 128;
+constexpr int PANEL_ROWS = PANEL_WROWS * (PANEL_THREADS / 32); // rows a CTA
+static_assert(POTRF_NB % PANEL_CLASSES == 0 && 32 % PANEL_CLASSES == 0, "panel lane map");
+constexpr size_t PANEL_SMEM = sizeof(double2) * (POTRF_NB * (POTRF_NB + 1) / 2 + POTRF_NB);
+// entry (j, k), k <= j, of a lower triangle packed by rows
 __device__ __forceinline__ int tri_at(int j, int k) { return j * (j + 1) / 2 + k; }
-__global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, long lda, int n, int nb, int c0, const int *info, const dd_t *rdiag) {
+__global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, long lda, int n, int c0, const int *info, const dd_t *rdiag) {
+    constexpr int NB = POTRF_NB, C = PANEL_CLASSES, W = PANEL_WROWS, NS = PANEL_SLOTS;
     extern __shared__ double2 sm[];
-    double2 *L11 = sm;                         // lower triangle of nb x nb, packed
-    double2 *P = sm + nb * (nb + 1) / 2;       // PANEL_ROWS x nb, column-major ld PANEL_ROWS
-    double2 *R = P + PANEL_ROWS * nb;          // nb reciprocals
+    double2 *L11 = sm;                   // lower triangle of NB x NB, packed
+    double2 *R = sm + NB * (NB + 1) / 2; // NB reciprocals
     if (*info != 0) return;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int r0 = c0 + nb + blockIdx.x * PANEL_ROWS;
-    const int rows = min(PANEL_ROWS, n - r0);
-    if (rows <= 0) return;
-    for (int e = tid; e < nb * nb; e += nt) {
-        int i = e % nb, j = e / nb;
-        if (i >= j) L11[tri_at(i, j)] = *reinterpret_cast<const double2 *>(A + (c0 + i) + lda * (long)(c0 + j));
-    }
-    for (int e = tid; e < PANEL_ROWS * nb; e += nt) {
-        int i = e % PANEL_ROWS, j = e / PANEL_ROWS;
-        P[e] = (i < rows) ? *reinterpret_cast<const double2 *>(A + (r0 + i) + lda * (long)(c0 + j)) : make_double2(0.0, 0.0);
-    }
-    for (int e = tid; e < nb; e += nt) R[e] = make_double2(rdiag[e].hi, rdiag[e].lo);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int j = warp; j < NB; j += PANEL_THREADS / 32)
+        for (int i = j + lane; i < NB; i += 32) L11[tri_at(i, j)] = *reinterpret_cast<const double2 *>(A + (c0 + i) + lda * (long)(c0 + j));
+    for (int e = tid; e < NB; e += PANEL_THREADS) R[e] = make_double2(rdiag[e].hi, rdiag[e].lo);
+    const int cls = lane / W, row = lane % W;
+    const long gi = (long)c0 + NB + (long)blockIdx.x * PANEL_ROWS + warp * W + row;
+    const bool live = gi < n;
+    dd_t *arow = A + gi + lda * (long)c0; // the row's panel entries, stride lda
+    dd_t x[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) x[s] = live ? ld_dd(arow + lda * (long)(cls + C * s)) : dd_from(0.0);
     __syncthreads();
     auto rk = [&](int k) { return dd_make(R[k].x, R[k].y); };
-    // column 0: scaling only
-    for (int e = tid; e < PANEL_ROWS; e += nt)
-        if (e < rows) {
-            const double2 v = P[e];
-            const dd_t x = dd_mul(rk(0), dd_make(v.x, v.y));
-            P[e] = make_double2(x.hi, x.lo);
-        }
-    __syncthreads();
-    // lane = row (PANEL_ROWS = 32), warps take the columns right of k
-    // round-robin
-    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-    for (int k = 0; k + 1 < nb; ++k) {
-        if (lane < rows) {
-            const double2 xik = P[lane + PANEL_ROWS * k];
-            const dd_t x_ik = dd_make(xik.x, xik.y);
-            for (int j = k + 1 + warp; j < nb; j += nw) {
-                const double2 ljk = L11[tri_at(j, k)], v = P[lane + PANEL_ROWS * j];
-                dd_t y = dd_sub(dd_make(v.x, v.y), dd_mul(dd_make(ljk.x, ljk.y), x_ik));
-                if (j == k + 1) y = dd_mul(rk(k + 1), y);
-                P[lane + PANEL_ROWS * j] = make_double2(y.hi, y.lo);
+    if (cls == 0) x[0] = dd_mul(rk(0), x[0]); // column 0: scaling only
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+        // step k = C q + t; slot s holds column cls + C (q + s), s < NS - q
+#pragma unroll 1
+        for (int t = 0; t < C; ++t) {
+            const int k = C * q + t;
+            if (k + 1 >= NB) break;
+            const dd_t xk = dd_make(__shfl_sync(0xffffffffu, x[0].hi, t * W + row), __shfl_sync(0xffffffffu, x[0].lo, t * W + row));
+            const double *lk = reinterpret_cast<const double *>(L11) + 2 * k;
+            dd_t y[NS];
+#pragma unroll
+            for (int s = 0; s < NS - q; ++s) {
+                const int j = cls + C * (q + s);
+                const double2 l = *reinterpret_cast<const double2 *>(lk + j * (j + 1));
+                y[s] = dd_sub(x[s], dd_mul(dd_make(l.x, l.y), xk));
+            }
+            // slot 0's column lies right of k only for classes above t
+            x[0] = cls > t ? y[0] : x[0];
+#pragma unroll
+            for (int s = 1; s < NS - q; ++s) x[s] = y[s];
+            // column k + 1 is final after its scaling: class t + 1 in slot 0,
+            // or class 0 in slot 1 at the round's last step
+            if (t + 1 < C) {
+                if (cls == t + 1) x[0] = dd_mul(rk(k + 1), x[0]);
+            } else if (q + 1 < NS) {
+                if (cls == 0) x[1] = dd_mul(rk(k + 1), x[1]);
             }
         }
-        __syncthreads();
-    }
-    for (int e = tid; e < PANEL_ROWS * nb; e += nt) {
-        int i = e % PANEL_ROWS, j = e / PANEL_ROWS;
-        if (i < rows) *reinterpret_cast<double2 *>(A + (r0 + i) + lda * (long)(c0 + j)) = P[e];
+        // column cls + C q is final
+        if (live) st_dd(arow + lda * (long)(cls + C * q), x[0]);
+#pragma unroll
+        for (int s = 0; s + 1 < NS - q; ++s) x[s] = x[s + 1];
     }
 }
 
@@ -367,7 +439,7 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
     static thread_local bool attr[64] = {};
     const int nbmax = POTRF_NB;
     const size_t smem_diag = sizeof(double2) * nbmax * nbmax;
-    const size_t smem_panel = sizeof(double2) * (nbmax * (nbmax + 1) / 2 + PANEL_ROWS * nbmax + nbmax);
+    const size_t smem_panel = PANEL_SMEM;
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (!attr[dev & 63]) {
@@ -393,8 +465,7 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
             if (below <= 0) break;
             {
                 PROF_SCOPE("potrf_panel", st);
-                potrf_panel_kernel<<<ceil_div(below, PANEL_ROWS), PANEL_THREADS, sizeof(double2) * (nb * (nb + 1) / 2 + PANEL_ROWS * nb + nb), st>>>(
-                    A, lda, n, nb, c0, info_dev, rdiag_dev);
+                potrf_panel_kernel<<<ceil_div(below, PANEL_ROWS), PANEL_THREADS, PANEL_SMEM, st>>>(A, lda, n, c0, info_dev, rdiag_dev);
                 CK_LAUNCH();
             }
             const int c1 = c0 + nb, nb1 = std::min(nbmax, n - c1);
@@ -430,8 +501,7 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
         if (below <= 0) break;
         {
             PROF_SCOPE("potrf_panel", st);
-            potrf_panel_kernel<<<ceil_div(below, PANEL_ROWS), PANEL_THREADS, sizeof(double2) * (nb * (nb + 1) / 2 + PANEL_ROWS * nb + nb), st>>>(A, lda, n, nb, c0, info_dev,
-                                                                                                                          rdiag_dev);
+            potrf_panel_kernel<<<ceil_div(below, PANEL_ROWS), PANEL_THREADS, PANEL_SMEM, st>>>(A, lda, n, c0, info_dev, rdiag_dev);
             CK_LAUNCH();
         }
         dd_t *panel = A + (c0 + nb) + lda * (long)c0;
@@ -444,6 +514,11 @@ void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag
             gemm(st, 'N', 'T', GEMM_SUB, below, below, nb, panel, lda, 0, panel, lda, 0, trail, lda, 0, 1, true);
         }
     }
+}
+
+int potrf_info_check(int info) {
+    if (info < 0) throw Error(ERR_CUDA, "potrf: a diagonal block's wait for one of its columns ran out");
+    return info;
 }
 
 void potrf_batched(cudaStream_t st, dd_t *A, long lda, int n, long sA, int batch, int *info_dev) {

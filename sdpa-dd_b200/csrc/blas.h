@@ -26,7 +26,11 @@ void gemm(cudaStream_t st, char ta, char tb, int mode, int M, int N, int K, cons
 // 'T' A c += alpha (sum_l A(l,i) B(l,j)).  op: 'N' or 'T'.
 void gemm_ab(cudaStream_t st, char ta, char tb, int M, int N, int K, dd_t alpha, const dd_t *A, long lda, const dd_t *B, long ldb, dd_t beta, dd_t *C,
              long ldc);
+// *info_dev = -1: a diagonal block's wait for one of its columns ran out
+// (the block is left as it was); potrf_info_check turns that into an error.
 void potrf(cudaStream_t st, dd_t *A, long lda, int n, int *info_dev, dd_t *rdiag_dev, OzakiWork *tc = nullptr);
+// Throws ERR_CUDA for a negative info (a wait that ran out); returns info.
+int potrf_info_check(int info);
 void zero_upper(cudaStream_t st, dd_t *A, long lda, int n, int batch = 1, long sA = 0);
 // Rpotrf("Lower") of `batch` matrices of order n <= 64, matrix b at A + b sA,
 // one CTA each (the single diagonal block of potrf); any failure sets

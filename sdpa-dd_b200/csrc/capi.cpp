@@ -659,7 +659,7 @@ int sddd_Rpotrf(sddd_ctx *ctx, char uplo, long n, sddd_dd *A, long lda) {
         CK(cudaMemcpyAsync(&info, c.info.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
         CK(cudaStreamSynchronize(c.stream));
         if (tc) sddd::ozaki_check(c.stream, *tc);
-        return info;
+        return sddd::potrf_info_check(info);
     });
 }
 

@@ -26,10 +26,22 @@ __device__ __forceinline__ dd_t sparse_dot_dense(int n, int nnz, const int *row,
 }
 
 // Rdot with one OpenMP thread: templ += x[k] y[k]; return 0 + templ
-// (mplapack/Rdot_omp.cpp).
+// (mplapack/Rdot_omp.cpp).  The loads of eight steps go out ahead of
+// their terms; the sum's order is unchanged.
 __device__ __forceinline__ dd_t seq_dot(long n, const dd_t *x, const dd_t *y) {
     dd_t t = dd_zero();
-    for (long k = 0; k < n; ++k) t = dd_acc(t, dd_mul(ld_dd(x + k), ld_dd(y + k)));
+    long k = 0;
+    for (; k + 8 <= n; k += 8) {
+        dd_t a[8], b[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            a[u] = ld_dd(x + k + u);
+            b[u] = ld_dd(y + k + u);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) t = dd_acc(t, dd_mul(a[u], b[u]));
+    }
+    for (; k < n; ++k) t = dd_acc(t, dd_mul(ld_dd(x + k), ld_dd(y + k)));
     return dd_acc(dd_zero(), t);
 }
 

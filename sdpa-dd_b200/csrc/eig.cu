@@ -247,24 +247,61 @@ __global__ void __launch_bounds__(LZ_THREADS) lanczos_kernel(const int *blk_ids,
             st_dd(q + i, qi);
         }
         __syncthreads();
+        // Each product below is a sequential chain per entry; the loads of
+        // eight steps go out ahead of their terms (same order of the sums).
         // w = L^T q (Rtrmv "Lower","Transpose")
         for (int j = tid; j < n; j += nt) {
-            dd_t t = dd_mul(ld_dd(q + j), ld_dd(L + j + (long)n * j));
-            for (int i = j + 1; i < n; ++i) t = dd_acc(t, dd_mul(ld_dd(L + i + (long)n * j), ld_dd(q + i)));
+            const dd_t *Lc = L + (long)n * j;
+            dd_t t = dd_mul(ld_dd(q + j), ld_dd(Lc + j));
+            int i = j + 1;
+            for (; i + 8 <= n; i += 8) {
+                dd_t a[8], b[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    a[u] = ld_dd(Lc + i + u);
+                    b[u] = ld_dd(q + i + u);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) t = dd_acc(t, dd_mul(a[u], b[u]));
+            }
+            for (; i < n; ++i) t = dd_acc(t, dd_mul(ld_dd(Lc + i), ld_dd(q + i)));
             st_dd(w + j, t);
         }
         __syncthreads();
         // tmp = X w (Rgemv "N", alpha 1, beta 0)
         for (int i = tid; i < n; i += nt) {
             dd_t t = dd_zero();
-            for (int j = 0; j < n; ++j) t = dd_acc(t, dd_mul(dd_mul(dd_from(1.0), ld_dd(w + j)), ld_dd(X + i + (long)n * j)));
+            int j = 0;
+            for (; j + 8 <= n; j += 8) {
+                dd_t a[8], b[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    a[u] = ld_dd(w + j + u);
+                    b[u] = ld_dd(X + i + (long)n * (j + u));
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) t = dd_acc(t, dd_mul(dd_mul(dd_from(1.0), a[u]), b[u]));
+            }
+            for (; j < n; ++j) t = dd_acc(t, dd_mul(dd_mul(dd_from(1.0), ld_dd(w + j)), ld_dd(X + i + (long)n * j)));
             st_dd(tmp + i, t);
         }
         __syncthreads();
         // w = L tmp (Rtrmv "Lower","NoTranspose": row i, j descending)
         for (int i = tid; i < n; i += nt) {
             dd_t t = dd_mul(ld_dd(tmp + i), ld_dd(L + i + (long)n * i));
-            for (int j = i - 1; j >= 0; --j) {
+            int j = i - 1;
+            for (; j >= 7; j -= 8) {
+                dd_t a[8], b[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    a[u] = ld_dd(tmp + j - u);
+                    b[u] = ld_dd(L + i + (long)n * (j - u));
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (!dd_is_zero(a[u])) t = dd_acc(t, dd_mul(a[u], b[u]));
+            }
+            for (; j >= 0; --j) {
                 dd_t xj = ld_dd(tmp + j);
                 if (!dd_is_zero(xj)) t = dd_acc(t, dd_mul(xj, ld_dd(L + i + (long)n * j)));
             }

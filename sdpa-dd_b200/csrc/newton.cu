@@ -173,6 +173,8 @@ int ScalarBatch::inverse_info() {
 bool ScalarBatch::inverse_ok(int g) const {
     int info[2];
     std::memcpy(info, &host[groups[g].first], sizeof(info));
+    potrf_info_check(info[0]);
+    potrf_info_check(info[1]);
     return info[0] == 0 && info[1] == 0;
 }
 
@@ -221,6 +223,7 @@ int schur_factor(Context &c) {
     potrf(c.stream, c.B.p, c.m, c.m, c.info.p, c.rdiag.p, tc);
     int info = 0;
     d2h(c, &info, c.info.p, sizeof(int));
+    potrf_info_check(info);
     if (tc) {
         ozaki_check(c.stream, *tc);
         if (info == 0) {

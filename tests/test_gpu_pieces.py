@@ -135,7 +135,7 @@ def test_dd_blas_argument_checks(ctx):
     assert b"parameter 5" in ctx.L.sddd_last_error(ctx.h)
 
 
-@pytest.mark.parametrize("n", [1, 5, 63, 64, 65, 130, 257])
+@pytest.mark.parametrize("n", [1, 5, 33, 63, 64, 65, 130, 257, 700])
 def test_device_potrf_trsv_match(ctx, oracle_lib, n):
     rng = np.random.default_rng(500 + n)
     A = spd(rng, n)
@@ -183,16 +183,20 @@ def test_device_trsv_wavefront_matches_rtrsv(ctx, oracle_lib, n, lda):
         assert same(from_dev(dx, n), x), tr
 
 
-def test_device_potrf_reports_failing_column(ctx, oracle_lib):
+@pytest.mark.parametrize("col", [0, 31, 32, 63, 97, 127, 149])
+def test_device_potrf_reports_failing_column(ctx, oracle_lib, col):
+    """A negative pivot at the first and last column of a diagonal block,
+    either side of the block's 32-column halves, and the matrix's last
+    column: the 1-based column comes back, as Rpotrf's info does."""
     rng = np.random.default_rng(9)
     n = 150
     A = spd(rng, n)
-    A["hi"][97 * n + 97] = -3.0
+    A["hi"][col * n + col] = -3.0
     want = A.copy()
     i1 = oracle_lib.o_potrf(ctypes.c_long(n), ptr(want), ctypes.c_long(n))
     dA = to_dev(A)
     i2 = ctx.L.sddd_Rpotrf(ctx.h, b"L", n, ctypes.c_void_p(dA.data_ptr()), n)
-    assert i1 == i2 == 98
+    assert i1 == i2 == col + 1
 
 
 def _dd_scalar_eq(a, b):
