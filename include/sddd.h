@@ -344,7 +344,9 @@ int sddd_sparse_solveSystems(sddd_ctx *ctx, int m, const int *diagonalIndex, con
 /* -- dd kernels on device memory: the MPLAPACK seam --
  * The argument lists of MPLAPACK's dd routines (mplapack/mpblas_dd.h:47,54,
  * mplapack/mplapack_dd.h:41) with the context first; pointers are device
- * pointers to column-major sddd_dd.  Bad arguments return SDDD_ERR_ARG
+ * pointers to column-major sddd_dd, 16-byte aligned (a cudaMalloc'd base
+ * plus whole sddd_dd; an unaligned base returns SDDD_ERR_ARG naming the
+ * argument).  Bad arguments return SDDD_ERR_ARG
  * naming the routine and the 1-based position the reference's Mxerbla_dd
  * would report (in its order of checks); valid forms SDPA never calls
  * return SDDD_ERR_UNSUPPORTED.  Results are the reference's bit for bit

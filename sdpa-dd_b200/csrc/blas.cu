@@ -209,13 +209,14 @@ void gemm(cudaStream_t st, char ta, char tb, int mode, int M, int N, int K, cons
 // order as the column-by-column form: x(i,j) -= L(j,k) L(i,k) for k
 // ascending, then the sqrt (diagonal) or the scaling by 1/L(j,j).
 constexpr int DIAG_THREADS = 1024;
-constexpr unsigned long long DIAG_WAIT_NS = 2000000000ull; // one column's wait, at most
+constexpr unsigned long long POTRF_WAIT_NS = 2000000000ull; // one mbarrier wait, at most
 static_assert(POTRF_NB <= 64 && DIAG_THREADS == 1024, "two columns a warp, two rows a lane");
-__device__ __forceinline__ bool diag_wait(uint64_t *b) {
+// Bounded wait for phase 0 of an mbarrier.
+__device__ __forceinline__ bool bar_wait0(uint64_t *b) {
     if (mbar_try_wait(b, 0)) return true;
     const unsigned long long t0 = globaltimer_ns();
     while (!mbar_try_wait(b, 0))
-        if (globaltimer_ns() - t0 > DIAG_WAIT_NS) return false;
+        if (globaltimer_ns() - t0 > POTRF_WAIT_NS) return false;
     return true;
 }
 __global__ void __launch_bounds__(DIAG_THREADS) potrf_diag_kernel(dd_t *A, long lda, int nb, int c0, int *info, dd_t *rdiag, long sA) {
@@ -294,7 +295,7 @@ __global__ void __launch_bounds__(DIAG_THREADS) potrf_diag_kernel(dd_t *A, long 
     if (warp == 0 && nb > 0) ok = finish(0);
     for (int k = 0; ok && k < last; ++k) {
         // warp-uniform outcomes: the lanes go on together or stop together
-        if (!__all_sync(0xffffffffu, diag_wait(&bar[k]))) {
+        if (!__all_sync(0xffffffffu, bar_wait0(&bar[k]))) {
             if (lane == 0) {
                 *vfail = 2;
                 atomicCAS(info, 0, -1);
@@ -341,8 +342,8 @@ __global__ void __launch_bounds__(DIAG_THREADS) potrf_diag_kernel(dd_t *A, long 
 // column leaving slot 0 is final and goes back to memory); the rounds are
 // unrolled so that each one updates exactly its live slots, without
 // branches between the slots' independent chains.  L11 (lower triangle,
-// packed by rows) and the reciprocals are shared by the CTA's warps.  The
-// panel is POTRF_NB columns wide.
+// packed by columns, one bulk copy per column) and the reciprocals are
+// shared by the CTA's warps.  The panel is POTRF_NB columns wide.
 constexpr int PANEL_CLASSES = 16;                           // lanes a row
 constexpr int PANEL_WROWS = 32 / PANEL_CLASSES;             // rows a warp
 constexpr int PANEL_SLOTS = POTRF_NB / PANEL_CLASSES;       // columns a lane
@@ -350,17 +351,31 @@ constexpr int PANEL_THREADS = 128;
 constexpr int PANEL_ROWS = PANEL_WROWS * (PANEL_THREADS / 32); // rows a CTA
 static_assert(POTRF_NB % PANEL_CLASSES == 0 && 32 % PANEL_CLASSES == 0, "panel lane map");
 constexpr size_t PANEL_SMEM = sizeof(double2) * (POTRF_NB * (POTRF_NB + 1) / 2 + POTRF_NB);
-// entry (j, k), k <= j, of a lower triangle packed by rows
-__device__ __forceinline__ int tri_at(int j, int k) { return j * (j + 1) / 2 + k; }
-__global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, long lda, int n, int c0, const int *info, const dd_t *rdiag) {
+// first entry of column k (rows k .. POTRF_NB-1) of a lower triangle packed
+// by columns
+__device__ __forceinline__ int col_off(int k) { return k * POTRF_NB - k * (k - 1) / 2; }
+__global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, long lda, int n, int c0, int *info, const dd_t *rdiag) {
     constexpr int NB = POTRF_NB, C = PANEL_CLASSES, W = PANEL_WROWS, NS = PANEL_SLOTS;
-    extern __shared__ double2 sm[];
-    double2 *L11 = sm;                   // lower triangle of NB x NB, packed
+    extern __shared__ __align__(16) double2 sm[];
+    double2 *L11 = sm;                   // lower triangle of NB x NB, packed by columns
     double2 *R = sm + NB * (NB + 1) / 2; // NB reciprocals
+    __shared__ uint64_t lbar;
+    __shared__ int lfail;
     if (*info != 0) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int j = warp; j < NB; j += PANEL_THREADS / 32)
-        for (int i = j + lane; i < NB; i += 32) L11[tri_at(i, j)] = *reinterpret_cast<const double2 *>(A + (c0 + i) + lda * (long)(c0 + j));
+    if (tid == 0) {
+        mbar_init(&lbar, 1);
+        mbar_init_fence();
+        lfail = 0;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        // column k of L11 (rows k .. NB-1) is contiguous in A: one bulk copy
+        if (lane == 0) mbar_expect_tx(&lbar, (uint32_t)(sizeof(double2) * NB * (NB + 1) / 2));
+        __syncwarp();
+        for (int k = lane; k < NB; k += 32)
+            bulk_g2s(L11 + col_off(k), A + (c0 + k) + lda * (long)(c0 + k), (uint32_t)(sizeof(double2) * (NB - k)), &lbar);
+    }
     for (int e = tid; e < NB; e += PANEL_THREADS) R[e] = make_double2(rdiag[e].hi, rdiag[e].lo);
     const int cls = lane / W, row = lane % W;
     const long gi = (long)c0 + NB + (long)blockIdx.x * PANEL_ROWS + warp * W + row;
@@ -369,7 +384,14 @@ __global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, lon
     dd_t x[NS];
 #pragma unroll
     for (int s = 0; s < NS; ++s) x[s] = live ? ld_dd(arow + lda * (long)(cls + C * s)) : dd_from(0.0);
+    if (tid == 0 && !bar_wait0(&lbar)) {
+        // the copies did not land in time: report, let them land (bounded)
+        lfail = 1;
+        atomicCAS(info, 0, -1);
+        bar_wait0(&lbar);
+    }
     __syncthreads();
+    if (lfail) return;
     auto rk = [&](int k) { return dd_make(R[k].x, R[k].y); };
     if (cls == 0) x[0] = dd_mul(rk(0), x[0]); // column 0: scaling only
 #pragma unroll
@@ -380,12 +402,12 @@ __global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, lon
             const int k = C * q + t;
             if (k + 1 >= NB) break;
             const dd_t xk = dd_make(__shfl_sync(0xffffffffu, x[0].hi, t * W + row), __shfl_sync(0xffffffffu, x[0].lo, t * W + row));
-            const double *lk = reinterpret_cast<const double *>(L11) + 2 * k;
+            const double2 *lk = L11 + col_off(k) - k; // L(j, k) at lk[j]
             dd_t y[NS];
 #pragma unroll
             for (int s = 0; s < NS - q; ++s) {
                 const int j = cls + C * (q + s);
-                const double2 l = *reinterpret_cast<const double2 *>(lk + j * (j + 1));
+                const double2 l = lk[j];
                 y[s] = dd_sub(x[s], dd_mul(dd_make(l.x, l.y), xk));
             }
             // slot 0's column lies right of k only for classes above t

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdint>
 #include <cstring>
 #include <ctime>
 #include <memory>
@@ -615,6 +616,11 @@ inline dd_t from(sddd_dd v) { return dd_t{v.hi, v.lo}; }
 [[noreturn]] void bad_arg(const char *routine, int pos, const char *what) {
     throw sddd::Error(SDDD_ERR_ARG, std::string(routine) + ": parameter " + std::to_string(pos) + " (" + what + ") is invalid");
 }
+// Device matrices are read and written as 16-byte dd pairs (and staged
+// with bulk copies), so their base must be 16-byte aligned.
+void need_aligned(const char *routine, int pos, const char *what, const void *p) {
+    if (p && (reinterpret_cast<uintptr_t>(p) & 15u) != 0) bad_arg(routine, pos, (std::string(what) + ", not 16-byte aligned").c_str());
+}
 } // namespace
 
 int sddd_Rgemm(sddd_ctx *ctx, char transa, char transb, long m, long n, long k, sddd_dd alpha, const sddd_dd *A, long lda, const sddd_dd *B, long ldb,
@@ -633,6 +639,9 @@ int sddd_Rgemm(sddd_ctx *ctx, char transa, char transb, long m, long n, long k, 
         if (lda < std::max(1L, nrowa)) bad_arg("Rgemm", 8, "lda");
         if (ldb < std::max(1L, nrowb)) bad_arg("Rgemm", 10, "ldb");
         if (ldc < std::max(1L, m)) bad_arg("Rgemm", 13, "ldc");
+        need_aligned("Rgemm", 7, "A", A);
+        need_aligned("Rgemm", 9, "B", B);
+        need_aligned("Rgemm", 12, "C", C);
         sddd::gemm_ab(ctx->c->stream, nota ? 'N' : 'T', notb ? 'N' : 'T', (int)m, (int)n, (int)k, from(alpha), reinterpret_cast<const dd_t *>(A), lda,
                       reinterpret_cast<const dd_t *>(B), ldb, from(beta), reinterpret_cast<dd_t *>(C), ldc);
         CK(cudaStreamSynchronize(ctx->c->stream));
@@ -647,6 +656,7 @@ int sddd_Rpotrf(sddd_ctx *ctx, char uplo, long n, sddd_dd *A, long lda) {
         if (u != 'L' && u != 'U') bad_arg("Rpotrf", 1, "uplo");
         if (n < 0) bad_arg("Rpotrf", 2, "n");
         if (lda < std::max(1L, n)) bad_arg("Rpotrf", 4, "lda");
+        need_aligned("Rpotrf", 3, "A", A);
         if (u == 'U') throw sddd::Error(SDDD_ERR_UNSUPPORTED, "Rpotrf: only uplo = 'L' (the form SDPA calls) is implemented");
         if (n == 0) return SDDD_OK;
         sddd::Context &c = *ctx->c;
@@ -696,6 +706,8 @@ int sddd_Rsyrk_tc(sddd_ctx *ctx, long n, long k, const sddd_dd *P, long ldp, sdd
         if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
         if (n < 0 || k < 0 || k > sddd::OZ_K || ldp < std::max(1L, n) || ldc < std::max(1L, n) || slices < 8 || slices > sddd::OZ_MAX_SLICES)
             throw sddd::Error(SDDD_ERR_ARG, "sddd_Rsyrk_tc: need 0 <= k <= 64, ld >= n and 8 <= slices <= 16");
+        need_aligned("sddd_Rsyrk_tc", 3, "P", P);
+        need_aligned("sddd_Rsyrk_tc", 5, "C", C);
         if (n == 0 || k == 0) return SDDD_OK;
         sddd::Context &c = *ctx->c;
         sddd::OzakiWork &w = sddd::tc_work(c, (int)n, slices);
@@ -711,6 +723,9 @@ int sddd_Rdot_pairs_tc(sddd_ctx *ctx, long n, long k, const sddd_dd *W, long ldw
         if (!ctx || !ctx->c) throw sddd::Error(SDDD_ERR_ARG, "null context");
         if (n < 0 || k < 1 || k > sddd::OG_MAX_K || ldw < k || ldv < k || ldc < std::max(1L, n) || slices < 8 || slices > sddd::OZ_MAX_SLICES)
             throw sddd::Error(SDDD_ERR_ARG, "sddd_Rdot_pairs_tc: need 1 <= k <= 32767, ldw, ldv >= k, ldc >= n and 8 <= slices <= 16");
+        need_aligned("sddd_Rdot_pairs_tc", 3, "W", W);
+        need_aligned("sddd_Rdot_pairs_tc", 5, "V", V);
+        need_aligned("sddd_Rdot_pairs_tc", 7, "C", C);
         if (n == 0) return SDDD_OK;
         sddd::Context &c = *ctx->c;
         sddd::OzakiGemmWork &w = sddd::tcg_work(c, (int)n, k, slices);
@@ -732,6 +747,8 @@ int sddd_Rtrsv(sddd_ctx *ctx, char uplo, char trans, char diag, long n, const sd
         if (n < 0) bad_arg("Rtrsv", 4, "n");
         if (lda < std::max(1L, n)) bad_arg("Rtrsv", 6, "lda");
         if (incx == 0) bad_arg("Rtrsv", 8, "incx");
+        need_aligned("Rtrsv", 5, "A", A);
+        need_aligned("Rtrsv", 7, "x", x);
         if (u != 'L' || d != 'N' || incx != 1)
             throw sddd::Error(SDDD_ERR_UNSUPPORTED, "Rtrsv: only uplo = 'L', diag = 'N', incx = 1 (the form SDPA calls) is implemented");
         if (n == 0) return SDDD_OK;
@@ -751,6 +768,8 @@ int sddd_Rpotrs(sddd_ctx *ctx, char uplo, long n, long nrhs, const sddd_dd *A, l
         if (nrhs < 0) bad_arg("Rpotrs", 3, "nrhs");
         if (lda < std::max(1L, n)) bad_arg("Rpotrs", 5, "lda");
         if (ldb < std::max(1L, n)) bad_arg("Rpotrs", 7, "ldb");
+        need_aligned("Rpotrs", 4, "A", A);
+        need_aligned("Rpotrs", 6, "B", B);
         if (u == 'U') throw sddd::Error(SDDD_ERR_UNSUPPORTED, "Rpotrs: only uplo = 'L' is implemented");
         if (n == 0 || nrhs == 0) return SDDD_OK;
         sddd::Context &c = *ctx->c;

@@ -133,6 +133,17 @@ def test_dd_blas_argument_checks(ctx):
     assert ctx.L.sddd_Rpotrf(ctx.h, b"U", 3, None, 3) == -7
     assert ctx.L.sddd_Rpotrs(ctx.h, b"L", 3, 1, None, 2, None, 3) == -1
     assert b"parameter 5" in ctx.L.sddd_last_error(ctx.h)
+    # a device base off the 16-byte dd alignment is refused on the host,
+    # before anything reads it
+    buf = to_dev(np.zeros(32, DD))
+    odd = ctypes.c_void_p(buf.data_ptr() + 8)
+    assert ctx.L.sddd_Rpotrf(ctx.h, b"L", 3, odd, 3) == -1
+    assert b"parameter 3" in ctx.L.sddd_last_error(ctx.h) and b"16-byte" in ctx.L.sddd_last_error(ctx.h)
+    ok = ctypes.c_void_p(buf.data_ptr())
+    assert ctx.L.sddd_Rgemm(ctx.h, b"N", b"N", 2, 2, 2, one, ok, 2, odd, 2, one, ok, 2) == -1
+    assert b"parameter 9" in ctx.L.sddd_last_error(ctx.h)
+    assert ctx.L.sddd_Rtrsv(ctx.h, b"L", b"N", b"N", 3, ok, 3, odd, 1) == -1
+    assert b"parameter 7" in ctx.L.sddd_last_error(ctx.h)
 
 
 @pytest.mark.parametrize("n", [1, 5, 33, 63, 64, 65, 130, 257, 700])
