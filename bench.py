@@ -670,7 +670,8 @@ def run_ours(args, world, rank, local):
 def profile_case(args):
     """One dd Cholesky of an m x m SPD matrix through sddd_Rpotrf (the
     kernels of the bench's dominant phase, at a size an ncu capture can
-    replay); prints its time."""
+    replay), then one solve with the factor (sddd_Rpotrs: the triangular
+    solves); prints their times."""
     sddd = load_pkg()
     L = sddd.lib()
     import torch
@@ -688,8 +689,15 @@ def profile_case(args):
         t = time.perf_counter()
         info = L.sddd_Rpotrf(ctx.h, b"L", m, ctypes.c_void_p(dd.data_ptr()), m)
         torch.cuda.synchronize()
-        print(json.dumps({"case": "potrf", "m": m, "info": info, "s": time.perf_counter() - t}))
-    return 0 if info == 0 else 1
+        t1 = time.perf_counter()
+        rc = -1
+        if info == 0:
+            b = torch.zeros(m, 2, dtype=torch.float64, device="cuda")
+            b[:, 0] = 1.0
+            rc = L.sddd_Rpotrs(ctx.h, b"L", m, 1, ctypes.c_void_p(dd.data_ptr()), m, ctypes.c_void_p(b.data_ptr()), m)
+            torch.cuda.synchronize()
+        print(json.dumps({"case": "potrf", "m": m, "info": info, "s": t1 - t, "potrs_rc": rc, "potrs_s": time.perf_counter() - t1}))
+    return 0 if info == 0 and rc == 0 else 1
 
 
 def profile_case_sparse(args):

@@ -99,13 +99,14 @@ OzakiWork &tc_work(Context &c, int n, int slices) {
     const int rows = (int)(ceil_div(n, OZ_ROWS_A) * OZ_ROWS_A);
     if (rows > c.tc.row_cap || !c.tc.slices) {
         CK(cudaStreamSynchronize(c.stream));
-        c.tc_slice_buf.alloc((size_t)OZ_MAX_SLICES * rows * OZ_K);
+        c.tc_slice_buf.alloc((size_t)2 * OZ_MAX_SLICES * rows * OZ_K);
         c.tc_exps.alloc((size_t)rows);
         if (!c.tc_err.p) {
             c.tc_err.alloc(1);
             CK(cudaMemsetAsync(c.tc_err.p, 0, sizeof(int), c.stream));
         }
         c.tc.slices = c.tc_slice_buf.p;
+        c.tc.slices_b = c.tc_slice_buf.p + (size_t)OZ_MAX_SLICES * rows * OZ_K;
         c.tc.exps = c.tc_exps.p;
         c.tc.err = c.tc_err.p;
         c.tc.h_err = static_cast<int *>(c.h_pin);

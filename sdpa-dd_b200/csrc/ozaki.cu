@@ -108,7 +108,8 @@ __device__ __forceinline__ uint64_t oz_desc(uint32_t saddr) {
 }
 
 struct OzArgs {
-    const int8_t *slices;
+    const int8_t *slices;   // slice by slice (A operands: a row block of one slice is contiguous)
+    const int8_t *slices_b; // by 16-row block (B operands: a tile's slices are contiguous)
     long slice_stride; // bytes between slices
     const int *exps;
     dd_t *C;
@@ -201,11 +202,10 @@ __device__ void oz_producer(const OzArgs &a, OzShared &S, uint8_t *smA, uint8_t 
     volatile int *abort_flag = &S.abort_flag;
     const int ns = a.ns;
     const long ntile = t_end - t_begin;
+    // one bulk copy per tile: the block's ns slices lie back to back
     auto load_B = [&](int jb, int st) {
         mbar_expect_tx(&S.barB[st], (uint32_t)(ns * OZ_B_BYTES));
-        for (int s = 0; s < ns; ++s)
-            bulk_g2s(smB + (size_t)st * OZ_TILE_B + (size_t)s * OZ_B_BYTES, a.slices + s * a.slice_stride + (long)jb * OZ_B_BYTES, OZ_B_BYTES,
-                     &S.barB[st]);
+        bulk_g2s(smB + (size_t)st * OZ_TILE_B, a.slices_b + (long)jb * ns * OZ_B_BYTES, (uint32_t)(ns * OZ_B_BYTES), &S.barB[st]);
     };
     const uint64_t descA = oz_desc(smem_u32(smA));
     const uint64_t descB0 = oz_desc(smem_u32(smB));
@@ -351,6 +351,10 @@ __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_e
         const int ei = a.exps[i]; // scale exponent of the row (padded rows hold 0)
         const int4 e4 = *reinterpret_cast<const int4 *>(a.exps + jb);
         const int ej[4] = {e4.x, e4.y, e4.z, e4.w};
+        // Drain first: every entry's dd from tensor memory, then the
+        // buffer goes back to the MMA warp; only then the entries meet C,
+        // so the accumulators are never held while C is in flight.
+        double phi[OZ_EPI_COLS], plo[OZ_EPI_COLS];
 #pragma unroll
         for (int ch = 0; ch < OZ_EPI_COLS / 2; ++ch) {
             int32_t v[OZ_MAX_SLICES][2];
@@ -370,22 +374,21 @@ __device__ void oz_epilogue(const OzArgs &a, OzShared &S, long t_begin, long t_e
                 if (lane == 0) mbar_arrive(&S.tempty[b]);
             }
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                const int cc = 2 * ch + c;
-                double phi, plo;
-                oz_entry_dd(v, c, phi, plo);
-                if (cc < ncol) {
-                    const int sc = ei + ej[cc] - 35;
-                    dd_t p;
-                    if (sc >= -1022 && sc <= 1023) {
-                        const double pw = oz_pow2(sc);
-                        p = dd_make(phi * pw, plo * pw);
-                    } else {
-                        p = dd_make(ldexp(phi, sc), ldexp(plo, sc));
-                    }
-                    const dd_t res = dd_sub(dd_make(cv[cc].x, cv[cc].y), p);
-                    __stcs(reinterpret_cast<double2 *>(cp + a.ldc * (long)cc), make_double2(res.hi, res.lo));
+            for (int c = 0; c < 2; ++c) oz_entry_dd(v, c, phi[2 * ch + c], plo[2 * ch + c]);
+        }
+#pragma unroll
+        for (int cc = 0; cc < OZ_EPI_COLS; ++cc) {
+            if (cc < ncol) {
+                const int sc = ei + ej[cc] - 35;
+                dd_t p;
+                if (sc >= -1022 && sc <= 1023) {
+                    const double pw = oz_pow2(sc);
+                    p = dd_make(phi[cc] * pw, plo[cc] * pw);
+                } else {
+                    p = dd_make(ldexp(phi[cc], sc), ldexp(plo[cc], sc));
                 }
+                const dd_t res = dd_sub(dd_make(cv[cc].x, cv[cc].y), p);
+                __stcs(reinterpret_cast<double2 *>(cp + a.ldc * (long)cc), make_double2(res.hi, res.lo));
             }
         }
         oz_tile_next(a.nJ, I, J);
@@ -441,8 +444,11 @@ __global__ void __maxnreg__(OZ_MAX_REGS) ozaki_syrk_kernel(OzArgs a) {
     }
 }
 
-// Digits of 32 rows per CTA; warp c takes K bytes 16c..16c+15.
-__global__ void __launch_bounds__(128) ozaki_split_kernel(const dd_t *P, long ldp, int n, int k, int ns, int8_t *slices, long slice_stride, int *exps) {
+// Digits of 32 rows per CTA; warp c takes K bytes 16c..16c+15.  Each
+// 16-byte group goes to both layouts: slice by slice (slices) and by
+// 16-row block, the block's ns slices back to back (slices_b).
+__global__ void __launch_bounds__(128) ozaki_split_kernel(const dd_t *P, long ldp, int n, int k, int ns, int8_t *slices, int8_t *slices_b, long slice_stride,
+                                                          int *exps) {
     __shared__ double rmax[4][32];
     const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
     const int r = blockIdx.x * 32 + lane;
@@ -466,7 +472,9 @@ __global__ void __launch_bounds__(128) ozaki_split_kernel(const dd_t *P, long ld
     if (c == 0) exps[r] = e;
 #pragma unroll
     for (int q = 0; q < 16; ++q) x[q] = dd_make(ldexp(x[q].hi, 7 - e), ldexp(x[q].lo, 7 - e));
-    int8_t *dst = slices + (long)(r >> 3) * 512 + c * 128 + (r & 7) * 16;
+    const int within = ((r >> 3) & 1) * 512 + c * 128 + (r & 7) * 16; // offset inside a 16-row block of one slice
+    int8_t *dst = slices + (long)(r >> 4) * 1024 + within;
+    int8_t *dstb = slices_b + (long)(r >> 4) * ns * 1024 + within;
     for (int s = 0; s < ns; ++s) {
         uint32_t w[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
@@ -476,7 +484,9 @@ __global__ void __launch_bounds__(128) ozaki_split_kernel(const dd_t *P, long ld
             double err, sum = ddm::two_sum(x[q].hi - d, x[q].lo, err);
             x[q] = dd_make(sum * 128.0, err * 128.0);
         }
-        *reinterpret_cast<uint4 *>(dst + (long)s * slice_stride) = make_uint4(w[0], w[1], w[2], w[3]);
+        const uint4 v = make_uint4(w[0], w[1], w[2], w[3]);
+        *reinterpret_cast<uint4 *>(dst + (long)s * slice_stride) = v;
+        *reinterpret_cast<uint4 *>(dstb + (long)s * 1024) = v;
     }
 }
 
@@ -487,12 +497,13 @@ void ozaki_syrk_sub_lower(cudaStream_t st, const dd_t *P, long ldp, int n, int k
     if (k > OZ_K) throw Error(ERR_ARG, "ozaki: panel wider than 64 columns");
     if (w.slices_used < 8 || w.slices_used > OZ_MAX_SLICES) throw Error(ERR_ARG, "ozaki: slice count must be 8..16");
     const int rows = (int)(ceil_div(n, OZ_ROWS_A) * OZ_ROWS_A);
-    if (rows > w.row_cap || !w.slices || !w.exps || !w.err) throw Error(ERR_ARG, "ozaki: workspace smaller than the panel");
+    if (rows > w.row_cap || !w.slices || !w.slices_b || !w.exps || !w.err) throw Error(ERR_ARG, "ozaki: workspace smaller than the panel");
     const long stride = (long)w.row_cap * OZ_K;
-    ozaki_split_kernel<<<rows / 32, 128, 0, st>>>(P, ldp, n, k, w.slices_used, w.slices, stride, w.exps);
+    ozaki_split_kernel<<<rows / 32, 128, 0, st>>>(P, ldp, n, k, w.slices_used, w.slices, w.slices_b, stride, w.exps);
     CK_LAUNCH();
     OzArgs a;
     a.slices = w.slices;
+    a.slices_b = w.slices_b;
     a.slice_stride = stride;
     a.exps = w.exps;
     a.C = C;

@@ -15,7 +15,8 @@ constexpr int OZ_COLS_B = 16;   // output tile columns (per B slice)
 // Device workspace of the split: slices for `row_cap` rows (a multiple of
 // 128), row exponents and an error word.
 struct OzakiWork {
-    int8_t *slices = nullptr; // OZ_MAX_SLICES x row_cap x 64 bytes, tiled
+    int8_t *slices = nullptr; // OZ_MAX_SLICES x row_cap x 64 bytes, tiled, slice by slice
+    int8_t *slices_b = nullptr; // the same digits by 16-row block: each block's slices contiguous
     int *exps = nullptr;      // row_cap
     int *err = nullptr;       // 0, or the code of a wait that gave up
     int *h_err = nullptr;     // pinned host word for reading err (or null)
