@@ -428,6 +428,8 @@ void upload_problem(Context &c, Problem &&p) {
         }
         ptr[k + 1] = (int)bl.size();
     }
+    c.inner_dense1 = c.nSDP == 1 && c.m > 0 && (int)bl.size() == c.m && c.blocks[0]->all_dense &&
+                     (size_t)c.sizes[0] * c.sizes[0] * sizeof(dd_t) <= INNER_DENSE1_SMEM;
     c.cb_ptr.upload(ptr, c.stream);
     c.cb_block.upload(bl, c.stream);
     c.cb_t.upload(tt, c.stream);

@@ -49,6 +49,10 @@ struct DBuf {
 };
 
 // Kernel-side view of one block's problem data (pointers into BlockDev).
+// Largest single block (bytes of n x n dd) whose constraint inner products
+// take the shared-memory form (constraint_inner).
+constexpr size_t INNER_DENSE1_SMEM = 160 * 1024;
+
 struct BlockView {
     int n, nc, nsparse, all_dense;
     const int *con, *formula, *perm, *coo_off, *nnz;
@@ -187,6 +191,9 @@ struct Context {
     DBuf<int> d_sizes;     // [l] block sizes
     // per constraint: (block, t) pairs ascending by block
     DBuf<int> cb_ptr, cb_block, cb_t;
+    // every constraint is one dense matrix of the single SDP block, whose
+    // order fits the shared-memory form of the constraint inner products
+    bool inner_dense1 = false;
     DBuf<dd_t> b;
     // iterate and derived (Solutions)
     Space X, Z, invCholX, invCholZ, invZ;

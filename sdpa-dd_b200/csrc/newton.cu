@@ -39,7 +39,67 @@ __global__ void constraint_inner_kernel(int m, const BlockView *views, const lon
     st_dd(out + i, dd_acc(dd_mul(MONE, ret), dd_mul(ONE, ld_dd(addv + i))));
 }
 
+// The same for one SDP block whose constraints are all dense: the block of
+// M is staged in shared memory once per CTA (every thread reads the same
+// entry at the same step), and each thread streams its constraint's n^2
+// entries with the next 16 in flight while it sums the current 16, in
+// Rdot's order.
+constexpr int INNER_CHUNK = 16;
+constexpr int INNER_DENSE1_THREADS = 128;
+__global__ void __launch_bounds__(INNER_DENSE1_THREADS) constraint_inner_dense1_kernel(int m, const BlockView *views, const int *cb_ptr,
+                                                                                     const int *cb_t, const dd_t *M, const dd_t *addv, dd_t *out) {
+    extern __shared__ double2 ms[];
+    const int n = views[0].n;
+    const long nn = (long)n * n;
+    for (long e = threadIdx.x; e < nn; e += blockDim.x) ms[e] = *reinterpret_cast<const double2 *>(M + e);
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const dd_t *A = views[0].dense + views[0].dense_off[cb_t[cb_ptr[i]]];
+    dd_t t = dd_zero();
+    dd_t a[INNER_CHUNK], b[INNER_CHUNK];
+    const long full = nn / INNER_CHUNK * INNER_CHUNK;
+    if (full > 0) {
+#pragma unroll
+        for (int u = 0; u < INNER_CHUNK; ++u) a[u] = ld_dd(A + u);
+    }
+    for (long k = 0; k < full; k += INNER_CHUNK) {
+#pragma unroll
+        for (int u = 0; u < INNER_CHUNK; ++u) b[u] = a[u];
+        if (k + INNER_CHUNK < full) {
+#pragma unroll
+            for (int u = 0; u < INNER_CHUNK; ++u) a[u] = ld_dd(A + k + INNER_CHUNK + u);
+        }
+#pragma unroll
+        for (int u = 0; u < INNER_CHUNK; ++u) {
+            const double2 y = ms[k + u];
+            t = dd_acc(t, dd_mul(b[u], dd_make(y.x, y.y)));
+        }
+    }
+    for (long k = full; k < nn; ++k) {
+        const double2 y = ms[k];
+        t = dd_acc(t, dd_mul(ld_dd(A + k), dd_make(y.x, y.y)));
+    }
+    // seq_dot's "0 + templ", then the caller's ret += tmp from zero
+    const dd_t ret = dd_acc(dd_zero(), dd_acc(dd_zero(), t));
+    st_dd(out + i, dd_acc(dd_mul(MONE, ret), dd_mul(ONE, ld_dd(addv + i))));
+}
+
 void constraint_inner(Context &c, const Space &M, const dd_t *addv, dd_t *out) {
+    if (c.inner_dense1) {
+        const size_t smem = sizeof(dd_t) * (size_t)c.sizes[0] * c.sizes[0];
+        static thread_local bool attr[64] = {};
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        if (!attr[dev & 63]) {
+            CK(cudaFuncSetAttribute(constraint_inner_dense1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INNER_DENSE1_SMEM));
+            attr[dev & 63] = true;
+        }
+        constraint_inner_dense1_kernel<<<ceil_div(c.m, INNER_DENSE1_THREADS), INNER_DENSE1_THREADS, smem, c.stream>>>(
+            c.m, c.views.p, c.cb_ptr.p, c.cb_t.p, M.buf.p + c.off[0], addv, out);
+        CK_LAUNCH();
+        return;
+    }
     constraint_inner_kernel<<<ceil_div(c.m, 64), 64, 0, c.stream>>>(c.m, c.views.p, c.d_off.p, c.cb_ptr.p, c.cb_block.p, c.cb_t.p, M.buf.p, addv, out);
     CK_LAUNCH();
 }
