@@ -52,13 +52,39 @@ __device__ int sturm_count_d(int k, const dd_t *d, const dd_t *e2, double x) {
 }
 
 // Smallest eigenvalue of the k x k tridiagonal (d, e) by multisection over
-// the 32 lanes of one warp; every lane returns the same value.  A first
-// multisection in double on the high parts narrows the Gershgorin bracket
-// to ~2^-40 of the spectrum's scale; that bracket is kept only when dd
-// Sturm counts confirm it (no eigenvalue below its lower end, one below
-// its upper end), and the dd multisection then runs from it.
-__device__ dd_t tri_min_eigenvalue(int k, const dd_t *d, const dd_t *e, dd_t *e2) {
-    const int lane = threadIdx.x & 31;
+// the lanes of nw warps (warps 0 .. nw-1 of the CTA, all of their threads
+// calling; nw = 1 runs on one warp alone); every thread returns the same
+// value.  A first multisection in double on the high parts narrows the
+// Gershgorin bracket to ~2^-40 of the spectrum's scale; that bracket is
+// kept only when dd Sturm counts confirm it (no eigenvalue below its lower
+// end, one below its upper end), and the dd multisection then runs from it.
+// P = 32 nw points a round; each warp's ballot goes to shared memory (ball:
+// 2 nw + 2 words, two alternating halves), so that every thread finds the
+// first point with a non-zero count.
+__device__ dd_t tri_min_eigenvalue(int k, const dd_t *d, const dd_t *e, dd_t *e2, int nw, unsigned *ball) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = threadIdx.x, P = 32 * nw;
+    auto sync = [&]() {
+        if (nw == 1)
+            __syncwarp();
+        else
+            asm volatile("bar.sync 1, %0;" ::"r"(P) : "memory");
+    };
+    // index of the first point (over all warps) whose flag is set, or -1
+    int half = 0;
+    auto first_set = [&](bool flag) {
+        const unsigned b = __ballot_sync(0xffffffffu, flag);
+        unsigned *hb = ball + half * nw;
+        if (lane == 0) hb[warp] = b;
+        sync();
+        int first = -1;
+        for (int w = 0; w < nw; ++w)
+            if (hb[w] != 0u) {
+                first = 32 * w + __ffs(hb[w]) - 1;
+                break;
+            }
+        half ^= 1; // the next round writes the other half: no second barrier
+        return first;
+    };
     dd_t lo = d[0], hi = d[0];
     for (int i = 0; i < k; ++i) {
         dd_t r = dd_zero();
@@ -68,27 +94,27 @@ __device__ dd_t tri_min_eigenvalue(int k, const dd_t *d, const dd_t *e, dd_t *e2
         if (dd_lt(a, lo)) lo = a;
         if (dd_gt(b, hi)) hi = b;
     }
-    if (lane == 0)
+    if (g == 0)
         for (int i = 0; i + 1 < k; ++i) e2[i] = dd_mul(e[i], e[i]);
-    __syncwarp();
+    sync();
     dd_t w = dd_sub(hi, lo);
     lo = dd_sub(lo, dd_mul_d(w, 1e-10));
     hi = dd_add(hi, dd_mul_d(w, 1e-10));
+    const double PP = (double)(P + 1);
     {
         double dlo = lo.hi, dhi = hi.hi;
         for (int round = 0; round < 12; ++round) {
             const double width = dhi - dlo;
-            const double x = dlo + width * (double)(lane + 1) / 33.0;
+            const double x = dlo + width * (double)(g + 1) / PP;
             const bool below = !(x > dlo) ? false : !(x < dhi) ? true : sturm_count_d(k, d, e2, x) >= 1;
-            const unsigned ball = __ballot_sync(0xffffffffu, below);
+            const int first = first_set(below);
             double nlo, nhi;
-            if (ball == 0) {
-                nlo = dlo + width * 32.0 / 33.0;
+            if (first < 0) {
+                nlo = dlo + width * (double)P / PP;
                 nhi = dhi;
             } else {
-                const int first = __ffs(ball) - 1;
-                nhi = dlo + width * (double)(first + 1) / 33.0;
-                nlo = first == 0 ? dlo : dlo + width * (double)first / 33.0;
+                nhi = dlo + width * (double)(first + 1) / PP;
+                nlo = first == 0 ? dlo : dlo + width * (double)first / PP;
             }
             if (!(nlo < nhi) || (nlo == dlo && nhi == dhi)) break;
             dlo = nlo;
@@ -96,20 +122,20 @@ __device__ dd_t tri_min_eigenvalue(int k, const dd_t *d, const dd_t *e, dd_t *e2
         }
         const double rad = (fabs(lo.hi) + fabs(hi.hi) + (hi.hi - lo.hi)) * 0x1p-40;
         const dd_t blo = dd_max(lo, dd_from(dlo - rad)), bhi = dd_min(hi, dd_from(dhi + rad));
-        int okv = 1;
-        if (lane == 0) okv = sturm_count(k, d, e2, blo) == 0;
-        if (lane == 1) okv = dd_lt(blo, bhi) && sturm_count(k, d, e2, bhi) >= 1;
-        if (__all_sync(0xffffffffu, okv)) {
+        bool bad = false;
+        if (g == 0) bad = sturm_count(k, d, e2, blo) != 0;
+        if (g == 1) bad = !(dd_lt(blo, bhi) && sturm_count(k, d, e2, bhi) >= 1);
+        if (first_set(bad) < 0) {
             lo = blo;
             hi = bhi;
         }
     }
     for (int round = 0; round < 40; ++round) {
         const dd_t width = dd_sub(hi, lo);
-        // 32 interior points x_lane = lo + width (lane+1)/33; the smallest
+        // P interior points x_g = lo + width (g+1)/(P+1); the smallest
         // eigenvalue lies below the first x with a non-zero Sturm count,
-        // or above x_31 when there is none.
-        const dd_t x = dd_add(lo, dd_div_d(dd_mul_d(width, (double)(lane + 1)), 33.0));
+        // or above x_(P-1) when there is none.
+        const dd_t x = dd_add(lo, dd_div_d(dd_mul_d(width, (double)(g + 1)), PP));
         bool below;
         if (!dd_gt(x, lo))
             below = false;
@@ -117,15 +143,14 @@ __device__ dd_t tri_min_eigenvalue(int k, const dd_t *d, const dd_t *e, dd_t *e2
             below = true;
         else
             below = sturm_count(k, d, e2, x) >= 1;
-        const unsigned ball = __ballot_sync(0xffffffffu, below);
+        const int first = first_set(below);
         dd_t nlo, nhi;
-        if (ball == 0) {
-            nlo = dd_add(lo, dd_div_d(dd_mul_d(width, 32.0), 33.0));
+        if (first < 0) {
+            nlo = dd_add(lo, dd_div_d(dd_mul_d(width, (double)P), PP));
             nhi = hi;
         } else {
-            const int first = __ffs(ball) - 1;
-            nhi = dd_add(lo, dd_div_d(dd_mul_d(width, (double)(first + 1)), 33.0));
-            nlo = first == 0 ? lo : dd_add(lo, dd_div_d(dd_mul_d(width, (double)first), 33.0));
+            nhi = dd_add(lo, dd_div_d(dd_mul_d(width, (double)(first + 1)), PP));
+            nlo = first == 0 ? lo : dd_add(lo, dd_div_d(dd_mul_d(width, (double)first), PP));
         }
         if (!dd_lt(nlo, nhi) || (dd_eq(nlo, lo) && dd_eq(nhi, hi))) break;
         lo = nlo;
@@ -136,10 +161,11 @@ __device__ dd_t tri_min_eigenvalue(int k, const dd_t *d, const dd_t *e, dd_t *e2
 
 // Last component of the unit eigenvector of (d, e) for eigenvalue l:
 // three steps of inverse iteration with a partially pivoted tridiagonal
-// solve (single thread; k <= LZ_KMAX).
+// solve (single thread; k <= LZ_KMAX).  T - l I is factored once; each
+// step solves with the factors.
 __device__ dd_t tri_last_component(int k, const dd_t *d, const dd_t *e, dd_t l, dd_t tnorm, dd_t *v, dd_t *dd_, dd_t *du, dd_t *du2, dd_t *dl, int *piv) {
     for (int i = 0; i < k; ++i) v[i] = dd_from(1.0);
-    for (int it = 0; it < 3; ++it) {
+    {
         for (int i = 0; i < k; ++i) {
             dd_[i] = dd_sub(d[i], l);
             du[i] = (i + 1 < k) ? e[i] : dd_zero();
@@ -168,6 +194,8 @@ __device__ dd_t tri_last_component(int k, const dd_t *d, const dd_t *e, dd_t l, 
             }
         }
         if (dd_is_zero(dd_[k - 1])) dd_[k - 1] = dd_mul_d(tnorm, 1e-32);
+    }
+    for (int it = 0; it < 3; ++it) {
         for (int i = 0; i + 1 < k; ++i) {
             if (piv[i]) {
                 dd_t t = v[i];
@@ -191,8 +219,12 @@ __device__ dd_t tri_last_component(int k, const dd_t *d, const dd_t *e, dd_t l, 
     return v[k - 1];
 }
 
+// Warps of the Lanczos CTA that run the checkpoint's multisection; the last
+// warp's lane 0 computes r.r beside them.
+constexpr int LZ_EIG_WARPS = LZ_THREADS / 32 - 1;
 struct LanczosShared {
     dd_t diag[LZ_KMAX], off[LZ_KMAX], e2[LZ_KMAX];
+    unsigned ball[2 * LZ_EIG_WARPS + 2];
     dd_t v[LZ_KMAX], t0[LZ_KMAX], t1[LZ_KMAX], t2[LZ_KMAX], t3[LZ_KMAX];
     int piv[LZ_KMAX];
     dd_t alpha, beta, value, mn, mn_old, err, rr;
@@ -327,8 +359,8 @@ __global__ void __launch_bounds__(LZ_THREADS) lanczos_kernel(const int *blk_ids,
         const bool check = dd_le_d(sk, (double)kk) || k == n - 1 || d_gt_dd((double)k, sqn9);
         if (check) {
             kk = 0;
-            if (tid < 32) {
-                dd_t lam = tri_min_eigenvalue(k + 1, S.diag, S.off, S.e2);
+            if (tid < 32 * LZ_EIG_WARPS) {
+                dd_t lam = tri_min_eigenvalue(k + 1, S.diag, S.off, S.e2, LZ_EIG_WARPS, S.ball);
                 if (tid == 0) {
                     dd_t lo = S.diag[0], hi = S.diag[0];
                     for (int i = 0; i <= k; ++i) {
@@ -343,8 +375,8 @@ __global__ void __launch_bounds__(LZ_THREADS) lanczos_kernel(const int *blk_ids,
                 }
             }
         }
-        // r.r on warp 1, beside warp 0's checkpoint
-        if (tid == 32) S.rr = seq_dot(n, r, r);
+        // r.r on the last warp, beside the checkpoint's warps
+        if (tid == 32 * LZ_EIG_WARPS) S.rr = seq_dot(n, r, r);
         __syncthreads();
         if (tid == 0) {
             S.beta = dd_sqrt(S.rr);
@@ -430,7 +462,8 @@ __global__ void __launch_bounds__(32) small_min_eig_kernel(const int *blk_ids, c
         if (lane + 1 < n) e[lane] = A[lane + 1][lane];
     }
     __syncwarp();
-    const dd_t lam = tri_min_eigenvalue(n, d, e, e2);
+    __shared__ unsigned ball[4];
+    const dd_t lam = tri_min_eigenvalue(n, d, e, e2, 1, ball);
     if (lane == 0) out[blockIdx.x] = lam;
 }
 
