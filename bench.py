@@ -434,7 +434,8 @@ def other_solves(sddd, args, local, world):
     return out
 
 
-KERNELS = ("potrf_trailing_update", "potrf_trailing_update_tc", "potrf_panel", "potrf_diag", "trsv", "schur_build", "min_eig")
+KERNELS = ("potrf_trailing_update", "potrf_trailing_update_tc", "potrf_panel", "potrf_diag", "potrf_diag_pre", "trsv", "trsv_diag_inverse", "schur_build",
+           "min_eig")
 
 
 def run_ours(args, world, rank, local):

@@ -432,17 +432,36 @@ __global__ void __launch_bounds__(PANEL_THREADS) potrf_panel_kernel(dd_t *A, lon
 // The next diagonal block's update by the panel just solved, ahead of the
 // trailing update (the split form's lookahead): D(i, j) -= P(j, k) P(i, k)
 // for k ascending, i >= j; CTA j takes column j, thread i row i.  D is the
-// nb x nb block at c0, P its rows of the nbp panel columns before c0, staged
-// in shared memory first (column by column, coalesced) so that the chain of
-// each entry reads no global memory.
-__global__ void potrf_diag_pre_kernel(dd_t *A, long lda, int c0, int nb, int nbp, const int *info) {
-    extern __shared__ double2 pre_sp[]; // pre_sp[k * blockDim.x + r] = P(r, k)
+// nb x nb block at c0, P its rows of the nbp panel columns before c0,
+// staged in shared memory first (one bulk copy per panel column: its nb
+// rows are contiguous) so that the chain of each entry reads no global
+// memory.
+__global__ void potrf_diag_pre_kernel(dd_t *A, long lda, int c0, int nb, int nbp, int *info) {
+    extern __shared__ __align__(16) double2 pre_sp[]; // pre_sp[k * blockDim.x + r] = P(r, k)
+    __shared__ uint64_t pbar;
+    __shared__ int pfail;
     if (*info != 0) return;
     const int j = blockIdx.x, i = threadIdx.x, w = blockDim.x;
     const dd_t *P = A + c0 + lda * (long)(c0 - nbp);
-    for (int k = 0; k < nbp; ++k) pre_sp[k * w + i] = i < nb ? *reinterpret_cast<const double2 *>(P + i + lda * (long)k) : make_double2(0.0, 0.0);
+    if (i == 0) {
+        mbar_init(&pbar, 1);
+        mbar_init_fence();
+        pfail = 0;
+    }
     __syncthreads();
-    if (i < j || i >= nb) return;
+    if (i < 32) {
+        if (i == 0) mbar_expect_tx(&pbar, (uint32_t)(sizeof(double2) * nb * nbp));
+        __syncwarp();
+        for (int k = i; k < nbp; k += 32) bulk_g2s(pre_sp + k * w, P + lda * (long)k, (uint32_t)(sizeof(double2) * nb), &pbar);
+    }
+    if (i == 0 && !bar_wait0(&pbar)) {
+        // the copies did not land in time: report, let them land (bounded)
+        pfail = 1;
+        atomicCAS(info, 0, -1);
+        bar_wait0(&pbar);
+    }
+    __syncthreads();
+    if (pfail || i < j || i >= nb) return;
     dd_t *d = A + (c0 + i) + lda * (long)(c0 + j);
     dd_t x = ld_dd(d);
     for (int k = 0; k < nbp; ++k) {
