@@ -128,9 +128,22 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
         }
 }
 
+// 64 x 64 tiles (4 x 4 entries a thread) when they fill the GPU; for
+// small products (fewer 64 x 64 tiles than half the SMs) 16 x 16 tiles
+// with one entry a thread, so the work spreads over more SMs.  Each
+// entry's k-order is the same either way.
+constexpr long GEMM_SMALL_TILES = 74;
 template <bool TA, bool TB, int MODE>
 static void gemm_launch(cudaStream_t st, int M, int N, int K, const dd_t *A, long lda, long sA, const dd_t *B, long ldb, long sB, dd_t *C, long ldc,
                         long sC, int batch, bool lower, dd_t alpha = dd_t{1.0, 0.0}) {
+    if ((long)ceil_div(N, 64) * ceil_div(M, 64) * batch < GEMM_SMALL_TILES) {
+        constexpr int BM = 16, BN = 16, BK = 16, TM = 1, TN = 1;
+        dim3 grid(ceil_div(N, BN), ceil_div(M, BM), batch);
+        gemm_kernel<BM, BN, BK, TM, TN, TA, TB, MODE>
+            <<<grid, (BM / TM) * (BN / TN), 0, st>>>(M, N, K, A, lda, sA, B, ldb, sB, C, ldc, sC, lower ? 1 : 0, alpha);
+        CK_LAUNCH();
+        return;
+    }
     constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4;
     dim3 grid(ceil_div(N, BN), ceil_div(M, BM), batch);
     gemm_kernel<BM, BN, BK, TM, TN, TA, TB, MODE>
