@@ -927,6 +927,52 @@ __global__ void inv_lower_kernel(const dd_t *L, long lda, int n, dd_t *X, long l
     }
     for (int i = tid; i < n; i += nt) *reinterpret_cast<double2 *>(X + i + ldx * (long)j) = col[i];
 }
+// The same for n <= 2 blockDim: thread t holds rows t and t + blockDim; the
+// L entries of step k+1 (its rows' L(i,k+1), and L(k+1,k+1) on thread 0)
+// are loaded while step k runs, so no step waits on global memory.
+constexpr int INV_THREADS = 128;
+__global__ void __launch_bounds__(INV_THREADS) inv_lower_small_kernel(const dd_t *L, long lda, int n, dd_t *X, long ldx, long sL, long sX) {
+    extern __shared__ double2 col[];
+    const int j = blockIdx.x, tid = threadIdx.x;
+    L += blockIdx.y * sL;
+    X += blockIdx.y * sX;
+    for (int i = tid; i < n; i += INV_THREADS) col[i] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+    auto lik_at = [&](int k, int r) {
+        const int i = tid + INV_THREADS * r;
+        return (i > k && i < n) ? ld_dd(L + i + lda * (long)k) : dd_zero();
+    };
+    dd_t lkk = tid == 0 ? ld_dd(L + j + lda * (long)j) : dd_zero();
+    dd_t lik[2] = {lik_at(j, 0), lik_at(j, 1)};
+    __syncthreads();
+    for (int k = j; k < n; ++k) {
+        const dd_t lkk_n = (tid == 0 && k + 1 < n) ? ld_dd(L + (k + 1) + lda * (long)(k + 1)) : dd_zero();
+        const dd_t lik_n[2] = {lik_at(k + 1, 0), lik_at(k + 1, 1)};
+        dd_t xk = dd_make(col[k].x, col[k].y);
+        if (!dd_is_zero(xk)) { // uniform across the CTA
+            if (tid == 0) {
+                xk = dd_div(xk, lkk);
+                col[k] = make_double2(xk.hi, xk.lo);
+            }
+            __syncthreads();
+            xk = dd_make(col[k].x, col[k].y);
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const int i = tid + INV_THREADS * r;
+                if (i > k && i < n) {
+                    dd_t v = dd_make(col[i].x, col[i].y);
+                    v = dd_sub(v, dd_mul(xk, lik[r]));
+                    col[i] = make_double2(v.hi, v.lo);
+                }
+            }
+            __syncthreads();
+        }
+        lkk = lkk_n;
+        lik[0] = lik_n[0];
+        lik[1] = lik_n[1];
+    }
+    for (int i = tid; i < n; i += INV_THREADS) *reinterpret_cast<double2 *>(X + i + ldx * (long)j) = col[i];
+}
+
 void inv_lower(cudaStream_t st, const dd_t *L, long lda, int n, dd_t *X, long ldx, int batch, long sL, long sX) {
     if (n <= 0 || batch <= 0) return;
     if (batch > MAX_GRID_YZ) {
@@ -935,6 +981,11 @@ void inv_lower(cudaStream_t st, const dd_t *L, long lda, int n, dd_t *X, long ld
     }
     const size_t smem = sizeof(double2) * n;
     if (smem > 227 * 1024) throw Error(ERR_UNSUPPORTED, "inv_lower: block too large for one CTA");
+    if (n <= 2 * INV_THREADS) {
+        inv_lower_small_kernel<<<dim3(n, batch), INV_THREADS, smem, st>>>(L, lda, n, X, ldx, sL, sX);
+        CK_LAUNCH();
+        return;
+    }
     if (smem > 48 * 1024) CK(cudaFuncSetAttribute(inv_lower_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     inv_lower_kernel<<<dim3(n, batch), 128, smem, st>>>(L, lda, n, X, ldx, sL, sX);
     CK_LAUNCH();
