@@ -3,8 +3,8 @@
 //   n > 20   Lanczos of Lal::getMinEigen (sdpa_linear.cpp:27-122) - same
 //            start vector, recurrences (Rtrmv/Rgemv/Rdot orders), checkpoint
 //            and stopping rules; the k x k tridiagonal eigenproblem at a
-//            checkpoint is solved for its smallest eigenpair by warp-parallel
-//            Sturm multisection plus inverse iteration (the reference uses
+//            checkpoint is solved for its smallest eigenpair by Sturm
+//            multisection over 15 warps plus inverse iteration (the reference uses
 //            implicit QR, Rsteqr; both give the eigenvalue and the last
 //            eigenvector component to dd rounding).
 //   n <= 20  M = L (D L^T) by two Rgemm, then the smallest eigenvalue of the
